@@ -1,0 +1,240 @@
+/*
+ * tanque.h — C-ABI of the B200 simulation step of the 2-D FLIP/APIC water tank.
+ *
+ * This is the drop-in boundary for the reference's CPU engine: one handle replaces one
+ * `new SimulacaoCPU(cena, opcoes)` (js/fisica-cpu.js:28-77) and each entry point below
+ * names the JavaScript method it stands in for.  Two more entry points stand in for the
+ * standalone exports of js/pressao-cpu.js (`resolverPCG`, `cicloV`).
+ *
+ * Conventions (the reference's JS owns typed arrays; here the caller owns host buffers):
+ *   - every function returns TQ_OK (0) or a negative TQ_E_* code and never throws;
+ *   - host pointers are plain caller-owned buffers, read or written only during the call;
+ *   - the library owns all device memory; one handle = one CUDA stream; a handle is not
+ *     thread-safe, separate handles may run on separate host threads;
+ *   - every wait on the device is bounded and reports TQ_E_TIMEOUT instead of hanging;
+ *   - particles are 12 floats each, the reference's CAMPOS layout
+ *     (x y vx vy cux cuy cvx cvy espuma absR absG absB, js/fisica-cpu.js:26);
+ *   - cell (i, j) is index i + j*nx; u faces (nx+1)*ny, v faces nx*(ny+1)
+ *     (js/fisica-cpu.js:39-40); the wall SDF is (2nx) x (2ny) (js/cena.js:19-24).
+ */
+#ifndef TANQUE_H
+#define TANQUE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+#define TQ_OK 0
+#define TQ_E_ARG (-1)       /* bad argument (null handle, size mismatch, bad enum) */
+#define TQ_E_CUDA (-2)      /* a CUDA runtime call failed */
+#define TQ_E_NOMEM (-3)     /* device or host allocation failed */
+#define TQ_E_CAPACITY (-4)  /* particle capacity or a fixed table size exceeded */
+#define TQ_E_TIMEOUT (-5)   /* a bounded device-side wait gave up */
+#define TQ_E_NODEV (-6)     /* no CUDA device, or the requested one is missing */
+#define TQ_E_STATE (-7)     /* call not valid in the handle's current state */
+
+/* ---------------------------------------------------------------- option enums */
+/* Storage type of the multigrid preconditioner's vectors (x, b, tmp on every level).
+ * Arithmetic is FP32 in all cases; CG vectors stay FP32, dots/norms FP64. */
+#define TQ_PREC_FP32 0
+#define TQ_PREC_FP16 1
+#define TQ_PREC_BF16 2
+
+/* Execution engine of the pressure solve.
+ * PLAIN: one kernel launch per reference dispatch (the decomposition of js/gpu/pcg.js and
+ *        js/gpu/multigrid.js), host-driven iteration loop.
+ * FUSED: the whole MGPCG solve in one persistent cooperative kernel with bounded grid
+ *        barriers; the coarse levels run inside one CTA's shared memory. */
+#define TQ_ENGINE_PLAIN 0
+#define TQ_ENGINE_FUSED 1
+
+/* Particle-to-grid transfer semantics (the oracle implements both; the CUDA library only
+ * TQ_P2G_FIXED, the integer accumulation of js/gpu/fisica.js:77-131). */
+#define TQ_P2G_FLOAT 0 /* js/fisica-cpu.js:198-267: float sums in particle order */
+#define TQ_P2G_FIXED 1 /* i32 sums of round(w*val*65536): order independent, bit-exact */
+
+/* ---------------------------------------------------------------- options */
+/* Mirrors `new SimulacaoCPU(cena, opcoes)` (js/fisica-cpu.js:29-37, 64) plus the scene
+ * size of `new Cena(nx, ny, h)` (js/cena.js:15-18). */
+typedef struct tq_options {
+  int32_t nx, ny;            /* grid cells (Cena.nx, Cena.ny) */
+  double h;                  /* cell size in metres (Cena.h) */
+  double gravity[2];         /* opcoes.gravidade, default {0, -9.81} */
+  int32_t iterations;        /* opcoes.iteracoes (ITERACOES_PCG = 3); with tolerance > 0:
+                                the iteration cap */
+  int32_t air;               /* opcoes.ar (bubble tracking on/off), default 1 */
+  double tau_density;        /* opcoes.tauDensidade, default TAU_DENSIDADE = 0.1 s */
+  double surface_tension;    /* opcoes.tensao, default TENSAO_SUPERFICIAL = 0.0728 N/m */
+  double tolerance;          /* 0: fixed iteration count as in the reference; > 0: stop when
+                                ||r|| <= tolerance * ||r0|| (same norm as js/pressao-cpu.js:342) */
+  int32_t precision;         /* TQ_PREC_* */
+  int32_t engine;            /* TQ_ENGINE_* */
+  int32_t p2g_mode;          /* TQ_P2G_* */
+  int32_t capacity;          /* particle capacity; 0: ceil(nx*ny*PARTICULAS_MAX_POR_CELULA) */
+  int32_t device;            /* CUDA device ordinal */
+  int32_t reserved[7];
+} tq_options;
+
+/* Fills defaults for an nx x ny tank of cell size h. */
+void tq_options_default(tq_options* o, int32_t nx, int32_t ny, double h);
+
+/* ---------------------------------------------------------------- tools */
+/* aplicarFerramenta(f) (js/fisica-cpu.js:129-152). kind: 0 none, 1 esponja (sponge, removes
+ * particles in the circle), 2 mao (hand, pulls velocities toward (vx, vy)), 3 corante (dye). */
+typedef struct tq_tool {
+  int32_t kind;
+  int32_t pad;
+  double x, y, radius, vx, vy;
+  double absorb[3];
+} tq_tool;
+
+/* ---------------------------------------------------------------- handle */
+typedef struct tq_sim tq_sim;
+
+/* new SimulacaoCPU(cena, opcoes) (js/fisica-cpu.js:29-77).  The walls start as the empty
+ * tank of `new Cena(nx, ny, h)` (frame of MOLDURA cells, js/cena.js:132-144). */
+int tq_create(const tq_options* opts, tq_sim** out);
+int tq_destroy(tq_sim* s);
+
+/* Cena edits + SimulacaoCPU.atualizarParedes() (js/fisica-cpu.js:80-85): uploads the caller's
+ * SDF (mw = 2*nx by mh = 2*ny floats, in cells) and recomputes the solid-cell mask
+ * (Cena.celulaSolida, js/cena.js:119-127). */
+int tq_set_walls(tq_sim* s, const float* sdf, int32_t mw, int32_t mh);
+
+/* SimulacaoCPU.adicionar(lista, checarCheia) (js/fisica-cpu.js:92-111).  Particles inside
+ * walls or (check_full) in a cell already holding >= 3 particles are skipped.  *accepted
+ * receives the count kept.  Particles beyond capacity: TQ_E_CAPACITY, nothing added. */
+int tq_add_particles(tq_sim* s, const float* list, int32_t n, int32_t check_full,
+                     int32_t* accepted);
+
+/* MotorCPU.limparAgua without the air reset: sim.n = 0, contagemCelula.fill(0)
+ * (js/motor.js:95). */
+int tq_clear_particles(tq_sim* s);
+
+/* SimulacaoCPU.aplicarFerramenta(f) (js/fisica-cpu.js:129-152). */
+int tq_apply_tool(tq_sim* s, const tq_tool* tool);
+
+/* SimulacaoCPU.avancar(dt, subpassos) (js/fisica-cpu.js:155-159): relabels the air once,
+ * then runs `substeps` substeps of dt/substeps. */
+int tq_advance(tq_sim* s, double dt, int32_t substeps);
+
+/* SimulacaoCPU.subpasso(dt) (js/fisica-cpu.js:176-189). */
+int tq_substep(tq_sim* s, double dt);
+
+/* SimulacaoCPU.atualizarAr() (js/fisica-cpu.js:162-167) — RastreadorDeAr.atualizar
+ * (js/ar.js:56-153) on the device. */
+int tq_update_air(tq_sim* s);
+
+/* SimulacaoCPU.reiniciarAr() (js/fisica-cpu.js:170-174). */
+int tq_reset_air(tq_sim* s);
+
+/* sim.n */
+int tq_count(tq_sim* s, int32_t* n);
+
+/* sim.p.subarray(0, 12*n) in the reference's order (insertion order, dead particles removed
+ * stably).  cap is the capacity of `out` in particles. */
+int tq_get_particles(tq_sim* s, float* out, int32_t cap, int32_t* n);
+
+/* Replaces every particle (state restore; no filtering). */
+int tq_set_particles(tq_sim* s, const float* list, int32_t n);
+
+/* Copies a field out of / into the handle.  `bytes` must equal the field's size. */
+enum tq_field {
+  TQ_FIELD_TIPO = 0,            /* u8  N      tipo            (js/fisica-cpu.js:52) */
+  TQ_FIELD_ROTULO = 1,          /* u32 N      rotulo          (js/ar.js:27) */
+  TQ_FIELD_CONTAGEM = 2,        /* u32 N      contagemCelula  (js/fisica-cpu.js:50) */
+  TQ_FIELD_SOLIDO = 3,          /* u8  N      solidoCelula    (js/fisica-cpu.js:53) */
+  TQ_FIELD_U = 4,               /* f32 nu     u               (js/fisica-cpu.js:41) */
+  TQ_FIELD_V = 5,               /* f32 nv     v */
+  TQ_FIELD_Q = 6,               /* f32 N      q (pressure, p*dt/(rho*h)) */
+  TQ_FIELD_DIV = 7,             /* f32 N      div */
+  TQ_FIELD_DENSIDADE = 8,       /* f32 N      densidade */
+  TQ_FIELD_FASE = 9,            /* f32 N      fase (blurred water fraction) */
+  TQ_FIELD_CURVATURA = 10,      /* f32 N      curvatura */
+  TQ_FIELD_QAR = 11,            /* f32 N      qAr */
+  TQ_FIELD_PRESSAO_BOLHA = 12,  /* f32 4096   pressaoBolha (Pa) */
+  TQ_FIELD_VOLUME_ALVO = 13,    /* f32 4096   rastreador.volumeAlvo */
+  TQ_FIELD_VOLUME_BOLHA = 14,   /* f32 4096   volumeBolha */
+  TQ_FIELD_RHS_BOLHA = 15,      /* f32 4096   rhsBolha */
+  TQ_FIELD_Y_BOLHA = 16,        /* f32 4096   yBolha */
+  TQ_FIELD_VIVO = 17,           /* u8  4096   rastreador.vivo */
+  TQ_FIELD_U_VALIDA = 18,       /* u8  nu     uValida */
+  TQ_FIELD_V_VALIDA = 19,       /* u8  nv     vValida */
+  TQ_FIELD_U_PESO = 20,         /* f32 nu     uPeso */
+  TQ_FIELD_V_PESO = 21,         /* f32 nv     vPeso */
+  TQ_FIELD_NORMAL_X = 22,       /* f32 N      normalX */
+  TQ_FIELD_NORMAL_Y = 23,       /* f32 N      normalY */
+  TQ_FIELD_COR_CELULA = 24,     /* f32 3N     corCelula */
+  TQ_FIELD_ACC_U = 25,          /* i32 2nu    fixed-point (value, weight) sums, TQ_P2G_FIXED */
+  TQ_FIELD_ACC_V = 26,          /* i32 2nv */
+  TQ_FIELD_ACC_CEL = 27,        /* i32 2N     (density*65536, particle count) */
+  TQ_FIELD_ACC_COR = 28,        /* i32 3N     dye*256 */
+  TQ_FIELD_SDF = 29,            /* f32 4N     wall SDF (2nx by 2ny) */
+  TQ_FIELD_COUNT_ = 30
+};
+int tq_get_field(tq_sim* s, int32_t field, void* out, int64_t bytes);
+int tq_set_field(tq_sim* s, int32_t field, const void* in, int64_t bytes);
+
+/* Scalars (read; some writable for state restore). */
+enum tq_scalar {
+  TQ_SCALAR_VMAX = 0,           /* sim.vMax: largest particle speed of the last G2P */
+  TQ_SCALAR_PRIMEIRA = 1,       /* rastreador.primeira (1/0) — writable */
+  TQ_SCALAR_TIPOS_PRONTOS = 2,  /* sim.tiposProntos (1/0) — writable */
+  TQ_SCALAR_PCG_ITERS = 3,      /* iterations run by the last pressure solve */
+  TQ_SCALAR_PCG_RES0 = 4,       /* ||r0|| of the last solve */
+  TQ_SCALAR_PCG_RES = 5,        /* final ||r|| of the last solve */
+  TQ_SCALAR_COUNT_ = 6
+};
+int tq_get_scalar(tq_sim* s, int32_t which, double* out);
+int tq_set_scalar(tq_sim* s, int32_t which, double value);
+
+/* The residual-norm history `normas` returned by the last resolverPCG call
+ * (js/pressao-cpu.js:343, 386, 401). */
+int tq_last_norms(tq_sim* s, double* out, int32_t cap, int32_t* n);
+
+/* Waits for the handle's stream. */
+int tq_sync(tq_sim* s);
+
+/* Device time (ms, CUDA events on the handle's stream) spent in each stage by the last
+ * tq_advance/tq_substep when timing is enabled; stage order: p2g, cells+labels, surface,
+ * divergence+bubbles, pressure, gradient+extrapolation, g2p, air relabel. */
+int tq_set_timing(tq_sim* s, int32_t enabled);
+int tq_get_timing(tq_sim* s, double* ms_out, int32_t cap, int32_t* n);
+
+/* ---------------------------------------------------------------- standalone solver */
+/* Bubble description for the standalone solve: `bolhas = { rotulo, rhs, y }` of
+ * resolverPCG (js/pressao-cpu.js:291-296).  y is read as the initial guess and receives
+ * the solved bubble pressures of the active bubbles. */
+typedef struct tq_bubbles {
+  const uint32_t* rotulo; /* N labels (0 none, 1 atmosphere, >=2 bubble) */
+  const float* rhs;       /* 4096 */
+  float* y;               /* 4096 */
+} tq_bubbles;
+
+/* resolverPCG(niveis, tipo, div, q, iteracoes, bolhas) (js/pressao-cpu.js:296-402) on the
+ * device: solves n*q - sum(q_nb) = -div on water cells starting from q.  tolerance = 0 runs
+ * exactly `iterations`; > 0 stops at ||r|| <= tolerance*||r0|| (cap `iterations`).
+ * norms receives the residual history (initial, then one per iteration). */
+int tq_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float* div, float* q,
+                      int32_t iterations, double tolerance, const tq_bubbles* bubbles,
+                      int32_t precision, int32_t engine, double* norms, int32_t norms_cap,
+                      int32_t* n_norms);
+
+/* cicloV(niveis) (js/pressao-cpu.js:241-255) on the device: one V-cycle approximately
+ * solving A x = b on the level-0 grid described by `tipo` (the types the preconditioner
+ * sees), starting from x = 0.  x receives the result. */
+int tq_vcycle(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float* x,
+              int32_t precision);
+
+/* ---------------------------------------------------------------- errors */
+const char* tq_status_string(int status);
+/* Last error message of the calling thread (CUDA error text or argument problem). */
+const char* tq_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TANQUE_H */

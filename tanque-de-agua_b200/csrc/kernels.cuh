@@ -1,0 +1,51 @@
+// kernels.cuh — host launchers of the substep kernels (one translation unit each).
+#pragma once
+#include "common.cuh"
+
+namespace tq {
+
+// particulas.cu
+void lancarP2G(const Dev& d, int nHint, cudaStream_t s);
+void lancarFaces(const Dev& d, float gdx, float gdy, cudaStream_t s);
+void lancarG2P(const Dev& d, int nHint, double dt, cudaStream_t s);
+void lancarCompactar(const Dev& d, int nHint, int* cont, int* offs, int* estado, cudaStream_t s);
+void lancarAdicionar(const Dev& d, const float* lista, int total, int checar, int* cont, int* offs,
+                     unsigned long long idBase, cudaStream_t s);
+void lancarEmpacotar(const Dev& d, float* out, int n, cudaStream_t s);
+void lancarDesempacotar(const Dev& d, const float* in, int n, unsigned long long idBase, cudaStream_t s);
+void lancarFerramenta(const Dev& d, int nHint, const tq_tool& f, cudaStream_t s);
+
+// grade.cu
+void lancarSolidos(const Dev& d, cudaStream_t s);
+void lancarTipos(const Dev& d, bool ar, cudaStream_t s);
+void lancarPropagarRotulos(const Dev& d, cudaStream_t s);
+void lancarSuperficie(const Dev& d, cudaStream_t s);
+void lancarPressaoDoAr(const Dev& d, double dt, double tensao, cudaStream_t s);
+void lancarClassificar(const Dev& d, double dt, double tau, cudaStream_t s);
+void lancarLadoDireitoBolhas(const Dev& d, double dt, cudaStream_t s);
+void lancarPosPressao(const Dev& d, double dt, bool ar, cudaStream_t s);
+void lancarGradiente(const Dev& d, cudaStream_t s);
+void lancarExtrapolar(const Dev& d, cudaStream_t s);
+
+// pcg.cu — the pressure solve on the handle's grid.
+struct Pcg;
+Pcg* criarPcg(int nx, int ny, int precisao, int motor);
+void destruirPcg(Pcg* p);
+// Solves for d.q on the cells d.tipo marks as water; bubbles from d.rotulo / d.rhsB / d.yB when
+// `bolhas`.  Returns TQ_OK or an error status; *iters receives the iterations done.
+int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s);
+int normasPcg(Pcg* p, double* out, int cap);
+int itersPcg(Pcg* p);
+// One V-cycle from device buffers (level-0 types, right-hand side, result).
+int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cudaStream_t s);
+
+// ar.cu — RastreadorDeAr.atualizar on the device.
+struct Rastreador;
+Rastreador* criarRastreador(int nx, int ny);
+void destruirRastreador(Rastreador* r);
+void reiniciarRastreador(Rastreador* r, const Dev& d, cudaStream_t s);
+int atualizarRastreador(Rastreador* r, const Dev& d, cudaStream_t s);
+int primeiraRastreador(Rastreador* r);
+void definirPrimeiraRastreador(Rastreador* r, int v);
+
+}  // namespace tq

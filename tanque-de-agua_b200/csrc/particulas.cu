@@ -1,0 +1,498 @@
+// particulas.cu — particle kernels of the substep: particle-to-grid transfer (fixed point),
+// face normalisation + gravity + wall faces, grid-to-particle transfer with APIC, micro-step
+// advection and wall collision, and the particle bookkeeping (insert, tools, compaction).
+//
+// Built with -fmad=false: the f32 operations of the fixed-point transfer must be exactly the
+// sequence the oracle restates (no contraction into fused multiply-adds), and the double
+// arithmetic of the grid-to-particle transfer then follows the reference's JavaScript
+// (double locals, f32 stores) operation for operation.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace tq {
+
+// ---------------------------------------------------------------- P2G
+// Integer particle-to-grid sums of js/gpu/fisica.js:77-131 (APIC velocity with affine term,
+// weights, bilinear density at cell centres, particle count, dye x256).  The CPU engine's
+// float sums (js/fisica-cpu.js:198-267) depend on particle order; integer sums do not, so
+// any thread schedule produces the same bits.
+__device__ __forceinline__ int chao(float v, int lo, int hi) {
+  float f = floorf(v);
+  f = fminf(fmaxf(f, (float)lo), (float)hi);
+  return (int)f;
+}
+
+__global__ void k_p2g(Dev d) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.esc->n) return;
+  const float4 a = d.p0[k];
+  const float x = a.x, y = a.y;
+  if (!(x == x)) return;  // marked dead earlier in this frame
+  const float4 c = d.p1[k];
+  const int nx = d.nx, ny = d.ny;
+  const float hf = d.hf;
+  const float inv = __fdiv_rn(1.0f, hf);
+  {
+    float fx = x * inv, fy = y * inv - 0.5f;
+    int i0 = chao(fx, 0, nx - 1), j0 = chao(fy, 0, ny - 2);
+    float tx = fx - (float)i0, ty = fy - (float)j0;
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int aa = 0; aa < 2; aa++) {
+        float wx = aa ? tx : 1.0f - tx, wy = b ? ty : 1.0f - ty;
+        float w = wx * wy;
+        float dx = (float)(i0 + aa) * hf - x;
+        float dy = ((float)(j0 + b) + 0.5f) * hf - y;
+        float t1 = c.x * dx, t2 = c.y * dy;
+        float val = a.z + (t1 + t2);
+        float wv = w * val;
+        int idx = i0 + aa + (j0 + b) * (nx + 1);
+        atomicAdd(&d.accU[idx].x, __float2int_rn(wv * 65536.0f));
+        atomicAdd(&d.accU[idx].y, __float2int_rn(w * 65536.0f));
+      }
+  }
+  {
+    float fx = x * inv - 0.5f, fy = y * inv;
+    int i0 = chao(fx, 0, nx - 2), j0 = chao(fy, 0, ny - 1);
+    float tx = fx - (float)i0, ty = fy - (float)j0;
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int aa = 0; aa < 2; aa++) {
+        float wx = aa ? tx : 1.0f - tx, wy = b ? ty : 1.0f - ty;
+        float w = wx * wy;
+        float dx = ((float)(i0 + aa) + 0.5f) * hf - x;
+        float dy = (float)(j0 + b) * hf - y;
+        float t1 = c.z * dx, t2 = c.w * dy;
+        float val = a.w + (t1 + t2);
+        float wv = w * val;
+        int idx = i0 + aa + (j0 + b) * nx;
+        atomicAdd(&d.accV[idx].x, __float2int_rn(wv * 65536.0f));
+        atomicAdd(&d.accV[idx].y, __float2int_rn(w * 65536.0f));
+      }
+  }
+  {
+    float fx = x * inv - 0.5f, fy = y * inv - 0.5f;
+    int i0 = chao(fx, 0, nx - 2), j0 = chao(fy, 0, ny - 2);
+    float tx = fx - (float)i0, ty = fy - (float)j0;
+    float ox = 1.0f - tx, oy = 1.0f - ty;
+    int cc = i0 + j0 * nx;
+    atomicAdd(&d.accCel[cc].x, __float2int_rn((ox * oy) * 65536.0f));
+    atomicAdd(&d.accCel[cc + 1].x, __float2int_rn((tx * oy) * 65536.0f));
+    atomicAdd(&d.accCel[cc + nx].x, __float2int_rn((ox * ty) * 65536.0f));
+    atomicAdd(&d.accCel[cc + nx + 1].x, __float2int_rn((tx * ty) * 65536.0f));
+  }
+  int ci = chao(x * inv, 0, nx - 1), cj = chao(y * inv, 0, ny - 1);
+  int cc = ci + cj * nx;
+  atomicAdd(&d.accCel[cc].y, 1);
+  const float4 e = d.p2[k];
+  if (e.y != 0.0f || e.z != 0.0f || e.w != 0.0f) {
+    atomicAdd(&d.accCor[3 * cc], __float2int_rn(e.y * 256.0f));
+    atomicAdd(&d.accCor[3 * cc + 1], __float2int_rn(e.z * 256.0f));
+    atomicAdd(&d.accCor[3 * cc + 2], __float2int_rn(e.w * 256.0f));
+  }
+}
+
+// Face velocity from the sums, gravity impulse where a particle contributed, zero on wall
+// faces: js/fisica-cpu.js:265-266 + :271-291 in the integer form of js/gpu/fisica.js:135-160.
+__global__ void k_faces(Dev d, float gdx, float gdy) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nx = d.nx, ny = d.ny;
+  if (k < d.nu) {
+    int i = k % (nx + 1), j = k / (nx + 1);
+    int2 a = d.accU[k];
+    float val = 0.0f;
+    if (a.y > 0) val = __fadd_rn(__fdiv_rn((float)a.x, (float)a.y), gdx);
+    bool s = i == 0 || i == nx || d.solido[i - 1 + j * nx] || d.solido[i + j * nx];
+    d.u[k] = s ? 0.0f : val;
+  }
+  if (k < d.nv) {
+    int i = k % nx, j = k / nx;
+    int2 a = d.accV[k];
+    float val = 0.0f;
+    if (a.y > 0) val = __fadd_rn(__fdiv_rn((float)a.x, (float)a.y), gdy);
+    bool s = j == 0 || j == ny || d.solido[i + (j - 1) * nx] || d.solido[i + j * nx];
+    d.v[k] = s ? 0.0f : val;
+  }
+}
+
+// ---------------------------------------------------------------- G2P
+// #velocidadeEm, js/fisica-cpu.js:641-661
+__device__ inline void velocidadeEm(const Dev& d, double x, double y, double vmax, double* ox, double* oy) {
+  const int nx = d.nx, ny = d.ny;
+  double inv = 1 / d.h;
+  double vx, vy;
+  {
+    double fx = x * inv, fy = y * inv - 0.5;
+    int i0 = clampi(floori(fx), 0, nx - 1), j0 = clampi(floori(fy), 0, ny - 2);
+    double tx = fx - i0, ty = fy - j0;
+    int k = i0 + j0 * (nx + 1);
+    vx = ((double)d.u[k] * (1 - tx) + (double)d.u[k + 1] * tx) * (1 - ty) +
+         ((double)d.u[k + nx + 1] * (1 - tx) + (double)d.u[k + nx + 2] * tx) * ty;
+  }
+  {
+    double fx = x * inv - 0.5, fy = y * inv;
+    int i0 = clampi(floori(fx), 0, nx - 2), j0 = clampi(floori(fy), 0, ny - 1);
+    double tx = fx - i0, ty = fy - j0;
+    int k = i0 + j0 * nx;
+    vy = ((double)d.v[k] * (1 - tx) + (double)d.v[k + 1] * tx) * (1 - ty) +
+         ((double)d.v[k + nx] * (1 - tx) + (double)d.v[k + nx + 1] * tx) * ty;
+  }
+  double vv = hypot(vx, vy);
+  if (vv > vmax) { *ox = vx * vmax / vv; *oy = vy * vmax / vv; }
+  else { *ox = vx; *oy = vy; }
+}
+
+// #paraParticulas, js/fisica-cpu.js:556-638: APIC gather of v and C, foam and dye, speed
+// clamp, micro-steps through the projected grid velocity with SDF push-out, kill when deep
+// in a wall.  Dead particles get x = NaN and are removed by the compaction at the end of the
+// call (the reference removes them at the end of the same loop, :636).
+__global__ void k_g2p(Dev d, double dt) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.esc->n) return;
+  const float4 a = d.p0[k];
+  if (!(a.x == a.x)) return;
+  const float4 e = d.p2[k];
+  const int nx = d.nx, ny = d.ny;
+  const double h = d.h;
+  double x = a.x, y = a.y;
+  const double inv = 1 / h;
+  const double vmax = (MICROPASSO * MAX_MICROPASSOS * h) / dt;
+  const double decai = exp(-dt / ESPUMA_VIDA);
+  const double mistura = fmin(1.0, dt / DIFUSAO_CORANTE);
+  double vx = 0, vy = 0, cux = 0, cuy = 0, cvx = 0, cvy = 0;
+  {
+    double fx = x * inv, fy = y * inv - 0.5;
+    int i0 = clampi(floori(fx), 0, nx - 1), j0 = clampi(floori(fy), 0, ny - 2);
+    double tx = fx - i0, ty = fy - j0;
+    for (int b = 0; b < 2; b++)
+      for (int aa = 0; aa < 2; aa++) {
+        double val = d.u[i0 + aa + (j0 + b) * (nx + 1)];
+        double wx = aa ? tx : 1 - tx, wy = b ? ty : 1 - ty;
+        vx += wx * wy * val;
+        cux += (aa ? 1 : -1) * wy * inv * val;
+        cuy += wx * (b ? 1 : -1) * inv * val;
+      }
+  }
+  {
+    double fx = x * inv - 0.5, fy = y * inv;
+    int i0 = clampi(floori(fx), 0, nx - 2), j0 = clampi(floori(fy), 0, ny - 1);
+    double tx = fx - i0, ty = fy - j0;
+    for (int b = 0; b < 2; b++)
+      for (int aa = 0; aa < 2; aa++) {
+        double val = d.v[i0 + aa + (j0 + b) * nx];
+        double wx = aa ? tx : 1 - tx, wy = b ? ty : 1 - ty;
+        vy += wx * wy * val;
+        cvx += (aa ? 1 : -1) * wy * inv * val;
+        cvy += wx * (b ? 1 : -1) * inv * val;
+      }
+  }
+  double vel = hypot(vx, vy);
+  int ci = clampi(floori(x * inv), 0, nx - 1), cj = clampi(floori(y * inv), 0, ny - 1);
+  int cc = ci + cj * nx;
+  int2 cel = d.accCel[cc];
+  double dens = (float)cel.x * (1.0f / 65536.0f);
+  double rarefeita = suave(0.95, 0.45, dens / PARTICULAS_POR_CELULA);
+  double fonte = suave(ESPUMA_V0, ESPUMA_V1, vel) * rarefeita;
+  double espuma = fmin(1.0, (double)e.x * decai + fonte * ESPUMA_TAXA * dt);
+  float abs0 = e.y, abs1 = e.z, abs2 = e.w;
+  if (cel.y > 1) {
+    double n = cel.y;
+    double c0 = (float)d.accCor[3 * cc] * (1.0f / 256.0f);
+    double c1 = (float)d.accCor[3 * cc + 1] * (1.0f / 256.0f);
+    double c2 = (float)d.accCor[3 * cc + 2] * (1.0f / 256.0f);
+    abs0 = (float)((double)abs0 + (c0 / n - (double)abs0) * mistura);
+    abs1 = (float)((double)abs1 + (c1 / n - (double)abs1) * mistura);
+    abs2 = (float)((double)abs2 + (c2 / n - (double)abs2) * mistura);
+  }
+  if (vel > vmax) { vx *= vmax / vel; vy *= vmax / vel; }
+  if (vel > 0) atomicMax(&d.esc->vmaxBits, (unsigned long long)__double_as_longlong(vel));
+  double micro = fmin(MAX_MICROPASSOS, fmax(1.0, ceil((fmin(vel, vmax) * dt) / (MICROPASSO * h))));
+  double dm = dt / micro;
+  int nm = (int)micro;
+  for (int m = 0; m < nm; m++) {
+    double wx = vx, wy = vy;
+    if (nm > 1) velocidadeEm(d, x, y, vmax, &wx, &wy);
+    x += wx * dm;
+    y += wy * dm;
+    double dist = distancia(d, x, y);
+    if (dist < RAIO_PARTICULA) {
+      if (dist < -SDF_MAX + 0.5) {
+        d.p0[k].x = __int_as_float(0x7fc00000);
+        atomicAdd(&d.esc->mortas, 1);
+        return;
+      }
+      double nX, nY;
+      normalSdf(d, x, y, &nX, &nY);
+      double empurra = (RAIO_PARTICULA - dist) * h;
+      x += nX * empurra;
+      y += nY * empurra;
+      double vn = vx * nX + vy * nY;
+      if (vn < 0) { vx -= vn * nX; vy -= vn * nY; }
+    }
+  }
+  d.p0[k] = make_float4((float)x, (float)y, (float)vx, (float)vy);
+  d.p1[k] = make_float4((float)cux, (float)cuy, (float)cvx, (float)cvy);
+  d.p2[k] = make_float4((float)espuma, abs0, abs1, abs2);
+}
+
+// ---------------------------------------------------------------- block scan helper
+// Exclusive rank of `keep` among the threads of a 1024-thread block; *total = block count.
+__device__ int rankNoBloco(bool keep, int* total) {
+  __shared__ int somas[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned m = __ballot_sync(0xffffffffu, keep);
+  int rank = __popc(m & ((1u << lane) - 1u));
+  __syncthreads();
+  if (lane == 0) somas[w] = __popc(m);
+  __syncthreads();
+  if (w == 0) {
+    int v = somas[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
+    }
+    somas[lane] = v;
+  }
+  __syncthreads();
+  int base = w ? somas[w - 1] : 0;
+  *total = somas[31];
+  return base + rank;
+}
+
+// Exclusive scan of `n` block counts by one 1024-thread block; returns the total.
+__device__ int scanUmBloco(const int* cont, int* offs, int n) {
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 1024) {
+    int i = base + threadIdx.x;
+    int v = i < n ? cont[i] : 0;
+    // inclusive scan of v across the block
+    __shared__ int s[1024];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      int t = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
+      __syncthreads();
+      s[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < n) offs[i] = carry + s[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += s[1023];
+    __syncthreads();
+  }
+  return carry;
+}
+
+// ---------------------------------------------------------------- compaction
+// Stable removal of particles whose x is NaN (dead in G2P, or removed by the sponge tool):
+// the reference's `remover` keeps the survivors' order (js/fisica-cpu.js:114-126).  All four
+// kernels return at once when nothing died.
+__global__ void k_compactar_contar(Dev d, int* cont) {
+  if (d.esc->mortas == 0) return;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int n = d.esc->n;
+  bool viva = k < n && d.p0[k].x == d.p0[k].x;
+  int total;
+  rankNoBloco(viva, &total);
+  if (threadIdx.x == 0) cont[blockIdx.x] = total;
+}
+
+__global__ void k_compactar_scan(Dev d, const int* cont, int* offs, int nb, int* estado) {
+  if (d.esc->mortas == 0) {
+    if (threadIdx.x == 0) estado[0] = 0;
+    return;
+  }
+  int total = scanUmBloco(cont, offs, nb);
+  if (threadIdx.x == 0) {
+    estado[0] = 1;
+    estado[1] = d.esc->n;  // count before
+    d.esc->n = total;
+    d.esc->mortas = 0;
+  }
+}
+
+__global__ void k_compactar_mover(Dev d, const int* offs, const int* estado) {
+  if (!estado[0]) return;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int n = estado[1];
+  bool viva = k < n && d.p0[k].x == d.p0[k].x;
+  int total;
+  int r = rankNoBloco(viva, &total);
+  if (viva) {
+    int o = offs[blockIdx.x] + r;
+    d.q0[o] = d.p0[k];
+    d.q1[o] = d.p1[k];
+    d.q2[o] = d.p2[k];
+    d.qid[o] = d.pid[k];
+  }
+}
+
+__global__ void k_compactar_copiar(Dev d, const int* estado) {
+  if (!estado[0]) return;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.esc->n) return;
+  d.p0[k] = d.q0[k];
+  d.p1[k] = d.q1[k];
+  d.p2[k] = d.q2[k];
+  d.pid[k] = d.qid[k];
+}
+
+// ---------------------------------------------------------------- insert
+// SimulacaoCPU.adicionar (js/fisica-cpu.js:92-111): keep a new particle when the SDF at it is
+// > RAIO_PARTICULA + 0.05 and, with checarCheia, its cell held < PARTICULAS_POR_CELULA - 1
+// particles at the last transfer.  Survivors are appended in list order.
+__global__ void k_adicionar_contar(Dev d, const float* lista, int total, int checar, int* cont) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  bool ok = false;
+  if (k < total) {
+    const float* o = lista + (size_t)k * CAMPOS;
+    double x = o[0], y = o[1];
+    ok = distancia(d, x, y) > RAIO_PARTICULA + 0.05;
+    if (ok && checar) {
+      double fi = floor(x / d.h), fj = floor(y / d.h);
+      if (fi < 0 || fj < 0 || fi >= d.nx || fj >= d.ny) ok = false;
+      else {
+        int c = (int)fi + (int)fj * d.nx;
+        if (d.accCel[c].y >= PARTICULAS_POR_CELULA - 1) ok = false;
+      }
+    }
+  }
+  int t;
+  rankNoBloco(ok, &t);
+  if (threadIdx.x == 0) cont[blockIdx.x] = t;
+}
+
+__global__ void k_adicionar_scan(Dev d, const int* cont, int* offs, int nb) {
+  int total = scanUmBloco(cont, offs, nb);
+  if (threadIdx.x == 0) d.esc->aceitas = total;
+}
+
+__global__ void k_adicionar_mover(Dev d, const float* lista, int total, int checar, const int* offs,
+                                  unsigned long long idBase) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  bool ok = false;
+  const float* o = lista + (size_t)min(k, max(total - 1, 0)) * CAMPOS;
+  if (k < total) {
+    double x = o[0], y = o[1];
+    ok = distancia(d, x, y) > RAIO_PARTICULA + 0.05;
+    if (ok && checar) {
+      double fi = floor(x / d.h), fj = floor(y / d.h);
+      if (fi < 0 || fj < 0 || fi >= d.nx || fj >= d.ny) ok = false;
+      else {
+        int c = (int)fi + (int)fj * d.nx;
+        if (d.accCel[c].y >= PARTICULAS_POR_CELULA - 1) ok = false;
+      }
+    }
+  }
+  int t;
+  int r = rankNoBloco(ok, &t);
+  if (ok) {
+    int pos = offs[blockIdx.x] + r;
+    int dst = d.esc->n + pos;  // esc->n grows only in k_adicionar_fim, after this kernel
+    d.p0[dst] = make_float4(o[0], o[1], o[2], o[3]);
+    d.p1[dst] = make_float4(o[4], o[5], o[6], o[7]);
+    d.p2[dst] = make_float4(o[8], o[9], o[10], o[11]);
+    d.pid[dst] = idBase + (unsigned long long)pos;
+  }
+}
+
+__global__ void k_adicionar_fim(Dev d) { d.esc->n += d.esc->aceitas; }
+
+// ---------------------------------------------------------------- state copies
+__global__ void k_empacotar(Dev d, float* out, int n) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  float4 a = d.p0[k], b = d.p1[k], c = d.p2[k];
+  float* o = out + (size_t)k * CAMPOS;
+  o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+  o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+  o[8] = c.x; o[9] = c.y; o[10] = c.z; o[11] = c.w;
+}
+
+__global__ void k_desempacotar(Dev d, const float* in, int n, unsigned long long idBase) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float* o = in + (size_t)k * CAMPOS;
+  d.p0[k] = make_float4(o[0], o[1], o[2], o[3]);
+  d.p1[k] = make_float4(o[4], o[5], o[6], o[7]);
+  d.p2[k] = make_float4(o[8], o[9], o[10], o[11]);
+  d.pid[k] = idBase + (unsigned long long)k;
+}
+
+// ---------------------------------------------------------------- tools
+// SimulacaoCPU.aplicarFerramenta (js/fisica-cpu.js:129-152).  The sponge marks particles dead
+// (removed by the compaction, order kept); the hand pulls velocities; the dye paints.
+__global__ void k_ferramenta(Dev d, tq_tool f) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.esc->n) return;
+  float4 a = d.p0[k];
+  if (!(a.x == a.x)) return;
+  double r2 = f.radius * f.radius;
+  double dx = (double)a.x - f.x, dy = (double)a.y - f.y;
+  double d2 = dx * dx + dy * dy;
+  if (f.kind == 1) {
+    if (d2 < r2) {
+      d.p0[k].x = __int_as_float(0x7fc00000);
+      atomicAdd(&d.esc->mortas, 1);
+    }
+    return;
+  }
+  if (d2 >= r2) return;
+  double peso = 1 - sqrt(d2 / r2);
+  if (f.kind == 2) {
+    double al = fmin(1.0, peso * 0.9);
+    a.z = (float)((double)a.z + (f.vx - (double)a.z) * al);
+    a.w = (float)((double)a.w + (f.vy - (double)a.w) * al);
+    d.p0[k] = a;
+  } else if (f.kind == 3) {
+    float4 e = d.p2[k];
+    e.y = (float)f.absorb[0];
+    e.z = (float)f.absorb[1];
+    e.w = (float)f.absorb[2];
+    d.p2[k] = e;
+  }
+}
+
+// ---------------------------------------------------------------- host launchers
+void lancarP2G(const Dev& d, int nHint, cudaStream_t s) {
+  if (nHint > 0) k_p2g<<<blocos(nHint, 256), 256, 0, s>>>(d);
+}
+void lancarFaces(const Dev& d, float gdx, float gdy, cudaStream_t s) {
+  int m = d.nu > d.nv ? d.nu : d.nv;
+  k_faces<<<blocos(m, 256), 256, 0, s>>>(d, gdx, gdy);
+}
+void lancarG2P(const Dev& d, int nHint, double dt, cudaStream_t s) {
+  if (nHint > 0) k_g2p<<<blocos(nHint, 128), 128, 0, s>>>(d, dt);
+}
+void lancarCompactar(const Dev& d, int nHint, int* cont, int* offs, int* estado, cudaStream_t s) {
+  if (nHint <= 0) return;
+  int nb = blocos(nHint, 1024);
+  k_compactar_contar<<<nb, 1024, 0, s>>>(d, cont);
+  k_compactar_scan<<<1, 1024, 0, s>>>(d, cont, offs, nb, estado);
+  k_compactar_mover<<<nb, 1024, 0, s>>>(d, offs, estado);
+  k_compactar_copiar<<<nb, 1024, 0, s>>>(d, estado);
+}
+void lancarAdicionar(const Dev& d, const float* lista, int total, int checar, int* cont, int* offs,
+                     unsigned long long idBase, cudaStream_t s) {
+  int nb = blocos(total, 1024);
+  k_adicionar_contar<<<nb, 1024, 0, s>>>(d, lista, total, checar, cont);
+  k_adicionar_scan<<<1, 1024, 0, s>>>(d, cont, offs, nb);
+  k_adicionar_mover<<<nb, 1024, 0, s>>>(d, lista, total, checar, offs, idBase);
+  k_adicionar_fim<<<1, 1, 0, s>>>(d);
+}
+void lancarEmpacotar(const Dev& d, float* out, int n, cudaStream_t s) {
+  if (n > 0) k_empacotar<<<blocos(n, 256), 256, 0, s>>>(d, out, n);
+}
+void lancarDesempacotar(const Dev& d, const float* in, int n, unsigned long long idBase, cudaStream_t s) {
+  if (n > 0) k_desempacotar<<<blocos(n, 256), 256, 0, s>>>(d, in, n, idBase);
+}
+void lancarFerramenta(const Dev& d, int nHint, const tq_tool& f, cudaStream_t s) {
+  if (nHint > 0) k_ferramenta<<<blocos(nHint, 256), 256, 0, s>>>(d, f);
+}
+
+}  // namespace tq

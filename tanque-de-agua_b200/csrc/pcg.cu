@@ -1,0 +1,794 @@
+// pcg.cu — MGPCG pressure projection: PCG with a multigrid V-cycle preconditioner, each
+// enclosed air pocket one extra unknown ("supercell").  Restates js/pressao-cpu.js
+// (resolverPCG :296-402, cicloV :241-255 and its parts) on the device.
+//
+// This file is the PLAIN engine: one launch per step of the algorithm, the iteration loop on
+// the host.  The V-cycle vectors (b, x, tmp of every level) are stored as T = float, __half or
+// __nv_bfloat16 (levels below 16k cells stay float); arithmetic is FP32; dot products and
+// norms are FP64 with a fixed reduction order (bitwise reproducible); per-bubble sums are
+// 64-bit fixed point.
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include <type_traits>
+
+namespace tq {
+
+// ---------------------------------------------------------------- types and neighbours
+// The preconditioner's level-0 types: bubble air counts as water (js/pressao-cpu.js:305-308).
+__global__ void k_mg_tipo0(const uint8_t* tipo, const uint32_t* rot, uint8_t* t0, int N, int bolhas) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  uint8_t t = tipo[c];
+  if (bolhas && t == AR && rot[c] >= 2) t = AGUA;
+  t0[c] = t;
+}
+
+// tiposGrossos (js/pressao-cpu.js:63-81): air if any child is air, else water if any is water.
+__global__ void k_mg_tipo_grosso(const uint8_t* tf, int fnx, int fny, uint8_t* tg, int gnx, int gny) {
+  int C = blockIdx.x * blockDim.x + threadIdx.x;
+  if (C >= gnx * gny) return;
+  int I = C % gnx, J = C / gnx;
+  bool ar = false, agua = false;
+  for (int b = 0; b < 2; b++)
+    for (int a = 0; a < 2; a++) {
+      int i = 2 * I + a, j = 2 * J + b;
+      if (i >= fnx || j >= fny) continue;
+      uint8_t t = tf[i + j * fnx];
+      if (t == AR) ar = true;
+      else if (t == AGUA) agua = true;
+    }
+  tg[C] = ar ? AR : agua ? AGUA : SOLIDO;
+}
+
+// prepararVizinhos (js/pressao-cpu.js:44-60) packed in one byte: bits 0-3 = free (non-wall)
+// left/right/down/up neighbours, bit 4 = the cell itself is water.
+__global__ void k_viz(const uint8_t* tipo, int nx, int ny, uint8_t* viz) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nx * ny) return;
+  int i = c % nx, j = c / nx;
+  int m = 0;
+  if (i > 0 && tipo[c - 1] != SOLIDO) m |= 1;
+  if (i < nx - 1 && tipo[c + 1] != SOLIDO) m |= 2;
+  if (j > 0 && tipo[c - nx] != SOLIDO) m |= 4;
+  if (j < ny - 1 && tipo[c + nx] != SOLIDO) m |= 8;
+  if (tipo[c] == AGUA) m |= 16;
+  viz[c] = (uint8_t)m;
+}
+
+// ---------------------------------------------------------------- V-cycle kernels
+// suavizar (js/pressao-cpu.js:99-150): each 16x16 block reads the snapshot `src` (18x18 with
+// its one-cell border, zero outside the grid), runs VARREDURAS red-black sweeps inside the
+// block, and writes water cells to `dst` (other cells 0).  desl = 0 or 8 shifts the block
+// lattice; ordem = 0 sweeps red then black, 1 black then red.
+template <class T>
+__global__ void __launch_bounds__(256) k_suavizar(NivelDev<T> n, int desl, int ordem, const T* __restrict__ src,
+                                                  T* __restrict__ dst, const T* __restrict__ b) {
+  __shared__ float qs[18 * 18];
+  const int nx = n.nx, ny = n.ny;
+  const int ox = (int)blockIdx.x * 16 - desl, oy = (int)blockIdx.y * 16 - desl;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int s = threadIdx.x; s < 324; s += 256) {
+    int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
+    qs[s] = (sx >= 0 && sy >= 0 && sx < nx && sy < ny) ? carregar(src[sx + sy * nx]) : 0.0f;
+  }
+  const int gx = ox + tx, gy = oy + ty;
+  const bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
+  const int c = gx + gy * nx;
+  int vz = dentro ? n.viz[c] : 0;
+  float bv = dentro ? carregar(b[c]) : 0.0f;
+  const int li = (ty + 1) * 18 + tx + 1;
+  const int m = vz & 15;
+  const int k = __popc(m);
+  const bool ativo = (vz & 16) && k > 0;
+  const float invk = ativo ? 1.0f / (float)k : 0.0f;
+  const int minhaCor = (gx + gy + 1) & 1;
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < VARREDURAS; it++) {
+#pragma unroll
+    for (int o = 0; o < 2; o++) {
+      int cor = o ^ ordem;
+      if (ativo && minhaCor == cor) {
+        float s = 0.0f;
+        if (m & 1) s += qs[li - 1];
+        if (m & 2) s += qs[li + 1];
+        if (m & 4) s += qs[li - 18];
+        if (m & 8) s += qs[li + 18];
+        float q = qs[li];
+        qs[li] = q + ((s + bv) * invk - q);
+      }
+      __syncthreads();
+    }
+  }
+  if (dentro) dst[c] = guardar<T>((vz & 16) ? qs[li] : 0.0f);
+}
+
+// restringir (js/pressao-cpu.js:159-188) as a gather: coarse b = P^T (b - A x) over the 4x4
+// fine window (weights 1/4, 3/4, 3/4, 1/4), only on coarse water cells; coarse x = 0.
+template <class TF>
+__device__ inline float residuoFino(const NivelDev<TF>& f, const TF* __restrict__ x, const TF* __restrict__ b, int i, int j) {
+  if (i < 0 || j < 0 || i >= f.nx || j >= f.ny) return 0.0f;
+  int c = i + j * f.nx;
+  int vz = f.viz[c];
+  if (!(vz & 16)) return 0.0f;
+  float s = 0.0f;
+  if (vz & 1) s += carregar(x[c - 1]);
+  if (vz & 2) s += carregar(x[c + 1]);
+  if (vz & 4) s += carregar(x[c - f.nx]);
+  if (vz & 8) s += carregar(x[c + f.nx]);
+  return carregar(b[c]) - ((float)__popc(vz & 15) * carregar(x[c]) - s);
+}
+
+template <class TF, class TG>
+__global__ void k_restringir(NivelDev<TF> f, const TF* __restrict__ xf, const TF* __restrict__ bf, NivelDev<TG> g) {
+  int C = blockIdx.x * blockDim.x + threadIdx.x;
+  if (C >= g.nx * g.ny) return;
+  g.x[C] = guardar<TG>(0.0f);
+  if (!(g.viz[C] & 16)) {
+    g.b[C] = guardar<TG>(0.0f);
+    return;
+  }
+  int I = C % g.nx, J = C / g.nx;
+  const float w[4] = {0.25f, 0.75f, 0.75f, 0.25f};
+  float s = 0.0f;
+  for (int bb = 0; bb < 4; bb++) {
+    int j = 2 * J - 1 + bb;
+    for (int a = 0; a < 4; a++) {
+      int i = 2 * I - 1 + a;
+      s += residuoFino(f, xf, bf, i, j) * (w[a] * w[bb]);
+    }
+  }
+  g.b[C] = guardar<TG>(s);
+}
+
+// prolongar (js/pressao-cpu.js:191-214): fine x += bilinear interpolation of the coarse
+// correction, coarse water cells only.
+__device__ inline int grossoBase(int i) { return (i & 1) == 0 ? (i >> 1) - 1 : (i - 1) >> 1; }
+__device__ inline float pesoBase(int i) { return (i & 1) == 0 ? 0.25f : 0.75f; }
+
+template <class TG, class TF>
+__global__ void k_prolongar(NivelDev<TG> g, NivelDev<TF> f, TF* __restrict__ xf) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= f.nx * f.ny) return;
+  if (!(f.viz[c] & 16)) return;
+  int i = c % f.nx, j = c / f.nx;
+  int I0 = grossoBase(i), J0 = grossoBase(j);
+  float wx0 = pesoBase(i), wy0 = pesoBase(j);
+  float e = 0.0f;
+  for (int b = 0; b < 2; b++) {
+    int J = J0 + b;
+    if (J < 0 || J >= g.ny) continue;
+    float wy = b ? 1.0f - wy0 : wy0;
+    for (int a = 0; a < 2; a++) {
+      int I = I0 + a;
+      if (I < 0 || I >= g.nx) continue;
+      int C = I + J * g.nx;
+      if (g.viz[C] & 16) e += carregar(g.x[C]) * ((a ? 1.0f - wx0 : wx0) * wy);
+    }
+  }
+  xf[c] = guardar<TF>(carregar(xf[c]) + e);
+}
+
+// resolverGrosso (js/pressao-cpu.js:217-238): VARREDURAS_GROSSO alternating red-black sweeps
+// in place on the coarsest level, one CTA; the level lives in shared memory when it fits.
+__global__ void __launch_bounds__(1024) k_grosso(NivelDev<float> n, int emShared) {
+  extern __shared__ unsigned char dyn[];
+  const int N = n.nx * n.ny, nx = n.nx;
+  float* x = n.x;
+  const float* b = n.b;
+  const uint8_t* viz = n.viz;
+  if (emShared) {
+    float* xs = (float*)dyn;
+    float* bs = xs + N;
+    uint8_t* vs = (uint8_t*)(bs + N);
+    for (int c = threadIdx.x; c < N; c += blockDim.x) {
+      xs[c] = x[c];
+      bs[c] = b[c];
+      vs[c] = viz[c];
+    }
+    x = xs;
+    b = bs;
+    viz = vs;
+    __syncthreads();
+  }
+  for (int k = 0; k < VARREDURAS_GROSSO; k++)
+    for (int o = 0; o < 2; o++) {
+      int cor = (k & 1) ? 1 - o : o;
+      for (int c = threadIdx.x; c < N; c += blockDim.x) {
+        int i = c % nx, j = c / nx;
+        int vz = viz[c];
+        if (!(vz & 16) || ((i + j + 1) & 1) != cor) continue;
+        int q = __popc(vz & 15);
+        if (!q) continue;
+        float s = 0.0f;
+        if (vz & 1) s += x[c - 1];
+        if (vz & 2) s += x[c + 1];
+        if (vz & 4) s += x[c - nx];
+        if (vz & 8) s += x[c + nx];
+        x[c] = (s + b[c]) / (float)q;
+      }
+      __syncthreads();
+    }
+  if (emShared)
+    for (int c = threadIdx.x; c < N; c += blockDim.x) n.x[c] = x[c];
+}
+
+// ---------------------------------------------------------------- PCG kernels
+// Value a water cell's neighbour contributes to A*v (js/pressao-cpu.js:84-93 after difundir,
+// :318-324): water -> v, air of an active bubble -> that bubble's value (as stored in the
+// f32 grid), anything else -> 0.
+__device__ inline float valorViz(const Dev& d, const float* v, const float* vbf, int n, bool bolhas) {
+  uint8_t t = d.tipo[n];
+  if (t == AGUA) return v[n];
+  if (bolhas && t == AR) {
+    uint32_t r = d.rotulo[n];
+    if (r >= 2 && r < (uint32_t)MAX_BOLHAS && d.facesB[r] > 0) return vbf[r];
+  }
+  return 0.0f;
+}
+__device__ inline float aplicarA(const Dev& d, const uint8_t* vizOp, const float* v, const float* vbf, int c, bool bolhas) {
+  int vz = vizOp[c];
+  float s = 0.0f;
+  if (vz & 1) s += valorViz(d, v, vbf, c - 1, bolhas);
+  if (vz & 2) s += valorViz(d, v, vbf, c + 1, bolhas);
+  if (vz & 4) s += valorViz(d, v, vbf, c - d.nx, bolhas);
+  if (vz & 8) s += valorViz(d, v, vbf, c + d.nx, bolhas);
+  return (float)__popc(vz & 15) * v[c] - s;
+}
+
+// r = -div - A q on water cells (js/pressao-cpu.js:331-338); q = 0 elsewhere.
+__global__ void k_pcg_inicio(Dev d, const uint8_t* vizOp, int bolhas) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.N) return;
+  if (d.tipo[c] != AGUA) {
+    d.q[c] = 0.0f;
+    d.r[c] = 0.0f;
+    return;
+  }
+  d.r[c] = -d.div[c] - aplicarA(d, vizOp, d.q, d.ybf, c, bolhas != 0);
+}
+
+// Active bubbles (montarBolhas, js/pressao-cpu.js:271-288): faces = number of (interior bubble
+// cell, water neighbour) pairs; cels = every air cell carrying an active label (:345-351).
+__global__ void k_bolhas_faces(Dev d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.N) return;
+  const int nx = d.nx;
+  int i = c % nx, j = c / nx;
+  if (i < 1 || j < 1 || i >= nx - 1 || j >= d.ny - 1) return;
+  uint32_t b = d.rotulo[c];
+  if (b < 2 || b >= (uint32_t)MAX_BOLHAS || d.tipo[c] != AR) return;
+  unsigned k = (d.tipo[c - 1] == AGUA) + (d.tipo[c + 1] == AGUA) + (d.tipo[c - nx] == AGUA) + (d.tipo[c + nx] == AGUA);
+  if (k) atomicAdd(&d.facesB[b], k);
+}
+__global__ void k_bolhas_celulas(Dev d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.N) return;
+  uint32_t b = d.rotulo[c];
+  if (b < 2 || b >= (uint32_t)MAX_BOLHAS || d.tipo[c] != AR || d.facesB[b] == 0) return;
+  atomicAdd(&d.celsB[b], 1u);
+}
+// Initial bubble values: y from the caller (f32), zero for inactive labels.
+__global__ void k_bolhas_inicio(Dev d) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= MAX_BOLHAS) return;
+  bool at = b >= 2 && d.facesB[b] > 0;
+  double y = at ? (double)d.yBolhaF[b] : 0.0;
+  d.yB[b] = y;
+  d.ybf[b] = (float)y;
+  d.rb[b] = d.zb[b] = d.zvb[b] = d.pb[b] = d.apb[b] = 0.0;
+  d.pbf[b] = 0.0f;
+}
+
+// Bubble rows of A*v (aplicarBolhas, js/pressao-cpu.js:325-328): out[b] = faces[b]*vb[b] -
+// sum over the bubble's water faces of v[water cell].  The sum is 64-bit fixed point (2^-40).
+constexpr double ESCALA_PCG = 1099511627776.0;  // 2^40
+__global__ void k_bolhas_somar_v(Dev d, const float* v) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.N) return;
+  const int nx = d.nx;
+  int i = c % nx, j = c / nx;
+  if (i < 1 || j < 1 || i >= nx - 1 || j >= d.ny - 1) return;
+  uint32_t b = d.rotulo[c];
+  if (b < 2 || b >= (uint32_t)MAX_BOLHAS || d.tipo[c] != AR) return;
+  double s = 0;
+  if (d.tipo[c - 1] == AGUA) s += (double)v[c - 1];
+  if (d.tipo[c + 1] == AGUA) s += (double)v[c + 1];
+  if (d.tipo[c - nx] == AGUA) s += (double)v[c - nx];
+  if (d.tipo[c + nx] == AGUA) s += (double)v[c + nx];
+  if (s != 0) somaFixa(&d.accB[b], s, ESCALA_PCG);
+}
+// modo 0: rb = rhs - (faces*y - sum)  (initial bubble residual, :339-341)
+// modo 1: apb = faces*pb - sum
+__global__ void k_bolhas_linhas(Dev d, int modo) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= MAX_BOLHAS) return;
+  if (b < 2 || d.facesB[b] == 0) return;
+  double soma = (double)d.accB[b] / ESCALA_PCG;
+  if (modo == 0) d.rb[b] = (double)d.rhsBolhaF[b] - (d.facesB[b] * d.yB[b] - soma);
+  else d.apb[b] = d.facesB[b] * d.pb[b] - soma;
+}
+
+// precondicionar, js/pressao-cpu.js:352-361 — before the V-cycle: level-0 b = r, each active
+// bubble's residual spread evenly over its cells; x = 0.  `escala` normalises the right-hand
+// side for half-precision storage (the V-cycle is linear).
+template <class T>
+__global__ void k_pre_espalhar(Dev d, NivelDev<T> n0, int bolhas) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.N) return;
+  float e = (float)d.esc->escalaMG;
+  float v = d.r[c];
+  if (bolhas && d.tipo[c] == AR) {
+    uint32_t b = d.rotulo[c];
+    if (b >= 2 && b < (uint32_t)MAX_BOLHAS && d.celsB[b] > 0) v = (float)(d.rb[b] / d.celsB[b]);
+  }
+  n0.b[c] = guardar<T>(v * e);
+  n0.x[c] = guardar<T>(0.0f);
+}
+// After the V-cycle: z = x, except active bubble cells, whose mean correction becomes the
+// bubble's z (the transpose of spreading) and whose grid value is zeroed.
+template <class T>
+__global__ void k_pre_juntar(Dev d, NivelDev<T> n0, int bolhas) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.N) return;
+  float inv = (float)(1.0 / d.esc->escalaMG);
+  float x = carregar(n0.x[c]) * inv;
+  if (bolhas && d.tipo[c] == AR) {
+    uint32_t b = d.rotulo[c];
+    if (b >= 2 && b < (uint32_t)MAX_BOLHAS && d.celsB[b] > 0) {
+      somaFixa(&d.accB[b], (double)x / d.celsB[b], ESCALA_PCG);
+      d.z[c] = 0.0f;
+      return;
+    }
+  }
+  d.z[c] = x;
+}
+__global__ void k_pre_bolhas(Dev d) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= MAX_BOLHAS) return;
+  d.zb[b] = (b >= 2 && d.facesB[b] > 0) ? (double)d.accB[b] / ESCALA_PCG : 0.0;
+}
+
+// ap = A p on water cells (js/pressao-cpu.js:367-373).
+__global__ void k_aplicar(Dev d, const uint8_t* vizOp, int bolhas) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.N) return;
+  d.ap[c] = d.tipo[c] == AGUA ? aplicarA(d, vizOp, d.p, d.pbf, c, bolhas != 0) : 0.0f;
+}
+
+// q += alpha p, r -= alpha Ap on water; bubbles likewise (js/pressao-cpu.js:377-385).
+__global__ void k_atualizar(Dev d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double alfa = d.esc->alpha;
+  if (c < MAX_BOLHAS && c >= 2 && d.facesB[c] > 0) {
+    d.yB[c] += alfa * d.pb[c];
+    d.rb[c] -= alfa * d.apb[c];
+    d.ybf[c] = (float)d.yB[c];
+  }
+  if (c >= d.N || d.tipo[c] != AGUA) return;
+  float a = (float)alfa;
+  d.q[c] = d.q[c] + a * d.p[c];
+  d.r[c] = d.r[c] - a * d.ap[c];
+}
+
+// p = z + beta p on water (0 elsewhere); bubbles likewise (js/pressao-cpu.js:395-396).
+__global__ void k_direcao(Dev d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double beta = d.esc->beta;
+  if (c < MAX_BOLHAS && c >= 2 && d.facesB[c] > 0) {
+    d.pb[c] = d.zb[c] + beta * d.pb[c];
+    d.pbf[c] = (float)d.pb[c];
+  }
+  if (c >= d.N) return;
+  d.p[c] = d.tipo[c] == AGUA ? d.z[c] + (float)beta * d.p[c] : 0.0f;
+}
+// p = z, pb = zb (js/pressao-cpu.js:363-364)
+__global__ void k_copiar_pz(Dev d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < MAX_BOLHAS) {
+    d.pb[c] = d.zb[c];
+    d.pbf[c] = (float)d.zb[c];
+    d.zvb[c] = 0.0;
+  }
+  if (c < d.N) d.p[c] = d.z[c];
+}
+// zOld = z, zvb = zb (js/pressao-cpu.js:388-389)
+__global__ void k_guardar_z(Dev d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < MAX_BOLHAS) d.zvb[c] = d.zb[c];
+  if (c < d.N) d.zOld[c] = d.z[c];
+}
+// End of the solve: non-water q = 0; bubbles hand back their pressure (js/pressao-cpu.js:399-400).
+__global__ void k_pcg_fim(Dev d, int bolhas) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bolhas && c >= 2 && c < MAX_BOLHAS && d.facesB[c] > 0) d.yBolhaF[c] = (float)d.yB[c];
+  if (c < d.N && d.tipo[c] != AGUA) d.q[c] = 0.0f;
+}
+
+// ---------------------------------------------------------------- dot products
+// Two FP64 dot products over water cells (a*b1, a*b2) plus the bubble terms, in a fixed
+// reduction order; the last block to finish does the scalar step of the running solve.
+enum ModoProduto { NORMA0 = 0, RZ0 = 1, PAP = 2, NORMA = 3, BETA = 4 };
+
+constexpr int DOT_BLOCOS = 296;
+constexpr int DOT_T = 256;
+
+__device__ inline double somaBloco(double v, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0;
+  if (w == 0) {
+    t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  }
+  __syncthreads();
+  return t;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(DOT_T) k_produto(Dev d, int modo, const float* a, const float* b1, const float* b2,
+                                                 int it, double tol, int bolhas, int meiaPrecisao) {
+  __shared__ double sh[32];
+  __shared__ bool ultimo;
+  double s1 = 0, s2 = 0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.N; c += gridDim.x * blockDim.x) {
+    if (d.tipo[c] != AGUA) continue;
+    double av = a[c];
+    s1 += av * (double)b1[c];
+    if (b2) s2 += av * (double)b2[c];
+  }
+  double t1 = somaBloco(s1, sh);
+  double t2 = b2 ? somaBloco(s2, sh) : 0.0;
+  if (threadIdx.x == 0) {
+    d.parciais[2 * blockIdx.x] = t1;
+    d.parciais[2 * blockIdx.x + 1] = t2;
+    __threadfence();
+    unsigned v = atomicAdd(&d.esc->tickets[0], 1u);
+    ultimo = v == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!ultimo) return;
+  __threadfence();
+  // the last block: partials in block order, then the bubble terms in label order
+  double p1 = 0, p2 = 0;
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+    p1 += __ldcg(&d.parciais[2 * k]);
+    p2 += __ldcg(&d.parciais[2 * k + 1]);
+  }
+  double q1 = 0, q2 = 0;
+  if (bolhas) {
+    for (int b = threadIdx.x; b < MAX_BOLHAS; b += blockDim.x) {
+      if (b < 2 || d.facesB[b] == 0) continue;
+      switch (modo) {
+        case NORMA0:
+        case NORMA: q1 += d.rb[b] * d.rb[b]; break;
+        case RZ0: q1 += d.rb[b] * d.zb[b]; break;
+        case PAP: q1 += d.pb[b] * d.apb[b]; break;
+        case BETA: q1 += d.rb[b] * d.zb[b]; q2 += d.rb[b] * d.zvb[b]; break;
+      }
+    }
+  }
+  double T1 = somaBloco(p1, sh), T2 = somaBloco(p2, sh);
+  double B1 = somaBloco(q1, sh), B2 = somaBloco(q2, sh);
+  if (threadIdx.x == 0) {
+    Escalares* e = d.esc;
+    e->tickets[0] = 0;
+    double x1 = T1 + B1, x2 = T2 + B2;
+    switch (modo) {
+      case NORMA0: {
+        double nr = sqrt(x1);
+        e->norma0 = e->norma = nr;
+        e->normas[0] = nr;
+        e->iters = 0;
+        e->pronto = tol > 0 && nr <= 0.0;
+        e->escalaMG = (meiaPrecisao && nr > 0) ? 1.0 / nr : 1.0;
+        break;
+      }
+      case RZ0: e->rz = x1; break;
+      case PAP: e->pap = x1; e->alpha = fabs(x1) < 1e-30 ? 0.0 : e->rz / x1; break;
+      case NORMA: {
+        double nr = sqrt(x1);
+        e->norma = nr;
+        if (it + 1 < 1024) e->normas[it + 1] = nr;
+        e->iters = it + 1;
+        e->pronto = tol > 0 && nr <= tol * e->norma0;
+        e->escalaMG = (meiaPrecisao && nr > 0) ? 1.0 / nr : 1.0;
+        break;
+      }
+      case BETA: {
+        double rzNovo = x1, cruzado = x2;
+        e->beta = fabs(e->rz) < 1e-30 ? 0.0 : fmax(0.0, (rzNovo - cruzado) / e->rz);
+        e->rz = rzNovo;
+        break;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- the solver object
+struct Pcg {
+  int nx, ny, N, precisao, motor;
+  int L;
+  int nxL[MAX_NIVEIS], nyL[MAX_NIVEIS];
+  bool meia[MAX_NIVEIS];  // level stored in half precision
+  uint8_t* tipoL[MAX_NIVEIS];
+  uint8_t* vizL[MAX_NIVEIS];
+  void *bL[MAX_NIVEIS], *xL[MAX_NIVEIS], *tmpL[MAX_NIVEIS];
+  uint8_t* vizOp;
+  std::vector<double> normas;
+  int iters = 0;
+  size_t smemGrosso = 0;
+};
+
+constexpr int MEIA_MIN_CELULAS = 16384;
+
+static size_t tamanhoElem(int prec, bool meia) { return (meia && prec != TQ_PREC_FP32) ? 2 : 4; }
+
+Pcg* criarPcg(int nx, int ny, int precisao, int motor) {
+  Pcg* p = new Pcg();
+  p->nx = nx;
+  p->ny = ny;
+  p->N = nx * ny;
+  p->precisao = precisao;
+  p->motor = motor;
+  // montarNiveis (js/pressao-cpu.js:24-41): halve (ceil) while min(nx, ny) > 12
+  int L = 0;
+  int a = nx, b = ny;
+  p->nxL[0] = a;
+  p->nyL[0] = b;
+  L = 1;
+  while ((a < b ? a : b) > 12 && L < MAX_NIVEIS) {
+    a = (a + 1) / 2;
+    b = (b + 1) / 2;
+    p->nxL[L] = a;
+    p->nyL[L] = b;
+    L++;
+  }
+  p->L = L;
+  bool ok = true;
+  for (int l = 0; l < L; l++) {
+    size_t n = (size_t)p->nxL[l] * p->nyL[l];
+    p->meia[l] = precisao != TQ_PREC_FP32 && n >= (size_t)MEIA_MIN_CELULAS;
+    size_t e = tamanhoElem(precisao, p->meia[l]);
+    ok &= cudaMalloc(&p->tipoL[l], n) == cudaSuccess;
+    ok &= cudaMalloc(&p->vizL[l], n) == cudaSuccess;
+    ok &= cudaMalloc(&p->bL[l], n * e) == cudaSuccess;
+    ok &= cudaMalloc(&p->xL[l], n * e) == cudaSuccess;
+    ok &= cudaMalloc(&p->tmpL[l], n * e) == cudaSuccess;
+  }
+  ok &= cudaMalloc(&p->vizOp, p->N) == cudaSuccess;
+  size_t nc = (size_t)p->nxL[L - 1] * p->nyL[L - 1];
+  p->smemGrosso = nc * 9 <= 200 * 1024 ? nc * 9 : 0;
+  if (p->smemGrosso) {
+    if (cudaFuncSetAttribute(k_grosso, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smemGrosso) != cudaSuccess)
+      p->smemGrosso = 0;
+  }
+  if (!ok) {
+    destruirPcg(p);
+    return nullptr;
+  }
+  return p;
+}
+
+void destruirPcg(Pcg* p) {
+  if (!p) return;
+  for (int l = 0; l < p->L; l++) {
+    cudaFree(p->tipoL[l]);
+    cudaFree(p->vizL[l]);
+    cudaFree(p->bL[l]);
+    cudaFree(p->xL[l]);
+    cudaFree(p->tmpL[l]);
+  }
+  cudaFree(p->vizOp);
+  delete p;
+}
+
+// Level descriptor with the storage type chosen at run time.
+template <class T>
+static NivelDev<T> nivel(Pcg* p, int l) {
+  NivelDev<T> n;
+  n.nx = p->nxL[l];
+  n.ny = p->nyL[l];
+  n.tipo = p->tipoL[l];
+  n.viz = p->vizL[l];
+  n.b = (T*)p->bL[l];
+  n.x = (T*)p->xL[l];
+  n.tmp = (T*)p->tmpL[l];
+  return n;
+}
+
+// Dispatch on the storage type of level l.
+template <class F>
+static void comTipo(Pcg* p, int l, F f) {
+  if (!p->meia[l]) f((float*)nullptr);
+  else if (p->precisao == TQ_PREC_FP16) f((__half*)nullptr);
+  else f((__nv_bfloat16*)nullptr);
+}
+
+static void suavizarNivel(Pcg* p, int l, int desl, int ordem, bool paraTmp, cudaStream_t s) {
+  comTipo(p, l, [&](auto* tag) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    NivelDev<T> n = nivel<T>(p, l);
+    dim3 g((n.nx + desl + 15) / 16, (n.ny + desl + 15) / 16);
+    if (paraTmp) k_suavizar<T><<<g, 256, 0, s>>>(n, desl, ordem, n.x, n.tmp, n.b);
+    else k_suavizar<T><<<g, 256, 0, s>>>(n, desl, ordem, n.tmp, n.x, n.b);
+  });
+}
+
+static void restringirNivel(Pcg* p, int l, cudaStream_t s) {
+  comTipo(p, l, [&](auto* tf) {
+    using TF = std::remove_pointer_t<decltype(tf)>;
+    comTipo(p, l + 1, [&](auto* tg) {
+      using TG = std::remove_pointer_t<decltype(tg)>;
+      NivelDev<TF> f = nivel<TF>(p, l);
+      NivelDev<TG> g = nivel<TG>(p, l + 1);
+      k_restringir<TF, TG><<<blocos((long)g.nx * g.ny, 256), 256, 0, s>>>(f, f.x, f.b, g);
+    });
+  });
+}
+
+static void prolongarNivel(Pcg* p, int l, cudaStream_t s) {
+  comTipo(p, l + 1, [&](auto* tg) {
+    using TG = std::remove_pointer_t<decltype(tg)>;
+    comTipo(p, l, [&](auto* tf) {
+      using TF = std::remove_pointer_t<decltype(tf)>;
+      NivelDev<TG> g = nivel<TG>(p, l + 1);
+      NivelDev<TF> f = nivel<TF>(p, l);
+      k_prolongar<TG, TF><<<blocos((long)f.nx * f.ny, 256), 256, 0, s>>>(g, f, f.x);
+    });
+  });
+}
+
+// cicloV (js/pressao-cpu.js:241-255); level-0 b and x = 0 already in place.
+static void cicloV(Pcg* p, cudaStream_t s) {
+  const int L = p->L;
+  for (int l = 0; l < L - 1; l++) {
+    suavizarNivel(p, l, 0, 0, true, s);
+    suavizarNivel(p, l, 8, 0, false, s);
+    restringirNivel(p, l, s);
+  }
+  NivelDev<float> g = nivel<float>(p, L - 1);
+  if (L == 1) cudaMemsetAsync(g.x, 0, sizeof(float) * g.nx * g.ny, s);
+  k_grosso<<<1, 1024, p->smemGrosso, s>>>(g, p->smemGrosso ? 1 : 0);
+  for (int l = L - 2; l >= 0; l--) {
+    prolongarNivel(p, l, s);
+    suavizarNivel(p, l, 8, 1, true, s);
+    suavizarNivel(p, l, 0, 1, false, s);
+  }
+}
+
+// Types and neighbour masks of every level for this solve.
+static void prepararNiveis(Pcg* p, const uint8_t* tipo0, cudaStream_t s) {
+  if (tipo0 != p->tipoL[0]) cudaMemcpyAsync(p->tipoL[0], tipo0, p->N, cudaMemcpyDeviceToDevice, s);
+  for (int l = 1; l < p->L; l++)
+    k_mg_tipo_grosso<<<blocos((long)p->nxL[l] * p->nyL[l], 256), 256, 0, s>>>(
+        p->tipoL[l - 1], p->nxL[l - 1], p->nyL[l - 1], p->tipoL[l], p->nxL[l], p->nyL[l]);
+  for (int l = 0; l < p->L; l++)
+    k_viz<<<blocos((long)p->nxL[l] * p->nyL[l], 256), 256, 0, s>>>(p->tipoL[l], p->nxL[l], p->nyL[l], p->vizL[l]);
+}
+
+static void precondicionar(Pcg* p, const Dev& d, bool bolhas, cudaStream_t s) {
+  int nb = blocos(d.N, 256);
+  comTipo(p, 0, [&](auto* tag) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    k_pre_espalhar<T><<<nb, 256, 0, s>>>(d, nivel<T>(p, 0), bolhas ? 1 : 0);
+  });
+  cicloV(p, s);
+  if (bolhas) cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
+  comTipo(p, 0, [&](auto* tag) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    k_pre_juntar<T><<<nb, 256, 0, s>>>(d, nivel<T>(p, 0), bolhas ? 1 : 0);
+  });
+  if (bolhas) k_pre_bolhas<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d);
+}
+
+static void produto(Pcg* p, const Dev& d, int modo, const float* a, const float* b1, const float* b2, int it,
+                    double tol, bool bolhas, cudaStream_t s) {
+  k_produto<<<DOT_BLOCOS, DOT_T, 0, s>>>(d, modo, a, b1, b2, it, tol, bolhas ? 1 : 0,
+                                         p->precisao != TQ_PREC_FP32 ? 1 : 0);
+}
+
+int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s) {
+  const int nb = blocos(d.N, 256);
+  const int nbx = blocos(d.N > MAX_BOLHAS ? d.N : MAX_BOLHAS, 256);
+  // operator (true types) and preconditioner types
+  k_viz<<<nb, 256, 0, s>>>(d.tipo, d.nx, d.ny, p->vizOp);
+  k_mg_tipo0<<<nb, 256, 0, s>>>(d.tipo, d.rotulo, p->tipoL[0], d.N, bolhas ? 1 : 0);
+  prepararNiveis(p, p->tipoL[0], s);
+  cudaMemsetAsync(d.facesB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
+  cudaMemsetAsync(d.celsB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
+  if (bolhas) {
+    k_bolhas_faces<<<nb, 256, 0, s>>>(d);
+    k_bolhas_celulas<<<nb, 256, 0, s>>>(d);
+  }
+  k_bolhas_inicio<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d);
+  k_pcg_inicio<<<nb, 256, 0, s>>>(d, p->vizOp, bolhas ? 1 : 0);
+  if (bolhas) {
+    cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
+    k_bolhas_somar_v<<<nb, 256, 0, s>>>(d, d.q);
+    k_bolhas_linhas<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d, 0);
+  }
+  produto(p, d, NORMA0, d.r, d.r, nullptr, 0, tol, bolhas, s);
+  precondicionar(p, d, bolhas, s);
+  k_copiar_pz<<<nbx, 256, 0, s>>>(d);
+  produto(p, d, RZ0, d.r, d.z, nullptr, 0, tol, bolhas, s);
+  int it = 0;
+  for (; it < iteracoes; it++) {
+    k_aplicar<<<nb, 256, 0, s>>>(d, p->vizOp, bolhas ? 1 : 0);
+    if (bolhas) {
+      cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
+      k_bolhas_somar_v<<<nb, 256, 0, s>>>(d, d.p);
+      k_bolhas_linhas<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d, 1);
+    }
+    produto(p, d, PAP, d.p, d.ap, nullptr, it, tol, bolhas, s);
+    k_atualizar<<<nbx, 256, 0, s>>>(d);
+    produto(p, d, NORMA, d.r, d.r, nullptr, it, tol, bolhas, s);
+    if (it == iteracoes - 1) break;
+    if (tol > 0) {
+      int pronto = 0;
+      if (cudaMemcpyAsync(&pronto, &d.esc->pronto, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        return TQ_E_CUDA;
+      if (pronto) break;
+    }
+    k_guardar_z<<<nbx, 256, 0, s>>>(d);
+    precondicionar(p, d, bolhas, s);
+    produto(p, d, BETA, d.r, d.z, d.zOld, it, tol, bolhas, s);
+    k_direcao<<<nbx, 256, 0, s>>>(d);
+  }
+  k_pcg_fim<<<nbx, 256, 0, s>>>(d, bolhas ? 1 : 0);
+  // residual history for tq_last_norms
+  int iters = 0;
+  if (cudaMemcpyAsync(&iters, &d.esc->iters, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return TQ_E_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return TQ_E_CUDA;
+  p->iters = iters;
+  p->normas.resize(iters + 1);
+  if (cudaMemcpyAsync(p->normas.data(), d.esc->normas, sizeof(double) * (iters + 1), cudaMemcpyDeviceToHost, s) !=
+      cudaSuccess)
+    return TQ_E_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return TQ_E_CUDA;
+  return cudaGetLastError() == cudaSuccess ? TQ_OK : TQ_E_CUDA;
+}
+
+int normasPcg(Pcg* p, double* out, int cap) {
+  int n = (int)p->normas.size();
+  for (int k = 0; k < n && k < cap; k++) out[k] = p->normas[k];
+  return n;
+}
+int itersPcg(Pcg* p) { return p->iters; }
+
+// One V-cycle on caller-provided device buffers (tq_vcycle).
+template <class T>
+__global__ void k_carregar_b(NivelDev<T> n0, const float* b) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n0.nx * n0.ny) return;
+  n0.b[c] = guardar<T>(b[c]);
+  n0.x[c] = guardar<T>(0.0f);
+}
+template <class T>
+__global__ void k_descarregar_x(NivelDev<T> n0, float* x) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n0.nx * n0.ny) return;
+  x[c] = carregar(n0.x[c]);
+}
+int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cudaStream_t s) {
+  prepararNiveis(p, tipo, s);
+  int nb = blocos(p->N, 256);
+  comTipo(p, 0, [&](auto* tag) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    k_carregar_b<T><<<nb, 256, 0, s>>>(nivel<T>(p, 0), b);
+  });
+  cicloV(p, s);
+  comTipo(p, 0, [&](auto* tag) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    k_descarregar_x<T><<<nb, 256, 0, s>>>(nivel<T>(p, 0), x);
+  });
+  return cudaGetLastError() == cudaSuccess ? TQ_OK : TQ_E_CUDA;
+}
+
+}  // namespace tq

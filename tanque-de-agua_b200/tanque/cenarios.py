@@ -1,0 +1,259 @@
+"""Scene builders: seeded particle seeding and the wall/water layouts of the workloads.
+
+`semente` is the seeded LCG of testes/apoio.js:4-9 and `semear_retangulo` the 2x2-jittered
+seeding of js/fisica-cpu.js:705-727, both producing the reference's exact floats.  The preset
+scenes (copo, vasos, ampulheta, labirinto, ...) follow js/modelos.js; they are the scenes the
+reference's tests run and the synthetic benchmark scenes are built from.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .constantes import CAMPOS, MOLDURA, PARTICULAS_POR_CELULA
+
+
+def semente(s: int = 1):
+    """testes/apoio.js:4-9: s = (s*1664525 + 1013904223) mod 2^32, returns s / 2^32."""
+    estado = [s & 0xFFFFFFFF]
+
+    def aleatorio() -> float:
+        estado[0] = (estado[0] * 1664525 + 1013904223) & 0xFFFFFFFF
+        return estado[0] / 4294967296
+    return aleatorio
+
+
+def semear_retangulo(x0, y0, x1, y1, h, absorcao=(0.0, 0.0, 0.0), aleatorio=None) -> np.ndarray:
+    """semearRetangulo (js/fisica-cpu.js:705-727): 2x2 jittered particles per cell."""
+    if aleatorio is None:
+        aleatorio = semente(1)
+    lado = round(math.sqrt(PARTICULAS_POR_CELULA))
+    passo = h / lado
+    xa, xb = min(x0, x1), max(x0, x1)
+    ya, yb = min(y0, y1), max(y0, y1)
+    ia, ib = math.ceil(xa / passo - 0.5), math.floor(xb / passo - 0.5)
+    ja, jb = math.ceil(ya / passo - 0.5), math.floor(yb / passo - 0.5)
+    n = max(0, ib - ia + 1) * max(0, jb - ja + 1)
+    lista = np.zeros(n * CAMPOS, dtype=np.float32)
+    k = 0
+    for j in range(ja, jb + 1):
+        for i in range(ia, ib + 1):
+            o = k * CAMPOS
+            lista[o] = (i + 0.5 + (aleatorio() - 0.5) * 0.5) * passo
+            lista[o + 1] = (j + 0.5 + (aleatorio() - 0.5) * 0.5) * passo
+            lista[o + 9], lista[o + 10], lista[o + 11] = absorcao
+            k += 1
+    return lista
+
+
+def semear_retangulo_rapido(x0, y0, x1, y1, h, absorcao=(0.0, 0.0, 0.0), s: int = 1) -> np.ndarray:
+    """semear_retangulo vectorised for large blocks (same LCG stream, same floats)."""
+    lado = round(math.sqrt(PARTICULAS_POR_CELULA))
+    passo = h / lado
+    xa, xb = min(x0, x1), max(x0, x1)
+    ya, yb = min(y0, y1), max(y0, y1)
+    ia, ib = math.ceil(xa / passo - 0.5), math.floor(xb / passo - 0.5)
+    ja, jb = math.ceil(ya / passo - 0.5), math.floor(yb / passo - 0.5)
+    ni, nj = max(0, ib - ia + 1), max(0, jb - ja + 1)
+    n = ni * nj
+    # the LCG stream: 2n draws, computed with 64-bit integers
+    r = _fluxo_lcg(s, 2 * n)
+    jj, ii = np.divmod(np.arange(n, dtype=np.int64), ni) if ni else (np.zeros(0, np.int64), np.zeros(0, np.int64))
+    i = ii + ia
+    j = jj + ja
+    lista = np.zeros((n, CAMPOS), dtype=np.float32)
+    lista[:, 0] = ((i + 0.5 + (r[0::2] - 0.5) * 0.5) * passo).astype(np.float32)
+    lista[:, 1] = ((j + 0.5 + (r[1::2] - 0.5) * 0.5) * passo).astype(np.float32)
+    lista[:, 9:12] = np.asarray(absorcao, dtype=np.float32)
+    return lista.ravel()
+
+
+def _fluxo_lcg(s: int, n: int) -> np.ndarray:
+    """n successive draws of semente(s) as float64 (vectorised by blocks of LCG jumps)."""
+    out = np.empty(n, dtype=np.float64)
+    if n == 0:
+        return out
+    a, c, m = 1664525, 1013904223, 1 << 32
+    bloco = min(n, 4096)
+    # coefficients of x_{k} = A_k x_0 + C_k for k = 1..bloco
+    A = np.empty(bloco, dtype=np.uint64)
+    Cc = np.empty(bloco, dtype=np.uint64)
+    ak, ck = 1, 0
+    for k in range(bloco):
+        ak = (ak * a) % m
+        ck = (ck * a + c) % m
+        A[k], Cc[k] = ak, ck
+    x = s & 0xFFFFFFFF
+    feito = 0
+    while feito < n:
+        t = min(bloco, n - feito)
+        v = (A[:t] * np.uint64(x) + Cc[:t]) & np.uint64(0xFFFFFFFF)
+        out[feito:feito + t] = v.astype(np.float64) / 4294967296
+        x = int(v[t - 1])
+        feito += t
+    return out
+
+
+def dentro_do_poligono(x, y, pts) -> bool:
+    """dentroDoPoligono (js/modelos.js:216-223), even-odd rule."""
+    dentro = False
+    j = len(pts) - 1
+    for i in range(len(pts)):
+        xi, yi = pts[i]
+        xj, yj = pts[j]
+        if (yi > y) != (yj > y) and x < ((xj - xi) * (y - yi)) / (yj - yi) + xi:
+            dentro = not dentro
+        j = i
+    return dentro
+
+
+def semear_agua(entrada: dict, h: float, absorcao=(0.0, 0.0, 0.0), aleatorio=None) -> np.ndarray:
+    """semearAgua (js/modelos.js:229-242): rectangle, or polygon clipped at limiteY."""
+    if "poligono" not in entrada:
+        return semear_retangulo(entrada["x0"], entrada["y0"], entrada["x1"], entrada["y1"], h, absorcao, aleatorio)
+    pts = entrada["poligono"]
+    xs = [q[0] for q in pts]
+    ys = [q[1] for q in pts]
+    topo = min(max(ys), entrada.get("limiteY", math.inf))
+    bruto = semear_retangulo(min(xs), min(ys), max(xs), topo, h, absorcao, aleatorio).reshape(-1, CAMPOS)
+    keep = [k for k in range(len(bruto)) if dentro_do_poligono(float(bruto[k, 0]), float(bruto[k, 1]), pts)]
+    return bruto[keep].ravel()
+
+
+# ------------------------------------------------------------------ preset scenes (js/modelos.js)
+def raio_de_parede(h: float) -> float:
+    return max(1.6 * h, 0.006)
+
+
+def _linha(pts, raio, fechar=False):
+    n = len(pts) if fechar else len(pts) - 1
+    return [dict(x0=pts[k][0], y0=pts[k][1], x1=pts[(k + 1) % len(pts)][0], y1=pts[(k + 1) % len(pts)][1], raio=raio)
+            for k in range(n)]
+
+
+def _palco(W, H, h):
+    m = MOLDURA * h
+    largura = min(W - 2 * m, 1.7 * H)
+    return dict(x0=(W - largura) / 2, largura=largura, chao=m, teto=H - m, altura=H - 2 * m,
+                X=lambda f: (W - largura) / 2 + f * largura, Y=lambda f: m + f * (H - 2 * m))
+
+
+def modelo_copo(W, H, h):
+    p, r = _palco(W, H, h), raio_de_parede(h)
+    cx = W / 2
+    meia = min(p["largura"] * 0.14, p["altura"] * 0.2)
+    base = p["chao"] + r
+    topo = p["Y"](0.46)
+    return dict(tracos=_linha([[cx - meia * 1.18, topo], [cx - meia, base], [cx + meia, base], [cx + meia * 1.18, topo]], r),
+                agua=[dict(x0=cx - meia * 0.75, y0=p["Y"](0.66), x1=cx + meia * 0.75, y1=p["Y"](0.97))])
+
+
+def modelo_ampulheta(W, H, h):
+    p, r = _palco(W, H, h), raio_de_parede(h)
+    cx = W / 2
+    meia = min(p["largura"] * 0.2, p["altura"] * 0.3)
+    pescoco = r + 1.8 * h
+    topo, meio, base = p["Y"](0.94), p["Y"](0.5), p["Y"](0.06)
+    contorno = [
+        [cx - meia, topo], [cx + meia, topo], [cx + meia, topo - (topo - meio) * 0.25],
+        [cx + pescoco, meio],
+        [cx + meia, base + (meio - base) * 0.25], [cx + meia, base], [cx - meia, base],
+        [cx - meia, base + (meio - base) * 0.25], [cx - pescoco, meio],
+        [cx - meia, topo - (topo - meio) * 0.25],
+    ]
+    folga = r + h
+    dentro = [
+        [cx - meia + folga, topo - folga], [cx + meia - folga, topo - folga],
+        [cx + meia - folga, topo - (topo - meio) * 0.25],
+        [cx + pescoco * 0.3, meio + (topo - meio) * 0.12],
+        [cx - pescoco * 0.3, meio + (topo - meio) * 0.12],
+        [cx - meia + folga, topo - (topo - meio) * 0.25],
+    ]
+    return dict(tracos=_linha(contorno, r, True), agua=[dict(poligono=dentro, limiteY=meio + (topo - meio) * 0.72)])
+
+
+def modelo_vasos(W, H, h):
+    p, r = _palco(W, H, h), raio_de_parede(h)
+    xa, xb = p["X"](0.18), p["X"](0.82)
+    topo = p["Y"](0.82)
+    vao = p["Y"](0.1)
+    d1, d2 = xa + (xb - xa) * 0.3, xa + (xb - xa) * 0.52
+    tracos = (_linha([[xa, topo], [xa, p["chao"]]], r) + _linha([[xb, topo], [xb, p["chao"]]], r)
+              + _linha([[d1, topo], [d1, vao]], r) + _linha([[d2, topo], [d2 + (xb - d2) * 0.18, vao]], r))
+    return dict(tracos=tracos, agua=[dict(x0=xa, y0=p["Y"](0.02), x1=d1, y1=p["Y"](0.62))])
+
+
+def labirinto(W, H, h, aleatorio, linhas=6, corredor=None, raio=None, x0=None, y0=None, colunas=None):
+    """Recursive-backtracker labyrinth of js/modelos.js:133-185.  With `corredor`/`raio` the
+    cell pitch and wall radius are given in metres (the benchmark's 8-cell corridors and
+    4-cell walls) instead of being fitted to the stage."""
+    p = _palco(W, H, h)
+    r = raio if raio is not None else raio_de_parede(h)
+    if corredor is None:
+        altura = p["altura"] * 0.78
+        tam = altura / linhas
+        colunas = max(3, min(10, math.floor((p["largura"] * 0.9) / tam)))
+    else:
+        tam = corredor
+    largura = colunas * tam
+    bx0 = W / 2 - largura / 2 if x0 is None else x0
+    by0 = p["chao"] + p["altura"] * 0.03 if y0 is None else y0
+    dir_ = [[True] * linhas for _ in range(colunas)]
+    baixo = [[True] * linhas for _ in range(colunas)]
+    visto = [[False] * linhas for _ in range(colunas)]
+    pilha = [(0, linhas - 1)]
+    visto[0][linhas - 1] = True
+    while pilha:
+        c, l = pilha[-1]
+        viz = [(a, b) for (a, b) in [(c + 1, l), (c - 1, l), (c, l + 1), (c, l - 1)]
+               if 0 <= a < colunas and 0 <= b < linhas and not visto[a][b]]
+        if not viz:
+            pilha.pop()
+            continue
+        a, b = viz[math.floor(aleatorio() * len(viz))]
+        if a == c + 1:
+            dir_[c][l] = False
+        elif a == c - 1:
+            dir_[a][l] = False
+        elif b == l + 1:
+            baixo[c][b] = False
+        else:
+            baixo[c][l] = False
+        visto[a][b] = True
+        pilha.append((a, b))
+    X = lambda c: bx0 + c * tam  # noqa: E731
+    Y = lambda l: by0 + l * tam  # noqa: E731
+    tracos = []
+
+    def seg(xa, ya, xb, yb):
+        tracos.append(dict(x0=xa, y0=ya, x1=xb, y1=yb, raio=r))
+    for c in range(colunas):
+        for l in range(linhas):
+            if dir_[c][l] and c < colunas - 1:
+                seg(X(c + 1), Y(l), X(c + 1), Y(l + 1))
+            if baixo[c][l] and l > 0:
+                seg(X(c), Y(l), X(c + 1), Y(l))
+    seg(X(0), Y(0), X(0), Y(linhas))
+    seg(X(colunas), Y(0), X(colunas), Y(linhas))
+    seg(X(1), Y(linhas), X(colunas), Y(linhas))
+    seg(X(0), Y(0), X(colunas - 1), Y(0))
+    folga = r + h
+    return dict(tracos=tracos, agua=[dict(x0=X(0) + folga, y0=Y(linhas) + p["altura"] * 0.04, x1=X(1) - folga,
+                                          y1=p["teto"] - 2 * h)], X=X, Y=Y, tam=tam, colunas=colunas)
+
+
+MODELOS = {"copo": modelo_copo, "ampulheta": modelo_ampulheta, "vasos": modelo_vasos}
+
+
+def montar_modelo(nome, nx, ny, h, aleatorio, Cena, fabrica):
+    """montarModelo of testes/fisica.test.js:18-26 with a simulation factory."""
+    cena = Cena(nx, ny, h)
+    m = MODELOS[nome](cena.largura, cena.altura, h)
+    for t in m["tracos"]:
+        cena.tracar(t["x0"], t["y0"], t["x1"], t["y1"], t["raio"])
+    cena.atualizar()
+    sim = fabrica(cena)
+    for a in m["agua"]:
+        sim.adicionar(semear_agua(a, h, (0.0, 0.0, 0.0), aleatorio), False)
+    return cena, sim, m

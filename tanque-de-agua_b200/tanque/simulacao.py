@@ -1,0 +1,270 @@
+"""SimulacaoGPU: the reference's `SimulacaoCPU` surface (js/fisica-cpu.js:28-671) over the C-ABI.
+
+Method and field names are the JavaScript ones, so code written against SimulacaoCPU (the
+reference's tests, MotorCPU) reads the same here.  Fields are copied out of the device on
+access; the handle owns the device state.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .constantes import CAMPOS, ITERACOES_PCG, MAX_BOLHAS, PARTICULAS_POR_CELULA, TAU_DENSIDADE, TENSAO_SUPERFICIAL
+
+_FERRAMENTAS = {"nenhuma": 0, "esponja": 1, "mao": 2, "corante": 3}
+
+
+class Simulacao:
+    """Drives any library exporting the tq_* entry points (or a prefixed mirror of them)."""
+
+    _DTYPES = {
+        "tipo": np.uint8, "solidoCelula": np.uint8, "vivo": np.uint8, "uValida": np.uint8, "vValida": np.uint8,
+        "rotulo": np.uint32, "contagemCelula": np.uint32, "accU": np.int32, "accV": np.int32, "accCel": np.int32,
+        "accCor": np.int32,
+    }
+
+    def __init__(self, ligacao: _abi.Ligacao, cena, opcoes: dict | None = None, criar: str = "create"):
+        opcoes = dict(opcoes or {})
+        self._lig = ligacao
+        self.cena = cena
+        self.nx, self.ny, self.h = cena.nx, cena.ny, cena.h
+        self.nu = (self.nx + 1) * self.ny
+        self.nv = self.nx * (self.ny + 1)
+        g = opcoes.pop("gravidade", None)
+        tensao = opcoes.pop("tensao", None)
+        o = _abi.opcoes_padrao(
+            self.nx, self.ny, self.h,
+            iterations=opcoes.pop("iteracoes", ITERACOES_PCG),
+            air=1 if opcoes.pop("ar", True) else 0,
+            tau_density=opcoes.pop("tauDensidade", TAU_DENSIDADE),
+            surface_tension=TENSAO_SUPERFICIAL if tensao is None else tensao,
+        )
+        if g is not None:
+            o.gravity[0], o.gravity[1] = g
+        for k, v in opcoes.items():  # tq_options field names (tolerance, precision, engine, ...)
+            if k == "gravity":
+                o.gravity[0], o.gravity[1] = v
+            else:
+                setattr(o, k, v)
+        self.opcoes = o
+        self.arAtivo = bool(o.air)
+        h = C.c_void_p()
+        self._lig(criar, C.byref(o), C.byref(h))
+        self._h = h
+        self.atualizarParedes()
+
+    # ---------------------------------------------------------------- lifecycle
+    def fechar(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lig("destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.fechar()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.fechar()
+
+    # ---------------------------------------------------------------- SimulacaoCPU surface
+    @property
+    def gravidade(self):
+        return (self.opcoes.gravity[0], self.opcoes.gravity[1])
+
+    def atualizarParedes(self):
+        """atualizarParedes (js/fisica-cpu.js:80-85) after Cena edits: upload the SDF."""
+        sdf = np.ascontiguousarray(self.cena.sdf, dtype=np.float32)
+        self._lig("set_walls", self._h, sdf.ctypes.data, self.cena.mw, self.cena.mh)
+
+    def adicionar(self, lista, checarCheia: bool = True) -> int:
+        """adicionar (js/fisica-cpu.js:92-111); returns the number of particles kept."""
+        a = np.ascontiguousarray(lista, dtype=np.float32).ravel()
+        n = a.size // CAMPOS
+        aceitas = C.c_int32(0)
+        self._lig("add_particles", self._h, a.ctypes.data, n, 1 if checarCheia else 0, C.byref(aceitas))
+        return aceitas.value
+
+    def aplicarFerramenta(self, f: dict | None):
+        """aplicarFerramenta (js/fisica-cpu.js:129-152)."""
+        if not f or f.get("tipo", "nenhuma") == "nenhuma":
+            return
+        t = _abi.TqTool()
+        t.kind = _FERRAMENTAS[f["tipo"]]
+        t.x, t.y, t.radius = f["x"], f["y"], f["raio"]
+        t.vx, t.vy = f.get("vx", 0.0), f.get("vy", 0.0)
+        ab = f.get("absorcao", (0.0, 0.0, 0.0))
+        t.absorb[0], t.absorb[1], t.absorb[2] = ab
+        self._lig("apply_tool", self._h, C.byref(t))
+
+    def avancar(self, dt: float, subpassos: int = 1):
+        """avancar (js/fisica-cpu.js:155-159)."""
+        self._lig("advance", self._h, float(dt), int(subpassos))
+        self._andou = True
+
+    def atualizarAr(self):
+        self._lig("update_air", self._h)
+
+    def reiniciarAr(self):
+        self._lig("reset_air", self._h)
+
+    def subpasso(self, dt: float):
+        self._lig("substep", self._h, float(dt))
+        self._andou = True
+
+    def area(self) -> float:
+        """area (js/fisica-cpu.js:192-194): water area in m^2 from the particle count."""
+        return (self.n / PARTICULAS_POR_CELULA) * self.h * self.h
+
+    def limparAgua(self):
+        """MotorCPU.limparAgua (js/motor.js:95)."""
+        self._lig("clear_particles", self._h)
+        self.reiniciarAr()
+
+    @property
+    def n(self) -> int:
+        v = C.c_int32(0)
+        self._lig("count", self._h, C.byref(v))
+        return v.value
+
+    @n.setter
+    def n(self, valor: int):
+        # The reference's tests empty the tank with `sim.n = 0` (testes/fisica.test.js:235).
+        if valor != 0:
+            raise ValueError("only sim.n = 0 is supported; use definirParticulas")
+        self._lig("clear_particles", self._h)
+
+    @property
+    def p(self) -> np.ndarray:
+        """sim.p.subarray(0, n*CAMPOS) in the reference's particle order."""
+        n = self.n
+        out = np.empty(n * CAMPOS, dtype=np.float32)
+        m = C.c_int32(0)
+        self._lig("get_particles", self._h, out.ctypes.data if n else None, n, C.byref(m))
+        return out[: m.value * CAMPOS]
+
+    def definirParticulas(self, lista):
+        a = np.ascontiguousarray(lista, dtype=np.float32).ravel()
+        self._lig("set_particles", self._h, a.ctypes.data if a.size else None, a.size // CAMPOS)
+
+    def _tamanho(self, nome: str) -> int:
+        N = self.nx * self.ny
+        tam = {
+            "u": self.nu, "v": self.nv, "uValida": self.nu, "vValida": self.nv, "uPeso": self.nu, "vPeso": self.nv,
+            "pressaoBolha": MAX_BOLHAS, "volumeAlvo": MAX_BOLHAS, "volumeBolha": MAX_BOLHAS, "rhsBolha": MAX_BOLHAS,
+            "yBolha": MAX_BOLHAS, "vivo": MAX_BOLHAS, "corCelula": 3 * N, "accCor": 3 * N, "accU": 2 * self.nu,
+            "accV": 2 * self.nv, "accCel": 2 * N, "sdf": 4 * N,
+        }
+        return tam.get(nome, N)
+
+    def campo(self, nome: str) -> np.ndarray:
+        """Copy of a state field (names of include/tanque.h's tq_field, as in the JavaScript)."""
+        dt = self._DTYPES.get(nome, np.float32)
+        out = np.empty(self._tamanho(nome), dtype=dt)
+        self._lig("get_field", self._h, _abi.CAMPOS_ENUM[nome], out.ctypes.data, out.nbytes)
+        return out
+
+    def definirCampo(self, nome: str, valores):
+        dt = self._DTYPES.get(nome, np.float32)
+        a = np.ascontiguousarray(valores, dtype=dt).ravel()
+        self._lig("set_field", self._h, _abi.CAMPOS_ENUM[nome], a.ctypes.data, a.nbytes)
+
+    def escalar(self, qual: int) -> float:
+        v = C.c_double(0)
+        self._lig("get_scalar", self._h, qual, C.byref(v))
+        return v.value
+
+    def definirEscalar(self, qual: int, valor: float):
+        self._lig("set_scalar", self._h, qual, float(valor))
+
+    def normas(self) -> np.ndarray:
+        n = C.c_int32(0)
+        buf = (C.c_double * 1024)()
+        self._lig("last_norms", self._h, buf, 1024, C.byref(n))
+        return np.array(buf[: n.value])
+
+    @property
+    def vMax(self):
+        """Largest particle speed of the last G2P; None before the first substep (the
+        reference's field is undefined until then, js/fisica-cpu.js:637)."""
+        if not getattr(self, "_andou", False):
+            return None
+        return self.escalar(_abi.TQ_SCALAR_VMAX)
+
+    # typed-array fields the reference's tests and facade read (testes/fisica.test.js, js/motor.js)
+    tipo = property(lambda self: self.campo("tipo"))
+    rotulo = property(lambda self: self.campo("rotulo"))
+    contagemCelula = property(lambda self: self.campo("contagemCelula"))
+    solidoCelula = property(lambda self: self.campo("solidoCelula"))
+    q = property(lambda self: self.campo("q"))
+    u = property(lambda self: self.campo("u"))
+    v = property(lambda self: self.campo("v"))
+    pressaoBolha = property(lambda self: self.campo("pressaoBolha"))
+
+
+class SimulacaoGPU(Simulacao):
+    """`new SimulacaoCPU(cena, opcoes)` on the B200 (libtanque.so)."""
+
+    def __init__(self, cena, opcoes: dict | None = None):
+        super().__init__(_abi.carregar(), cena, opcoes)
+
+    def sincronizar(self):
+        self._lig("sync", self._h)
+
+    def tempos(self, ligar: bool | None = None):
+        """Per-stage device times (ms) of the last substep; `ligar` switches timing on/off."""
+        if ligar is not None:
+            self._lig("set_timing", self._h, 1 if ligar else 0)
+            return None
+        n = C.c_int32(0)
+        buf = (C.c_double * 16)()
+        self._lig("get_timing", self._h, buf, 16, C.byref(n))
+        return list(buf[: n.value])
+
+
+def resolver_pressao(tipo, div, q, iteracoes=ITERACOES_PCG, tolerancia=0.0, bolhas=None, precisao=0, motor=0,
+                     ligacao: _abi.Ligacao | None = None):
+    """resolverPCG (js/pressao-cpu.js:296-402) through tq_solve_pressure; q is updated in place.
+
+    bolhas: optional dict(rotulo=uint32[N], rhs=float32[4096], y=float32[4096]); y is updated.
+    Returns the residual-norm history."""
+    lig = ligacao or _abi.carregar()
+    ny, nx = tipo.shape
+    tipo = np.ascontiguousarray(tipo, dtype=np.uint8)
+    div = np.ascontiguousarray(div, dtype=np.float32)
+    assert q.dtype == np.float32 and q.flags.c_contiguous
+    b = None
+    if bolhas is not None:
+        b = _abi.TqBubbles()
+        b.rotulo = bolhas["rotulo"].ctypes.data
+        b.rhs = bolhas["rhs"].ctypes.data
+        b.y = bolhas["y"].ctypes.data
+    normas = (C.c_double * 1024)()
+    nn = C.c_int32(0)
+    args = [nx, ny, tipo.ctypes.data, div.ctypes.data, q.ctypes.data, iteracoes, tolerancia,
+            C.byref(b) if b is not None else None]
+    if lig.prefixo == "tq_":
+        args += [precisao, motor]
+    args += [normas, 1024, C.byref(nn)]
+    lig("solve_pressure", *args)
+    return np.array(normas[: nn.value])
+
+
+def ciclo_v(tipo, b, precisao=0, ligacao: _abi.Ligacao | None = None) -> np.ndarray:
+    """cicloV (js/pressao-cpu.js:241-255) through tq_vcycle: one V-cycle from x = 0."""
+    lig = ligacao or _abi.carregar()
+    ny, nx = tipo.shape
+    tipo = np.ascontiguousarray(tipo, dtype=np.uint8)
+    b = np.ascontiguousarray(b, dtype=np.float32)
+    x = np.zeros_like(b)
+    args = [nx, ny, tipo.ctypes.data, b.ctypes.data, x.ctypes.data]
+    if lig.prefixo == "tq_":
+        args.append(precisao)
+    lig("vcycle", *args)
+    return x
