@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Throughput of the tank's simulation step on the 450k-cell ultra scene (B200).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 840x536 MAC grid, h = 1.6 mm, a seeded labyrinth (8-cell corridors, 4-cell walls)
+in the upper half of the tank, water up to 85 % of the height, a faucet jet 12 cells wide at
+1.2 m/s at the labyrinth's entrance, surface tension 0.0728 N/m, air pockets tracked.  A bench
+step is one simulated 1/60 s frame: one air relabel and 14 substeps of 1/840 s (below the
+capillary limit of 1.197 ms at this h).  Every pressure solve runs to ||r|| <= 1e-6 ||r0||.
+The metric is substeps per second.
+
+`value` is the mixed-precision configuration (FP16 V-cycle storage) timed on the device with
+inputs resident; `fp32_plain` is the one-launch-per-step FP32 engine on the same frames; `e2e`
+is the mixed configuration through the C-ABI with host buffers (faucet particles in, every
+particle out, each frame).  --impl reference times the CPU oracle (the reference engine's
+algorithm restated in C++, single-threaded as the reference is) on the same scene.
+With --gpus N > 1 (torchrun) each rank advances its own replica (a tank does not shard).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+RAIZ = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(RAIZ, "tanque-de-agua_b200"),):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "steps/s @450k cells & MGPCG HBM GB/s: mixed vs FP32 plain at 1e-6 residual"
+NX, NY, H = 840, 536, 0.0016
+SUB = 14
+DT_QUADRO = 1 / 60
+TOL = 1e-6
+MAX_ITER = 200
+# Algorithmic HBM bytes of one PCG iteration per fine cell (5-point operator, V-cycle with
+# 4 smoother passes per level, restriction and prolongation, dots and vector updates) for
+# FP32 V-cycle storage and for 16-bit storage, plus the setup of a solve (initial residual,
+# first V-cycle).
+BYTES_ITER = {"fp32": 156.0, "fp16": 120.0, "bf16": 120.0}
+BYTES_SETUP = {"fp32": 110.0, "fp16": 85.0, "bf16": 85.0}
+
+
+def picos():
+    try:
+        with open(os.path.join(RAIZ, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ scene
+def construir_cena(Cena, semente, labirinto, semear):
+    """Walls and water of the ultra scene; returns (cena, traces, particles, faucet)."""
+    cena = Cena(NX, NY, H)
+    W, Hh = cena.largura, cena.altura
+    tam = 12 * H
+    colunas, linhas = 56, 22
+    x0 = (W - colunas * tam) / 2
+    y0 = 0.40 * Hh
+    lab = labirinto(W, Hh, H, semente(3), linhas=linhas, corredor=tam, raio=2 * H, x0=x0, y0=y0, colunas=colunas)
+    for t in lab["tracos"]:
+        cena.tracar(t["x0"], t["y0"], t["x1"], t["y1"], t["raio"])
+    m = 2 * H
+    agua = semear(m, m, W - m, 0.85 * Hh, H, (0.0, 0.0, 0.0), s=3)
+    torneira = dict(x=lab["X"](0) + tam / 2, y=lab["Y"](linhas) + 10 * H, raio=6 * H, vx=0.0, vy=-1.2)
+    return cena, lab["tracos"], agua, torneira
+
+
+def jato(torneira, quadro, dt=DT_QUADRO):
+    """emitirTorneira (js/principal.js:301-321) with a seeded LCG in place of Math.random:
+    particles in a disk of the jet's radius, at the jet velocity."""
+    from tanque.cenarios import semente
+    r0 = torneira["raio"]
+    vx, vy = torneira["vx"], torneira["vy"]
+    vazao = 2 * r0 * max(0.7, math.hypot(vx, vy))
+    n = min(40000, round((vazao * dt) / (H * H) * 4))
+    al = semente(1000 + quadro)
+    lista = np.zeros((n, 12), dtype=np.float32)
+    for k in range(n):
+        a = al() * math.pi * 2
+        r = math.sqrt(al()) * r0
+        lista[k, 0] = torneira["x"] + math.cos(a) * r
+        lista[k, 1] = torneira["y"] + math.sin(a) * r
+        lista[k, 2] = vx
+        lista[k, 3] = vy
+    return lista.ravel()
+
+
+# ------------------------------------------------------------------ clocks
+class Relogios:
+    """nvidia-smi sampling during the timed region (clocks and throttle reasons)."""
+
+    CAMPOS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, indice):
+        self.indice = indice
+        self.proc = None
+        self.saida = None
+
+    def __enter__(self):
+        try:
+            self.saida = open(os.devnull if False else f"/tmp/tq_clocks_{os.getpid()}.csv", "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.indice}", f"--query-gpu={self.CAMPOS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.saida, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.saida:
+            self.saida.close()
+
+    def resumo(self):
+        try:
+            linhas = [l.split(",") for l in open(self.saida.name).read().strip().splitlines() if l.strip()]
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(l[1]) for l in linhas if len(l) >= 9]
+        mx = [float(l[2]) for l in linhas if len(l) >= 9]
+        razoes = set()
+        nomes = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in linhas:
+            if len(l) < 9:
+                continue
+            for nome, v in zip(nomes, l[5:9]):
+                if v.strip().lower() == "active":
+                    razoes.add(nome)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sob_carga = [v for v in sm if v > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(sob_carga), "sm_max_mhz": max(mx), "reasons": sorted(razoes),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU oracle
+def medir_oraculo(passos, aquecimento, orcamento_s=None):
+    """Substeps/s of the CPU oracle (reference CPU semantics: float P2G sums) on the scene."""
+    sys.path.insert(0, os.path.join(RAIZ, "tests"))
+    from oraculo import CenaOraculo, SimulacaoOraculo
+    from tanque import _abi
+    from tanque.cenarios import labirinto, semear_retangulo_rapido, semente
+    cena, _, agua, _ = construir_cena(CenaOraculo, semente, labirinto, semear_retangulo_rapido)
+    sim = SimulacaoOraculo(cena, {"p2g_mode": _abi.TQ_P2G_FLOAT, "tolerance": TOL, "iterations": MAX_ITER})
+    sim.adicionar(agua, False)
+    n_part = sim.n
+    dt = DT_QUADRO / SUB
+    sim.atualizarAr()
+    for _ in range(aquecimento):
+        sim.subpasso(dt)
+    feitos = 0
+    t0 = time.perf_counter()
+    while feitos < passos:
+        sim.subpasso(dt)
+        feitos += 1
+        if orcamento_s is not None and time.perf_counter() - t0 > orcamento_s:
+            break
+    t = time.perf_counter() - t0
+    return feitos / t, feitos, n_part
+
+
+# ------------------------------------------------------------------ GPU arm
+def executar_gpu(args, rank, mundo, dist):
+    import torch
+    from tanque import Cena, SimulacaoGPU, _abi
+    from tanque.cenarios import labirinto, semear_retangulo_rapido, semente
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    cena, _, agua, torneira = construir_cena(Cena, semente, labirinto, semear_retangulo_rapido)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    hbm, origem_pico = picos()
+
+    def nova(precisao, motor):
+        s = SimulacaoGPU(cena, {"tolerance": TOL, "iterations": MAX_ITER, "precision": precisao, "engine": motor,
+                                "device": dev})
+        s.adicionar(agua, False)
+        return s
+
+    def barreira():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def medir(precisao, motor, com_relogio=False):
+        """Device-timed frames with inputs resident; returns a dict of results."""
+        s = nova(precisao, motor)
+        ext = torch.cuda.ExternalStream(s.stream())
+        for q in range(args.warmup):
+            s.avancar(DT_QUADRO, SUB)
+        s.sincronizar()
+        barreira()
+        s.tempos(True)
+        l0 = SimulacaoGPU.lancamentos()
+        eventos = []
+        rel = Relogios(dev) if com_relogio else None
+        if rel:
+            rel.__enter__()
+        for q in range(args.steps):
+            with torch.cuda.stream(ext):
+                flush.zero_()  # L2 flush between timed steps (outside the events)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(ext)
+            s.avancar(DT_QUADRO, SUB)
+            e1.record(ext)
+            eventos.append((e0, e1))
+        s.sincronizar()
+        torch.cuda.synchronize()
+        if rel:
+            rel.__exit__()
+        lanc = SimulacaoGPU.lancamentos() - l0
+        ms = sum(a.elapsed_time(b) for a, b in eventos)
+        et = s.tempos()
+        n_part = s.n
+        s.fechar()
+        return dict(ms=ms, etapas=et, lancamentos=lanc, particulas=n_part, relogios=rel.resumo() if rel else None)
+
+    def medir_e2e(precisao, motor):
+        s = nova(precisao, motor)
+        ext = torch.cuda.ExternalStream(s.stream())
+        cap = s.opcoes.capacity or math.ceil(NX * NY * 4.6)
+        saida = torch.empty(cap * 12, dtype=torch.float32, pin_memory=True).numpy()
+        entradas = []
+        for q in range(args.warmup + args.steps):
+            j = jato(torneira, q)
+            buf = torch.empty(j.size, dtype=torch.float32, pin_memory=True).numpy()
+            buf[:] = j
+            entradas.append(buf)
+        h2d = d2h = 0
+        for q in range(args.warmup):
+            s.adicionar(entradas[q], True)
+            s.avancar(DT_QUADRO, SUB)
+        s.sincronizar()
+        barreira()
+        eventos = []
+        import ctypes as C
+        lig = _abi.carregar()
+        for q in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(ext):
+                flush.zero_()
+            e0.record(ext)
+            ent = entradas[args.warmup + q]
+            s.adicionar(ent, True)
+            s.avancar(DT_QUADRO, SUB)
+            n = C.c_int32(0)
+            lig("get_particles", s._h, saida.ctypes.data, cap, C.byref(n))
+            e1.record(ext)
+            eventos.append((e0, e1))
+            h2d += ent.nbytes
+            d2h += n.value * 48
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in eventos)
+        s.fechar()
+        return dict(ms=ms, h2d=h2d / args.steps, d2h=d2h / args.steps)
+
+    precisao_mista = _abi.TQ_PREC_FP16
+    motor_misto = _abi.TQ_ENGINE_FUSED if getattr(args, "fused", True) else _abi.TQ_ENGINE_PLAIN
+    try:
+        misto = medir(precisao_mista, motor_misto, com_relogio=True)
+    except _abi.ErroTanque as e:
+        if e.status != _abi.TQ_E_ARG:
+            raise
+        motor_misto = _abi.TQ_ENGINE_PLAIN
+        misto = medir(precisao_mista, motor_misto, com_relogio=True)
+    plano = medir(_abi.TQ_PREC_FP32, _abi.TQ_ENGINE_PLAIN)
+    e2e = medir_e2e(precisao_mista, motor_misto)
+
+    # max over ranks
+    tempos = np.array([misto["ms"], plano["ms"], e2e["ms"]], dtype=np.float64)
+    if dist is not None:
+        t = torch.tensor(tempos, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tempos = t.cpu().numpy()
+    subpassos_total = mundo * args.steps * SUB
+    valor = subpassos_total / (tempos[0] / 1000)
+    valor_plano = subpassos_total / (tempos[1] / 1000)
+    valor_e2e = subpassos_total / (tempos[2] / 1000)
+
+    def roofline(res, rotulo):
+        et = res["etapas"]
+        n_sub = max(et["subpassos"], 1)
+        iters = et["iteracoes"] / n_sub
+        t_solve = et["pressao"] / n_sub / 1000
+        b = NX * NY * (iters * BYTES_ITER[rotulo] + BYTES_SETUP[rotulo])
+        gbs = b / t_solve / 1e9 if t_solve > 0 else 0.0
+        return dict(iters=iters, ms_solve=t_solve * 1000, gbs=gbs, bytes=b)
+
+    r_m = roofline(misto, "fp16")
+    r_p = roofline(plano, "fp32")
+    if rank != 0:
+        return None
+    linha = {
+        "metric": METRIC,
+        "value": round(valor, 2),
+        "unit": "steps/s",
+        "n_gpus": mundo,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(tempos[0] / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": "ultra scene 840x536 h=1.6mm, labyrinth 8-cell corridors/4-cell walls, faucet 12 cells at 1.2 m/s, "
+                        "sigma=0.0728; one step = 1 relabel + 14 substeps of 1/840 s",
+            "particles": misto["particulas"], "tolerance": TOL, "mixed_precision": "fp16 V-cycle storage",
+            "mixed_engine": "fused" if motor_misto == _abi.TQ_ENGINE_FUSED else "plain",
+            "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{mundo}",
+        },
+        "fp32_plain": {"value": round(valor_plano, 2), "unit": "steps/s", "mgpcg_gbs": round(r_p["gbs"], 1),
+                       "pcg_iters": round(r_p["iters"], 2), "ms_solve": round(r_p["ms_solve"], 4)},
+        "mixed": {"mgpcg_gbs": round(r_m["gbs"], 1), "pcg_iters": round(r_m["iters"], 2),
+                  "ms_solve": round(r_m["ms_solve"], 4), "speedup_vs_fp32_plain": round(valor / valor_plano, 3)},
+        "stages_ms_per_substep": {k: round(misto["etapas"][k] / max(misto["etapas"]["subpassos"], 1), 4)
+                                  for k in SimulacaoGPU.ETAPAS},
+        "roofline": {"kernel": "MGPCG pressure solve", "bound": "hbm", "achieved": round(r_m["gbs"], 1),
+                     "peak": hbm, "peak_source": origem_pico, "unit": "GB/s",
+                     "frac": round(r_m["gbs"] / hbm, 4), "traffic": None,
+                     "bytes_per_launch": round(r_m["bytes"])},
+        "e2e": {"value": round(valor_e2e, 2), "unit": "steps/s", "h2d_bytes_per_step": int(e2e["h2d"]),
+                "d2h_bytes_per_step": int(e2e["d2h"])},
+        "gpu_launches": int(misto["lancamentos"]),
+        "clocks": misto["relogios"],
+    }
+    return linha
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-oracle timing")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", dest="fused", action="store_false", help="mixed config on the plain engine")
+    args = ap.parse_args()
+
+    mundo = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # each step: one substep of the scene on the CPU oracle
+        v, feitos, n_part = medir_oraculo(args.steps, args.warmup)
+        linha = {
+            "metric": METRIC, "impl": "reference", "value": round(v, 4), "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": feitos, "warmup": args.warmup, "ms_per_step": round(1000 / v, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "ultra scene 840x536 h=1.6mm (as ours); one step = one substep of 1/840 s",
+                       "particles": n_part, "tolerance": TOL},
+            "cpu_baseline": {"value": round(v, 4), "unit": "steps/s", "cores": 1, "kind": "port",
+                             "sample": f"{feitos} substeps after {args.warmup} warm-up substeps, CPU oracle "
+                                       "(reference CPU engine restated in C++, single thread)"},
+            "e2e": {"value": round(v, 4), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(linha))
+        return
+
+    dist = None
+    if mundo > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    linha = executar_gpu(args, rank, mundo, dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0 and linha is not None:
+        if mundo == 1 and not args.no_cpu_baseline:
+            v, feitos, n_part = medir_oraculo(10 ** 6, 1, orcamento_s=args.cpu_budget)
+            linha["cpu_baseline"] = {"value": round(v, 4), "unit": "steps/s", "cores": 1, "kind": "port",
+                                     "sample": f"{feitos} substeps of the same scene after 1 warm-up substep "
+                                               "(CPU oracle, single thread)"}
+        print(json.dumps(linha))
+
+
+if __name__ == "__main__":
+    main()

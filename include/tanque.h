@@ -186,7 +186,8 @@ enum tq_scalar {
   TQ_SCALAR_PCG_ITERS = 3,      /* iterations run by the last pressure solve */
   TQ_SCALAR_PCG_RES0 = 4,       /* ||r0|| of the last solve */
   TQ_SCALAR_PCG_RES = 5,        /* final ||r|| of the last solve */
-  TQ_SCALAR_COUNT_ = 6
+  TQ_SCALAR_LAUNCHES = 6,       /* kernels launched by this process so far (all handles) */
+  TQ_SCALAR_COUNT_ = 7
 };
 int tq_get_scalar(tq_sim* s, int32_t which, double* out);
 int tq_set_scalar(tq_sim* s, int32_t which, double value);
@@ -198,9 +199,15 @@ int tq_last_norms(tq_sim* s, double* out, int32_t cap, int32_t* n);
 /* Waits for the handle's stream. */
 int tq_sync(tq_sim* s);
 
-/* Device time (ms, CUDA events on the handle's stream) spent in each stage by the last
- * tq_advance/tq_substep when timing is enabled; stage order: p2g, cells+labels, surface,
- * divergence+bubbles, pressure, gradient+extrapolation, g2p, air relabel. */
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own device work
+ * or timing events with the simulation's. */
+int tq_get_stream(tq_sim* s, void** stream);
+
+/* Stage timing with CUDA events on the handle's stream.  tq_set_timing(1) starts (and resets)
+ * the accumulation; tq_get_timing returns 11 values accumulated since then:
+ * [0..6] ms in p2g+faces, cell flags+labels, surface, divergence+bubbles, pressure solve,
+ * gradient+extrapolation, g2p; [7] ms in air relabels; [8] substeps timed; [9] pressure
+ * iterations in total; [10] relabels timed. */
 int tq_set_timing(tq_sim* s, int32_t enabled);
 int tq_get_timing(tq_sim* s, double* ms_out, int32_t cap, int32_t* n);
 

@@ -92,10 +92,19 @@ __global__ void k_ar_unir(Rastreador r, const uint8_t* tipo) {
   if (j > 0 && tipo[c - r.nx] == AR) ok &= unir(r.pai, c, c - r.nx);
   if (!ok) atomicExch(&r.cont[4], 1);
 }
+// Every cell points straight at its root afterwards.  The walk only reads: a path-halving
+// write here could replace a root some other thread has just stored with a non-root
+// ancestor.  The only writes of this kernel store roots, so concurrent walks stay valid.
 __global__ void k_ar_achatar(Rastreador r) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= r.N || r.pai[c] < 0) return;
-  r.pai[c] = raiz(r.pai, c);
+  int a = c;
+  for (int g = 0; g < LIMITE_UNIAO; g++) {
+    int p = r.pai[a];
+    if (p == a) break;
+    a = p;
+  }
+  r.pai[c] = a;
 }
 
 // Per-cell statistics of js/ar.js:75-95, gathered at the component's root: cells, touches the
@@ -285,14 +294,14 @@ __global__ void k_preencher(unsigned long long* key, unsigned long long* val, in
 static void ordenar(unsigned long long* key, unsigned long long* val, int n, cudaStream_t s) {
   if (n <= 1) return;
   if (n <= 2048) {
-    k_bitonic_local<<<1, 1024, 0, s>>>(key, val, n);
+    lanca(k_bitonic_local, 1, 1024, 0, s, key, val, n);
     return;
   }
   int m = 1;
   while (m < n) m <<= 1;
-  k_preencher<<<blocos(m - n, 256), 256, 0, s>>>(key, val, n, m);
+  lanca(k_preencher, blocos(m - n, 256), 256, 0, s, key, val, n, m);
   for (int kk = 2; kk <= m; kk <<= 1)
-    for (int j = kk >> 1; j > 0; j >>= 1) k_bitonic_passo<<<blocos(m, 256), 256, 0, s>>>(key, val, m, kk, j);
+    for (int j = kk >> 1; j > 0; j >>= 1) lanca(k_bitonic_passo, blocos(m, 256), 256, 0, s, key, val, m, kk, j);
 }
 
 // ---------------------------------------------------------------- canonicalisation
@@ -525,19 +534,19 @@ int atualizarRastreador(Rastreador* r, const Dev& d, cudaStream_t s) {
   cudaMemsetAsync(r->cont, 0, 8 * sizeof(int), s);
   cudaMemsetAsync(r->hk, 0xff, (size_t)r->Hc * 8, s);
   cudaMemsetAsync(r->hcnt, 0, (size_t)r->Hc * 4, s);
-  k_preencher_int<<<blocos(r->Hc, 256), 256, 0, s>>>(r->hfirst, 0x7fffffff, r->Hc);
+  lanca(k_preencher_int, blocos(r->Hc, 256), 256, 0, s, r->hfirst, 0x7fffffff, r->Hc);
   cudaMemsetAsync(r->sob, 0, MAX_BOLHAS * 4, s);
   cudaMemsetAsync(r->vivoNovo, 0, MAX_BOLHAS, s);
   cudaMemsetAsync(r->nasceu, 0, MAX_BOLHAS * 4, s);
-  k_preencher_int<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(r->ganhador, 0x7fffffff, MAX_BOLHAS);
-  k_ar_iniciar<<<nb, 256, 0, s>>>(R, d.tipo);
-  k_ar_unir<<<nb, 256, 0, s>>>(R, d.tipo);
-  k_ar_achatar<<<nb, 256, 0, s>>>(R);
-  k_ar_estatisticas<<<nb, 256, 0, s>>>(R, d.rotulo);
-  k_ar_raizes_contar<<<r->nBlocos, 1024, 0, s>>>(R);
-  k_ar_raizes_scan<<<1, 1024, 0, s>>>(R);
-  k_ar_raizes_gravar<<<r->nBlocos, 1024, 0, s>>>(R);
-  k_ar_pares<<<blocos(r->Hc, 256), 256, 0, s>>>(R);
+  lanca(k_preencher_int, blocos(MAX_BOLHAS, 256), 256, 0, s, r->ganhador, 0x7fffffff, MAX_BOLHAS);
+  lanca(k_ar_iniciar, nb, 256, 0, s, R, d.tipo);
+  lanca(k_ar_unir, nb, 256, 0, s, R, d.tipo);
+  lanca(k_ar_achatar, nb, 256, 0, s, R);
+  lanca(k_ar_estatisticas, nb, 256, 0, s, R, d.rotulo);
+  lanca(k_ar_raizes_contar, r->nBlocos, 1024, 0, s, R);
+  lanca(k_ar_raizes_scan, 1, 1024, 0, s, R);
+  lanca(k_ar_raizes_gravar, r->nBlocos, 1024, 0, s, R);
+  lanca(k_ar_pares, blocos(r->Hc, 256), 256, 0, s, R);
   int h[8];
   if (cudaMemcpyAsync(h, r->cont, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess) return TQ_E_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return TQ_E_CUDA;
@@ -545,10 +554,10 @@ int atualizarRastreador(Rastreador* r, const Dev& d, cudaStream_t s) {
   const int K = h[0], P = h[1];
   ordenar(r->parKey, r->parVal, P, s);
   if (K > 0) {
-    k_ar_gas_scan<<<1, 1024, 0, s>>>(R);
-    k_ar_sobreposicao<<<blocos(P > 0 ? P : 1, 256), 256, 0, s>>>(R);
-    k_ar_alvo<<<blocos(K, 256), 256, 0, s>>>(R, d.volumeAlvo);
-    k_ar_ordem<<<blocos(K, 256), 256, 0, s>>>(R);
+    lanca(k_ar_gas_scan, 1, 1024, 0, s, R);
+    lanca(k_ar_sobreposicao, blocos(P > 0 ? P : 1, 256), 256, 0, s, R);
+    lanca(k_ar_alvo, blocos(K, 256), 256, 0, s, R, d.volumeAlvo);
+    lanca(k_ar_ordem, blocos(K, 256), 256, 0, s, R);
   }
   if (cudaMemcpyAsync(h, r->cont, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess) return TQ_E_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return TQ_E_CUDA;
@@ -556,18 +565,18 @@ int atualizarRastreador(Rastreador* r, const Dev& d, cudaStream_t s) {
   ordenar(r->ordKey, nullptr, M, s);
   int nbM = blocos(M > 0 ? M : 1, 1024);
   if (M > 0) {
-    k_ar_donos_marcar<<<blocos(M, 256), 256, 0, s>>>(R);
-    k_ar_donos_gravar<<<blocos(M, 256), 256, 0, s>>>(R);
+    lanca(k_ar_donos_marcar, blocos(M, 256), 256, 0, s, R);
+    lanca(k_ar_donos_gravar, blocos(M, 256), 256, 0, s, R);
   }
-  k_ar_livres<<<1, 1024, 0, s>>>(R, d.vivo);
+  lanca(k_ar_livres, 1, 1024, 0, s, R, d.vivo);
   if (M > 0) {
-    k_ar_nascer_contar<<<nbM, 1024, 0, s>>>(R);
-    k_ar_nascer_scan<<<1, 1024, 0, s>>>(R, nbM);
-    k_ar_nascer<<<nbM, 1024, 0, s>>>(R, d.pressaoBolha);
+    lanca(k_ar_nascer_contar, nbM, 1024, 0, s, R);
+    lanca(k_ar_nascer_scan, 1, 1024, 0, s, R, nbM);
+    lanca(k_ar_nascer, nbM, 1024, 0, s, R, d.pressaoBolha);
   }
-  k_ar_aplicar_bolhas<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(R, d.pressaoBolha, d.volumeAlvo, d.vivo);
-  if (K > 0) k_ar_volumes<<<blocos(K, 256), 256, 0, s>>>(R, d.volumeAlvo);
-  k_ar_rotular<<<nb, 256, 0, s>>>(R, d.rotulo);
+  lanca(k_ar_aplicar_bolhas, blocos(MAX_BOLHAS, 256), 256, 0, s, R, d.pressaoBolha, d.volumeAlvo, d.vivo);
+  if (K > 0) lanca(k_ar_volumes, blocos(K, 256), 256, 0, s, R, d.volumeAlvo);
+  lanca(k_ar_rotular, nb, 256, 0, s, R, d.rotulo);
   r->primeira = 0;
   return cudaGetLastError() == cudaSuccess ? TQ_OK : TQ_E_CUDA;
 }

@@ -190,4 +190,13 @@ __device__ inline void somaFixa(long long* acc, double v, double escala) {
 
 inline int blocos(long n, int t) { return (int)((n + t - 1) / t); }
 
+// Every kernel launch of the library goes through `lanca`, which counts it (the count is
+// reported by tq_get_scalar(TQ_SCALAR_LAUNCHES)).
+void contarLancamento();
+template <class... P, class... A>
+inline void lanca(void (*k)(P...), dim3 g, dim3 b, size_t sm, cudaStream_t s, A&&... a) {
+  contarLancamento();
+  k<<<g, b, sm, s>>>(static_cast<P>(a)...);
+}
+
 }  // namespace tq

@@ -340,54 +340,54 @@ __global__ void k_extrapolar(Dev d, int volta) {
 }
 
 // ---------------------------------------------------------------- host launchers
-void lancarSolidos(const Dev& d, cudaStream_t s) { k_solidos<<<blocos(d.N, 256), 256, 0, s>>>(d); }
+void lancarSolidos(const Dev& d, cudaStream_t s) { lanca(k_solidos, blocos(d.N, 256), 256, 0, s, d); }
 void lancarTipos(const Dev& d, bool ar, cudaStream_t s) {
-  k_tipos<<<blocos(d.N, 256), 256, 0, s>>>(d, ar ? 1 : 0, 1);
+  lanca(k_tipos, blocos(d.N, 256), 256, 0, s, d, ar ? 1 : 0, 1);
 }
 void lancarPropagarRotulos(const Dev& d, cudaStream_t s) {
   for (int passada = 0; passada < 2; passada++) {
-    k_rotulos_pendentes<<<blocos(d.N, 256), 256, 0, s>>>(d, passada);
-    k_rotulos_resolver<<<1, 1024, 0, s>>>(d);
+    lanca(k_rotulos_pendentes, blocos(d.N, 256), 256, 0, s, d, passada);
+    lanca(k_rotulos_resolver, 1, 1024, 0, s, d);
   }
 }
 void lancarSuperficie(const Dev& d, cudaStream_t s) {
   int nb = blocos(d.N, 256);
   for (int passada = 0; passada <= 2; passada++) {
     for (int camada = 1; camada <= 3; camada++) {
-      k_estender<<<nb, 256, 0, s>>>(d, camada);
-      k_estender_gravar<<<nb, 256, 0, s>>>(d, camada);
+      lanca(k_estender, nb, 256, 0, s, d, camada);
+      lanca(k_estender_gravar, nb, 256, 0, s, d, camada);
     }
     if (passada == 2) break;
-    k_borrar_x<<<nb, 256, 0, s>>>(d);
-    k_borrar_y<<<nb, 256, 0, s>>>(d);
+    lanca(k_borrar_x, nb, 256, 0, s, d);
+    lanca(k_borrar_y, nb, 256, 0, s, d);
   }
-  k_normais<<<nb, 256, 0, s>>>(d);
-  k_curvatura<<<nb, 256, 0, s>>>(d);
+  lanca(k_normais, nb, 256, 0, s, d);
+  lanca(k_curvatura, nb, 256, 0, s, d);
 }
 void lancarPressaoDoAr(const Dev& d, double dt, double tensao, cudaStream_t s) {
-  k_pressao_ar<<<blocos(d.N, 256), 256, 0, s>>>(d, dt, tensao);
+  lanca(k_pressao_ar, blocos(d.N, 256), 256, 0, s, d, dt, tensao);
 }
 void lancarClassificar(const Dev& d, double dt, double tau, cudaStream_t s) {
-  k_classificar<<<blocos(d.N, 256), 256, 0, s>>>(d, dt, tau);
+  lanca(k_classificar, blocos(d.N, 256), 256, 0, s, d, dt, tau);
 }
 void lancarLadoDireitoBolhas(const Dev& d, double dt, cudaStream_t s) {
   cudaMemsetAsync(d.volB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
   cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
-  k_bolhas_somar<<<blocos(d.N, 256), 256, 0, s>>>(d);
-  k_bolhas_fechar<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d, dt);
+  lanca(k_bolhas_somar, blocos(d.N, 256), 256, 0, s, d);
+  lanca(k_bolhas_fechar, blocos(MAX_BOLHAS, 256), 256, 0, s, d, dt);
 }
 void lancarPosPressao(const Dev& d, double dt, bool ar, cudaStream_t s) {
-  k_pos_pressao<<<blocos(d.N, 256), 256, 0, s>>>(d, ar ? 1 : 0);
-  if (ar) k_pos_pressao_bolhas<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d, dt);
+  lanca(k_pos_pressao, blocos(d.N, 256), 256, 0, s, d, ar ? 1 : 0);
+  if (ar) lanca(k_pos_pressao_bolhas, blocos(MAX_BOLHAS, 256), 256, 0, s, d, dt);
 }
 void lancarGradiente(const Dev& d, cudaStream_t s) {
   int m = d.nu > d.nv ? d.nu : d.nv;
-  k_gradiente<<<blocos(m, 256), 256, 0, s>>>(d);
+  lanca(k_gradiente, blocos(m, 256), 256, 0, s, d);
 }
 void lancarExtrapolar(const Dev& d, cudaStream_t s) {
   int m = d.nu > d.nv ? d.nu : d.nv;
-  k_extrapolar<<<blocos(m, 256), 256, 0, s>>>(d, 0);
-  k_extrapolar<<<blocos(m, 256), 256, 0, s>>>(d, 1);
+  lanca(k_extrapolar, blocos(m, 256), 256, 0, s, d, 0);
+  lanca(k_extrapolar, blocos(m, 256), 256, 0, s, d, 1);
 }
 
 }  // namespace tq

@@ -460,39 +460,39 @@ __global__ void k_ferramenta(Dev d, tq_tool f) {
 
 // ---------------------------------------------------------------- host launchers
 void lancarP2G(const Dev& d, int nHint, cudaStream_t s) {
-  if (nHint > 0) k_p2g<<<blocos(nHint, 256), 256, 0, s>>>(d);
+  if (nHint > 0) lanca(k_p2g, blocos(nHint, 256), 256, 0, s, d);
 }
 void lancarFaces(const Dev& d, float gdx, float gdy, cudaStream_t s) {
   int m = d.nu > d.nv ? d.nu : d.nv;
-  k_faces<<<blocos(m, 256), 256, 0, s>>>(d, gdx, gdy);
+  lanca(k_faces, blocos(m, 256), 256, 0, s, d, gdx, gdy);
 }
 void lancarG2P(const Dev& d, int nHint, double dt, cudaStream_t s) {
-  if (nHint > 0) k_g2p<<<blocos(nHint, 128), 128, 0, s>>>(d, dt);
+  if (nHint > 0) lanca(k_g2p, blocos(nHint, 128), 128, 0, s, d, dt);
 }
 void lancarCompactar(const Dev& d, int nHint, int* cont, int* offs, int* estado, cudaStream_t s) {
   if (nHint <= 0) return;
   int nb = blocos(nHint, 1024);
-  k_compactar_contar<<<nb, 1024, 0, s>>>(d, cont);
-  k_compactar_scan<<<1, 1024, 0, s>>>(d, cont, offs, nb, estado);
-  k_compactar_mover<<<nb, 1024, 0, s>>>(d, offs, estado);
-  k_compactar_copiar<<<nb, 1024, 0, s>>>(d, estado);
+  lanca(k_compactar_contar, nb, 1024, 0, s, d, cont);
+  lanca(k_compactar_scan, 1, 1024, 0, s, d, cont, offs, nb, estado);
+  lanca(k_compactar_mover, nb, 1024, 0, s, d, offs, estado);
+  lanca(k_compactar_copiar, nb, 1024, 0, s, d, estado);
 }
 void lancarAdicionar(const Dev& d, const float* lista, int total, int checar, int* cont, int* offs,
                      unsigned long long idBase, cudaStream_t s) {
   int nb = blocos(total, 1024);
-  k_adicionar_contar<<<nb, 1024, 0, s>>>(d, lista, total, checar, cont);
-  k_adicionar_scan<<<1, 1024, 0, s>>>(d, cont, offs, nb);
-  k_adicionar_mover<<<nb, 1024, 0, s>>>(d, lista, total, checar, offs, idBase);
-  k_adicionar_fim<<<1, 1, 0, s>>>(d);
+  lanca(k_adicionar_contar, nb, 1024, 0, s, d, lista, total, checar, cont);
+  lanca(k_adicionar_scan, 1, 1024, 0, s, d, cont, offs, nb);
+  lanca(k_adicionar_mover, nb, 1024, 0, s, d, lista, total, checar, offs, idBase);
+  lanca(k_adicionar_fim, 1, 1, 0, s, d);
 }
 void lancarEmpacotar(const Dev& d, float* out, int n, cudaStream_t s) {
-  if (n > 0) k_empacotar<<<blocos(n, 256), 256, 0, s>>>(d, out, n);
+  if (n > 0) lanca(k_empacotar, blocos(n, 256), 256, 0, s, d, out, n);
 }
 void lancarDesempacotar(const Dev& d, const float* in, int n, unsigned long long idBase, cudaStream_t s) {
-  if (n > 0) k_desempacotar<<<blocos(n, 256), 256, 0, s>>>(d, in, n, idBase);
+  if (n > 0) lanca(k_desempacotar, blocos(n, 256), 256, 0, s, d, in, n, idBase);
 }
 void lancarFerramenta(const Dev& d, int nHint, const tq_tool& f, cudaStream_t s) {
-  if (nHint > 0) k_ferramenta<<<blocos(nHint, 256), 256, 0, s>>>(d, f);
+  if (nHint > 0) lanca(k_ferramenta, blocos(nHint, 256), 256, 0, s, d, f);
 }
 
 }  // namespace tq

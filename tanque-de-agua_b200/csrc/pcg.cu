@@ -615,8 +615,8 @@ static void suavizarNivel(Pcg* p, int l, int desl, int ordem, bool paraTmp, cuda
     using T = std::remove_pointer_t<decltype(tag)>;
     NivelDev<T> n = nivel<T>(p, l);
     dim3 g((n.nx + desl + 15) / 16, (n.ny + desl + 15) / 16);
-    if (paraTmp) k_suavizar<T><<<g, 256, 0, s>>>(n, desl, ordem, n.x, n.tmp, n.b);
-    else k_suavizar<T><<<g, 256, 0, s>>>(n, desl, ordem, n.tmp, n.x, n.b);
+    if (paraTmp) lanca(k_suavizar<T>, g, 256, 0, s, n, desl, ordem, n.x, n.tmp, n.b);
+    else lanca(k_suavizar<T>, g, 256, 0, s, n, desl, ordem, n.tmp, n.x, n.b);
   });
 }
 
@@ -627,7 +627,7 @@ static void restringirNivel(Pcg* p, int l, cudaStream_t s) {
       using TG = std::remove_pointer_t<decltype(tg)>;
       NivelDev<TF> f = nivel<TF>(p, l);
       NivelDev<TG> g = nivel<TG>(p, l + 1);
-      k_restringir<TF, TG><<<blocos((long)g.nx * g.ny, 256), 256, 0, s>>>(f, f.x, f.b, g);
+      lanca(k_restringir<TF, TG>, blocos((long)g.nx * g.ny, 256), 256, 0, s, f, f.x, f.b, g);
     });
   });
 }
@@ -639,7 +639,7 @@ static void prolongarNivel(Pcg* p, int l, cudaStream_t s) {
       using TF = std::remove_pointer_t<decltype(tf)>;
       NivelDev<TG> g = nivel<TG>(p, l + 1);
       NivelDev<TF> f = nivel<TF>(p, l);
-      k_prolongar<TG, TF><<<blocos((long)f.nx * f.ny, 256), 256, 0, s>>>(g, f, f.x);
+      lanca(k_prolongar<TG, TF>, blocos((long)f.nx * f.ny, 256), 256, 0, s, g, f, f.x);
     });
   });
 }
@@ -654,7 +654,7 @@ static void cicloV(Pcg* p, cudaStream_t s) {
   }
   NivelDev<float> g = nivel<float>(p, L - 1);
   if (L == 1) cudaMemsetAsync(g.x, 0, sizeof(float) * g.nx * g.ny, s);
-  k_grosso<<<1, 1024, p->smemGrosso, s>>>(g, p->smemGrosso ? 1 : 0);
+  lanca(k_grosso, 1, 1024, p->smemGrosso, s, g, p->smemGrosso ? 1 : 0);
   for (int l = L - 2; l >= 0; l--) {
     prolongarNivel(p, l, s);
     suavizarNivel(p, l, 8, 1, true, s);
@@ -666,67 +666,67 @@ static void cicloV(Pcg* p, cudaStream_t s) {
 static void prepararNiveis(Pcg* p, const uint8_t* tipo0, cudaStream_t s) {
   if (tipo0 != p->tipoL[0]) cudaMemcpyAsync(p->tipoL[0], tipo0, p->N, cudaMemcpyDeviceToDevice, s);
   for (int l = 1; l < p->L; l++)
-    k_mg_tipo_grosso<<<blocos((long)p->nxL[l] * p->nyL[l], 256), 256, 0, s>>>(
-        p->tipoL[l - 1], p->nxL[l - 1], p->nyL[l - 1], p->tipoL[l], p->nxL[l], p->nyL[l]);
+    lanca(k_mg_tipo_grosso, blocos((long)p->nxL[l] * p->nyL[l], 256), 256, 0, s, p->tipoL[l - 1], p->nxL[l - 1],
+          p->nyL[l - 1], p->tipoL[l], p->nxL[l], p->nyL[l]);
   for (int l = 0; l < p->L; l++)
-    k_viz<<<blocos((long)p->nxL[l] * p->nyL[l], 256), 256, 0, s>>>(p->tipoL[l], p->nxL[l], p->nyL[l], p->vizL[l]);
+    lanca(k_viz, blocos((long)p->nxL[l] * p->nyL[l], 256), 256, 0, s, p->tipoL[l], p->nxL[l], p->nyL[l], p->vizL[l]);
 }
 
 static void precondicionar(Pcg* p, const Dev& d, bool bolhas, cudaStream_t s) {
   int nb = blocos(d.N, 256);
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
-    k_pre_espalhar<T><<<nb, 256, 0, s>>>(d, nivel<T>(p, 0), bolhas ? 1 : 0);
+    lanca(k_pre_espalhar<T>, nb, 256, 0, s, d, nivel<T>(p, 0), bolhas ? 1 : 0);
   });
   cicloV(p, s);
   if (bolhas) cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
-    k_pre_juntar<T><<<nb, 256, 0, s>>>(d, nivel<T>(p, 0), bolhas ? 1 : 0);
+    lanca(k_pre_juntar<T>, nb, 256, 0, s, d, nivel<T>(p, 0), bolhas ? 1 : 0);
   });
-  if (bolhas) k_pre_bolhas<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d);
+  if (bolhas) lanca(k_pre_bolhas, blocos(MAX_BOLHAS, 256), 256, 0, s, d);
 }
 
 static void produto(Pcg* p, const Dev& d, int modo, const float* a, const float* b1, const float* b2, int it,
                     double tol, bool bolhas, cudaStream_t s) {
-  k_produto<<<DOT_BLOCOS, DOT_T, 0, s>>>(d, modo, a, b1, b2, it, tol, bolhas ? 1 : 0,
-                                         p->precisao != TQ_PREC_FP32 ? 1 : 0);
+  lanca(k_produto, DOT_BLOCOS, DOT_T, 0, s, d, modo, a, b1, b2, it, tol, bolhas ? 1 : 0,
+        p->precisao != TQ_PREC_FP32 ? 1 : 0);
 }
 
 int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s) {
   const int nb = blocos(d.N, 256);
   const int nbx = blocos(d.N > MAX_BOLHAS ? d.N : MAX_BOLHAS, 256);
   // operator (true types) and preconditioner types
-  k_viz<<<nb, 256, 0, s>>>(d.tipo, d.nx, d.ny, p->vizOp);
-  k_mg_tipo0<<<nb, 256, 0, s>>>(d.tipo, d.rotulo, p->tipoL[0], d.N, bolhas ? 1 : 0);
+  lanca(k_viz, nb, 256, 0, s, d.tipo, d.nx, d.ny, p->vizOp);
+  lanca(k_mg_tipo0, nb, 256, 0, s, d.tipo, d.rotulo, p->tipoL[0], d.N, bolhas ? 1 : 0);
   prepararNiveis(p, p->tipoL[0], s);
   cudaMemsetAsync(d.facesB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
   cudaMemsetAsync(d.celsB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
   if (bolhas) {
-    k_bolhas_faces<<<nb, 256, 0, s>>>(d);
-    k_bolhas_celulas<<<nb, 256, 0, s>>>(d);
+    lanca(k_bolhas_faces, nb, 256, 0, s, d);
+    lanca(k_bolhas_celulas, nb, 256, 0, s, d);
   }
-  k_bolhas_inicio<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d);
-  k_pcg_inicio<<<nb, 256, 0, s>>>(d, p->vizOp, bolhas ? 1 : 0);
+  lanca(k_bolhas_inicio, blocos(MAX_BOLHAS, 256), 256, 0, s, d);
+  lanca(k_pcg_inicio, nb, 256, 0, s, d, p->vizOp, bolhas ? 1 : 0);
   if (bolhas) {
     cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
-    k_bolhas_somar_v<<<nb, 256, 0, s>>>(d, d.q);
-    k_bolhas_linhas<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d, 0);
+    lanca(k_bolhas_somar_v, nb, 256, 0, s, d, d.q);
+    lanca(k_bolhas_linhas, blocos(MAX_BOLHAS, 256), 256, 0, s, d, 0);
   }
   produto(p, d, NORMA0, d.r, d.r, nullptr, 0, tol, bolhas, s);
   precondicionar(p, d, bolhas, s);
-  k_copiar_pz<<<nbx, 256, 0, s>>>(d);
+  lanca(k_copiar_pz, nbx, 256, 0, s, d);
   produto(p, d, RZ0, d.r, d.z, nullptr, 0, tol, bolhas, s);
   int it = 0;
   for (; it < iteracoes; it++) {
-    k_aplicar<<<nb, 256, 0, s>>>(d, p->vizOp, bolhas ? 1 : 0);
+    lanca(k_aplicar, nb, 256, 0, s, d, p->vizOp, bolhas ? 1 : 0);
     if (bolhas) {
       cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
-      k_bolhas_somar_v<<<nb, 256, 0, s>>>(d, d.p);
-      k_bolhas_linhas<<<blocos(MAX_BOLHAS, 256), 256, 0, s>>>(d, 1);
+      lanca(k_bolhas_somar_v, nb, 256, 0, s, d, d.p);
+      lanca(k_bolhas_linhas, blocos(MAX_BOLHAS, 256), 256, 0, s, d, 1);
     }
     produto(p, d, PAP, d.p, d.ap, nullptr, it, tol, bolhas, s);
-    k_atualizar<<<nbx, 256, 0, s>>>(d);
+    lanca(k_atualizar, nbx, 256, 0, s, d);
     produto(p, d, NORMA, d.r, d.r, nullptr, it, tol, bolhas, s);
     if (it == iteracoes - 1) break;
     if (tol > 0) {
@@ -736,12 +736,12 @@ int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas
         return TQ_E_CUDA;
       if (pronto) break;
     }
-    k_guardar_z<<<nbx, 256, 0, s>>>(d);
+    lanca(k_guardar_z, nbx, 256, 0, s, d);
     precondicionar(p, d, bolhas, s);
     produto(p, d, BETA, d.r, d.z, d.zOld, it, tol, bolhas, s);
-    k_direcao<<<nbx, 256, 0, s>>>(d);
+    lanca(k_direcao, nbx, 256, 0, s, d);
   }
-  k_pcg_fim<<<nbx, 256, 0, s>>>(d, bolhas ? 1 : 0);
+  lanca(k_pcg_fim, nbx, 256, 0, s, d, bolhas ? 1 : 0);
   // residual history for tq_last_norms
   int iters = 0;
   if (cudaMemcpyAsync(&iters, &d.esc->iters, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return TQ_E_CUDA;
@@ -781,12 +781,12 @@ int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cud
   int nb = blocos(p->N, 256);
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
-    k_carregar_b<T><<<nb, 256, 0, s>>>(nivel<T>(p, 0), b);
+    lanca(k_carregar_b<T>, nb, 256, 0, s, nivel<T>(p, 0), b);
   });
   cicloV(p, s);
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
-    k_descarregar_x<T><<<nb, 256, 0, s>>>(nivel<T>(p, 0), x);
+    lanca(k_descarregar_x<T>, nb, 256, 0, s, nivel<T>(p, 0), x);
   });
   return cudaGetLastError() == cudaSuccess ? TQ_OK : TQ_E_CUDA;
 }

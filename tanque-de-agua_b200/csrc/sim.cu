@@ -1,6 +1,8 @@
 // sim.cu — the tq_sim handle and the C-ABI entry points of include/tanque.h: device memory,
 // the substep orchestration (SimulacaoCPU.subpasso, js/fisica-cpu.js:176-189), state copies
 // and error reporting.  Every entry point returns a status and never throws.
+#include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -12,6 +14,11 @@
 #include "kernels.cuh"
 
 using namespace tq;
+
+namespace tq {
+static std::atomic<long long> g_lancamentos{0};
+void contarLancamento() { g_lancamentos.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace tq
 
 namespace {
 
@@ -60,9 +67,15 @@ struct tq_sim {
   float* staging = nullptr;
   size_t stagingCap = 0;
   std::vector<void*> alocados;
+  // Stage timing (tq_set_timing): a pool of events recorded at the stage boundaries of every
+  // substep and relabel, read back once by tq_get_timing.
   bool timing = false;
-  cudaEvent_t ev[16] = {};
-  std::vector<double> tempos;
+  std::vector<cudaEvent_t> pool;
+  size_t usados = 0;
+  std::vector<std::array<int, 8>> regSub;
+  std::vector<std::array<int, 2>> regAr;
+  std::array<int, 8>* atual = nullptr;
+  long long itersTotal = 0;
 };
 
 namespace {
@@ -98,8 +111,30 @@ int lerContagem(tq_sim* s, int* n) {
 
 void compactar(tq_sim* s) { lancarCompactar(s->d, s->nHint, s->cont, s->offs, s->estado, s->s); }
 
+constexpr size_t MAX_EVENTOS = 1 << 15;
+
+// Records the next pool event on the stream; returns its index, or -1 when timing is off or
+// the pool is exhausted.
+int evento(tq_sim* s) {
+  if (!s->timing) return -1;
+  if (s->usados == s->pool.size()) {
+    if (s->pool.size() >= MAX_EVENTOS) return -1;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    s->pool.push_back(e);
+  }
+  int i = (int)s->usados++;
+  cudaEventRecord(s->pool[i], s->s);
+  return i;
+}
+// Stage boundary i (0..7) of the running substep.
 void marca(tq_sim* s, int i) {
-  if (s->timing) cudaEventRecord(s->ev[i], s->s);
+  if (!s->timing) return;
+  if (i == 0) {
+    s->regSub.push_back({-1, -1, -1, -1, -1, -1, -1, -1});
+    s->atual = &s->regSub.back();
+  }
+  if (s->atual) (*s->atual)[i] = evento(s);
 }
 
 // P2G + flags only (the first half of atualizarAr when the flags are stale, js/fisica-cpu.js:164).
@@ -138,6 +173,7 @@ int subpasso(tq_sim* s, double dt) {
   marca(s, 4);
   int r = resolverPressao(s->pcg, d, s->o.iterations, s->o.tolerance, ar, st);  // #pressao
   if (r) return r == TQ_E_CUDA ? falha(r, "pressure solve failed") : r;
+  if (s->timing) s->itersTotal += itersPcg(s->pcg);
   lancarPosPressao(d, dt, ar, st);
   marca(s, 5);
   lancarGradiente(d, st);                                                  // #gradiente
@@ -246,6 +282,7 @@ int tq_create(const tq_options* o, tq_sim** out) {
   if (o->p2g_mode != TQ_P2G_FIXED) return falha(TQ_E_ARG, "the CUDA library implements TQ_P2G_FIXED only");
   if (o->precision < TQ_PREC_FP32 || o->precision > TQ_PREC_BF16) return falha(TQ_E_ARG, "bad precision");
   if (o->engine != TQ_ENGINE_PLAIN && o->engine != TQ_ENGINE_FUSED) return falha(TQ_E_ARG, "bad engine");
+  if (o->engine == TQ_ENGINE_FUSED) return falha(TQ_E_ARG, "fused engine not available in this build");
   int st = iniciarCuda(o->device);
   if (st) return st;
   tq_sim* s = new (std::nothrow) tq_sim();
@@ -310,7 +347,6 @@ int tq_create(const tq_options* o, tq_sim** out) {
     tq_destroy(s);
     return falha(TQ_E_CUDA, "upload failed");
   }
-  for (auto& e : s->ev) cudaEventCreate(&e);
   lancarSolidos(d, s->s);
   if (cudaStreamSynchronize(s->s) != cudaSuccess) {
     tq_destroy(s);
@@ -327,8 +363,7 @@ int tq_destroy(tq_sim* s) {
   destruirRastreador(s->ar);
   for (void* p : s->alocados) cudaFree(p);
   if (s->staging) cudaFree(s->staging);
-  for (auto& e : s->ev)
-    if (e) cudaEventDestroy(e);
+  for (auto& e : s->pool) cudaEventDestroy(e);
   if (s->s) cudaStreamDestroy(s->s);
   delete s;
   return TQ_OK;
@@ -368,7 +403,7 @@ int tq_clear_particles(tq_sim* s) {
   if (!s) return falha(TQ_E_ARG, "null handle");
   CK(cudaMemsetAsync(&s->d.esc->n, 0, sizeof(int), s->s));
   CK(cudaMemsetAsync(&s->d.esc->mortas, 0, sizeof(int), s->s));
-  k_zerar_contagem<<<blocos(s->N, 256), 256, 0, s->s>>>(s->d.accCel, s->N);
+  lanca(k_zerar_contagem, blocos(s->N, 256), 256, 0, s->s, s->d.accCel, s->N);
   CK(cudaStreamSynchronize(s->s));
   s->nHint = 0;
   return TQ_OK;
@@ -387,9 +422,10 @@ int tq_apply_tool(tq_sim* s, const tq_tool* t) {
 int tq_update_air(tq_sim* s) {
   if (!s) return falha(TQ_E_ARG, "null handle");
   if (!s->tiposProntos) paraGradeETipos(s);
-  marca(s, 8);
+  int e0 = evento(s);
   int r = atualizarRastreador(s->ar, s->d, s->s);
-  marca(s, 9);
+  int e1 = evento(s);
+  if (e0 >= 0 && e1 >= 0) s->regAr.push_back({e0, e1});
   if (r == TQ_E_TIMEOUT) return falha(r, "air labelling: union-find retry bound reached");
   if (r) return falha(r, "air labelling failed");
   return TQ_OK;
@@ -560,7 +596,7 @@ int tq_set_field(tq_sim* s, int32_t f, const void* in, int64_t bytes) {
       uint32_t* tmp = nullptr;
       CK(cudaMallocAsync((void**)&tmp, bytes, s->s));
       CK(cudaMemcpyAsync(tmp, in, bytes, cudaMemcpyHostToDevice, s->s));
-      k_gravar_contagem<<<blocos(s->N, 256), 256, 0, s->s>>>(d.accCel, tmp, s->N);
+      lanca(k_gravar_contagem, blocos(s->N, 256), 256, 0, s->s, d.accCel, tmp, s->N);
       CK(cudaFreeAsync(tmp, s->s));
       CK(cudaStreamSynchronize(s->s));
       return TQ_OK;
@@ -574,6 +610,10 @@ int tq_set_field(tq_sim* s, int32_t f, const void* in, int64_t bytes) {
 }
 
 int tq_get_scalar(tq_sim* s, int32_t w, double* out) {
+  if (out && w == TQ_SCALAR_LAUNCHES) {  // process-wide: no handle needed
+    *out = (double)g_lancamentos.load();
+    return TQ_OK;
+  }
   if (!s || !out) return falha(TQ_E_ARG, "null argument");
   switch (w) {
     case TQ_SCALAR_VMAX: {
@@ -585,6 +625,7 @@ int tq_get_scalar(tq_sim* s, int32_t w, double* out) {
       *out = v;
       return TQ_OK;
     }
+    case TQ_SCALAR_LAUNCHES: *out = (double)g_lancamentos.load(); return TQ_OK;
     case TQ_SCALAR_PRIMEIRA: *out = primeiraRastreador(s->ar); return TQ_OK;
     case TQ_SCALAR_TIPOS_PRONTOS: *out = s->tiposProntos ? 1 : 0; return TQ_OK;
     case TQ_SCALAR_PCG_ITERS: *out = itersPcg(s->pcg); return TQ_OK;
@@ -632,34 +673,52 @@ int tq_sync(tq_sim* s) {
   return TQ_OK;
 }
 
-int tq_set_timing(tq_sim* s, int32_t on) {
-  if (!s) return falha(TQ_E_ARG, "null handle");
-  s->timing = on != 0;
+int tq_get_stream(tq_sim* s, void** stream) {
+  if (!s || !stream) return falha(TQ_E_ARG, "null argument");
+  *stream = (void*)s->s;
   return TQ_OK;
 }
 
-// Stage times of the last substep (ms): p2g+faces, flags+labels, surface, divergence+bubbles,
-// pressure, gradient+extrapolation, g2p; then the air relabel of the last update.
+int tq_set_timing(tq_sim* s, int32_t on) {
+  if (!s) return falha(TQ_E_ARG, "null handle");
+  CK(cudaStreamSynchronize(s->s));
+  s->timing = on != 0;
+  s->usados = 0;
+  s->regSub.clear();
+  s->regAr.clear();
+  s->atual = nullptr;
+  s->itersTotal = 0;
+  return TQ_OK;
+}
+
+// Accumulated stage times since tq_set_timing (ms): [0..6] p2g+faces, flags+labels, surface,
+// divergence+bubbles, pressure solve, gradient+extrapolation, g2p; [7] air relabels;
+// [8] substeps timed; [9] pressure iterations in total; [10] relabels timed.
 int tq_get_timing(tq_sim* s, double* ms, int32_t cap, int32_t* n) {
   if (!s) return falha(TQ_E_ARG, "null handle");
-  if (!s->timing) {
-    if (n) *n = 0;
-    return TQ_OK;
+  double v[11] = {0};
+  if (s->timing) {
+    CK(cudaStreamSynchronize(s->s));
+    auto dur = [&](int a, int b) -> double {
+      float t = 0;
+      if (a < 0 || b < 0 || cudaEventElapsedTime(&t, s->pool[a], s->pool[b]) != cudaSuccess) return 0.0;
+      return t;
+    };
+    int completos = 0;
+    for (auto& r : s->regSub) {
+      if (r[7] < 0) continue;
+      for (int i = 0; i < 7; i++) v[i] += dur(r[i], r[i + 1]);
+      completos++;
+    }
+    for (auto& r : s->regAr) v[7] += dur(r[0], r[1]);
+    v[8] = completos;
+    v[9] = (double)s->itersTotal;
+    v[10] = (double)s->regAr.size();
+    cudaGetLastError();
   }
-  CK(cudaStreamSynchronize(s->s));
-  double v[8];
-  for (int i = 0; i < 7; i++) {
-    float t = 0;
-    if (cudaEventElapsedTime(&t, s->ev[i], s->ev[i + 1]) != cudaSuccess) t = 0;
-    v[i] = t;
-  }
-  float t = 0;
-  if (cudaEventElapsedTime(&t, s->ev[8], s->ev[9]) != cudaSuccess) t = 0;
-  v[7] = t;
-  cudaGetLastError();
-  if (n) *n = 8;
+  if (n) *n = 11;
   if (ms)
-    for (int i = 0; i < 8 && i < cap; i++) ms[i] = v[i];
+    for (int i = 0; i < 11 && i < cap; i++) ms[i] = v[i];
   return TQ_OK;
 }
 

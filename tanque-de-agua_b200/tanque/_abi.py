@@ -36,6 +36,7 @@ CAMPOS_ENUM = {
 }
 TQ_SCALAR_VMAX, TQ_SCALAR_PRIMEIRA, TQ_SCALAR_TIPOS_PRONTOS = 0, 1, 2
 TQ_SCALAR_PCG_ITERS, TQ_SCALAR_PCG_RES0, TQ_SCALAR_PCG_RES = 3, 4, 5
+TQ_SCALAR_LAUNCHES = 6
 
 
 class TqOptions(C.Structure):
@@ -98,6 +99,7 @@ ASSINATURAS = {
 }
 SO_PRODUTO = {
     "sync": (C.c_int, [_P]),
+    "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "set_timing": (C.c_int, [_P, _I]),
     "get_timing": (C.c_int, [_P, C.POINTER(_D), _I, C.POINTER(_I)]),
     "options_default": (None, [C.POINTER(TqOptions), _I, _I, _D]),

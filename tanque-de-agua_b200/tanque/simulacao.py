@@ -217,15 +217,36 @@ class SimulacaoGPU(Simulacao):
     def sincronizar(self):
         self._lig("sync", self._h)
 
+    ETAPAS = ["p2g", "tipos_rotulos", "superficie", "divergencia_bolhas", "pressao", "gradiente_extrapolacao", "g2p"]
+
     def tempos(self, ligar: bool | None = None):
-        """Per-stage device times (ms) of the last substep; `ligar` switches timing on/off."""
+        """Stage timing (CUDA events on the handle's stream).  `ligar=True` starts/resets the
+        accumulation; without arguments returns the totals since then (ms per stage, air
+        relabel ms, substeps, pressure iterations, relabels)."""
         if ligar is not None:
             self._lig("set_timing", self._h, 1 if ligar else 0)
             return None
         n = C.c_int32(0)
         buf = (C.c_double * 16)()
         self._lig("get_timing", self._h, buf, 16, C.byref(n))
-        return list(buf[: n.value])
+        v = list(buf[: n.value])
+        out = {e: v[i] for i, e in enumerate(self.ETAPAS)}
+        out.update(ar=v[7], subpassos=int(v[8]), iteracoes=int(v[9]), reetiquetagens=int(v[10]))
+        return out
+
+    def stream(self) -> int:
+        """The handle's cudaStream_t (as an integer), for torch.cuda.ExternalStream."""
+        p = C.c_void_p()
+        self._lig("get_stream", self._h, C.byref(p))
+        return p.value or 0
+
+    @staticmethod
+    def lancamentos() -> int:
+        """Kernels launched by this process so far (all handles)."""
+        lig = _abi.carregar()
+        v = C.c_double(0)
+        lig.f["get_scalar"](None, _abi.TQ_SCALAR_LAUNCHES, C.byref(v))
+        return int(v.value)
 
 
 def resolver_pressao(tipo, div, q, iteracoes=ITERACOES_PCG, tolerancia=0.0, bolhas=None, precisao=0, motor=0,

@@ -1,0 +1,62 @@
+"""Helpers shared by the GPU parity tests: scenes, state transfer oracle -> CUDA, comparisons."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from oraculo import CenaOraculo, SimulacaoOraculo
+from tanque import _abi
+from tanque.cenarios import MODELOS, semear_agua, semear_retangulo, semente
+from tanque.constantes import CAMPOS, MOLDURA
+
+# Fields that describe the state between substeps (what SimulacaoCPU carries over).
+ESTADO = ["q", "rotulo", "pressaoBolha", "volumeAlvo", "vivo", "tipo", "contagemCelula"]
+ESCALARES = [_abi.TQ_SCALAR_PRIMEIRA, _abi.TQ_SCALAR_TIPOS_PRONTOS]
+
+
+def cena_barragem(Cn, nx=60, ny=40, h=0.01):
+    cena = Cn(nx, ny, h)
+    m = MOLDURA * h
+    agua = semear_retangulo(m, m, 0.45 * nx * h, 0.6 * ny * h, h, (0, 0, 0), semente(1))
+    return cena, agua
+
+
+def cena_bolha(Cn, n=60, h=0.01):
+    cena = Cn(n, n, h)
+    m = MOLDURA * h
+    agua = semear_retangulo(m, m, n * h - m, 0.45, h, (0, 0, 0), semente(5)).reshape(-1, CAMPOS)
+    x, y = agua[:, 0].astype(np.float64), agua[:, 1].astype(np.float64)
+    fora = (x - 0.3) ** 2 + (y - 0.12) ** 2 >= 0.05 ** 2
+    # some dye so the dye sums are exercised
+    agua[: len(agua) // 3, 9] = 1.5
+    agua[: len(agua) // 5, 11] = 0.25
+    return cena, agua[fora].ravel()
+
+
+def cena_copo(Cn, nx=90, ny=60, h=0.01):
+    cena = Cn(nx, ny, h)
+    m = MODELOS["copo"](cena.largura, cena.altura, h)
+    for t in m["tracos"]:
+        cena.tracar(t["x0"], t["y0"], t["x1"], t["y1"], t["raio"])
+    agua = np.concatenate([semear_agua(a, h, (0, 0, 0), semente(11)) for a in m["agua"]])
+    return cena, agua
+
+
+CENAS = {"barragem": cena_barragem, "bolha": cena_bolha, "copo": cena_copo}
+
+
+def copiar_estado(de, para):
+    """Copies the between-substeps state of `de` into `para` (both Simulacao)."""
+    para.definirParticulas(de.p)
+    for nome in ESTADO:
+        para.definirCampo(nome, de.campo(nome))
+    for s in ESCALARES:
+        para.definirEscalar(s, de.escalar(s))
+
+
+def erro_relativo(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    escala = max(float(np.max(np.abs(b))) if b.size else 0.0, 1e-30)
+    return float(np.max(np.abs(a - b))) / escala if a.size else 0.0
