@@ -211,6 +211,11 @@ int tq_get_stream(tq_sim* s, void** stream);
 int tq_set_timing(tq_sim* s, int32_t enabled);
 int tq_get_timing(tq_sim* s, double* ms_out, int32_t cap, int32_t* n);
 
+/* With tq_set_timing(s, 2) the fused engine also records a phase trace of its last pressure
+ * solve: the device %globaltimer (ns) as each grid barrier completes.  Consecutive
+ * differences are the durations of the solve's phases. */
+int tq_get_phase_trace(tq_sim* s, uint64_t* out, int32_t cap, int32_t* n);
+
 /* ---------------------------------------------------------------- standalone solver */
 /* Bubble description for the standalone solve: `bolhas = { rotulo, rhs, y }` of
  * resolverPCG (js/pressao-cpu.js:291-296).  y is read as the initial guess and receives

@@ -36,6 +36,9 @@ void destruirPcg(Pcg* p);
 int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s);
 int normasPcg(Pcg* p, double* out, int cap);
 int itersPcg(Pcg* p);
+// Phase trace of the fused engine (%globaltimer at each grid barrier of the last solve).
+void perfilPcg(Pcg* p, bool ligar);
+int lerPerfilPcg(Pcg* p, unsigned long long* out, int cap);
 // One V-cycle from device buffers (level-0 types, right-hand side, result).
 int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cudaStream_t s);
 

@@ -11,6 +11,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "pcg_interno.cuh"
 #include <type_traits>
 
 namespace tq {
@@ -511,23 +512,7 @@ __global__ void __launch_bounds__(DOT_T) k_produto(Dev d, int modo, const float*
 }
 
 // ---------------------------------------------------------------- the solver object
-struct Pcg {
-  int nx, ny, N, precisao, motor;
-  int L;
-  int nxL[MAX_NIVEIS], nyL[MAX_NIVEIS];
-  bool meia[MAX_NIVEIS];  // level stored in half precision
-  uint8_t* tipoL[MAX_NIVEIS];
-  uint8_t* vizL[MAX_NIVEIS];
-  void *bL[MAX_NIVEIS], *xL[MAX_NIVEIS], *tmpL[MAX_NIVEIS];
-  uint8_t* vizOp;
-  std::vector<double> normas;
-  int iters = 0;
-  size_t smemGrosso = 0;
-};
 
-constexpr int MEIA_MIN_CELULAS = 16384;
-
-static size_t tamanhoElem(int prec, bool meia) { return (meia && prec != TQ_PREC_FP32) ? 2 : 4; }
 
 Pcg* criarPcg(int nx, int ny, int precisao, int motor) {
   Pcg* p = new Pcg();
@@ -554,7 +539,7 @@ Pcg* criarPcg(int nx, int ny, int precisao, int motor) {
   for (int l = 0; l < L; l++) {
     size_t n = (size_t)p->nxL[l] * p->nyL[l];
     p->meia[l] = precisao != TQ_PREC_FP32 && n >= (size_t)MEIA_MIN_CELULAS;
-    size_t e = tamanhoElem(precisao, p->meia[l]);
+    const size_t e = 4;  // room for FP32 whatever the engine stores
     ok &= cudaMalloc(&p->tipoL[l], n) == cudaSuccess;
     ok &= cudaMalloc(&p->vizL[l], n) == cudaSuccess;
     ok &= cudaMalloc(&p->bL[l], n * e) == cudaSuccess;
@@ -568,6 +553,15 @@ Pcg* criarPcg(int nx, int ny, int precisao, int motor) {
     if (cudaFuncSetAttribute(k_grosso, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smemGrosso) != cudaSuccess)
       p->smemGrosso = 0;
   }
+  if (ok && motor == TQ_ENGINE_FUSED) {
+    // Grids with a single level (min(nx, ny) <= 12) have nothing to hand to the coarse
+    // section: they run on the plain engine.
+    p->fundido = criarFundido(p);
+    if (!p->fundido) {
+      cudaGetLastError();
+      p->motor = TQ_ENGINE_PLAIN;
+    }
+  }
   if (!ok) {
     destruirPcg(p);
     return nullptr;
@@ -577,6 +571,7 @@ Pcg* criarPcg(int nx, int ny, int precisao, int motor) {
 
 void destruirPcg(Pcg* p) {
   if (!p) return;
+  destruirFundido(p->fundido);
   for (int l = 0; l < p->L; l++) {
     cudaFree(p->tipoL[l]);
     cudaFree(p->vizL[l]);
@@ -694,6 +689,7 @@ static void produto(Pcg* p, const Dev& d, int modo, const float* a, const float*
 }
 
 int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s) {
+  if (p->motor == TQ_ENGINE_FUSED) return resolverPressaoFundido(p, d, iteracoes, tol, bolhas, s);
   const int nb = blocos(d.N, 256);
   const int nbx = blocos(d.N > MAX_BOLHAS ? d.N : MAX_BOLHAS, 256);
   // operator (true types) and preconditioner types
@@ -761,6 +757,8 @@ int normasPcg(Pcg* p, double* out, int cap) {
   return n;
 }
 int itersPcg(Pcg* p) { return p->iters; }
+void perfilPcg(Pcg* p, bool ligar) { perfilFundido(p->fundido, ligar); }
+int lerPerfilPcg(Pcg* p, unsigned long long* out, int cap) { return lerPerfilFundido(p->fundido, out, cap); }
 
 // One V-cycle on caller-provided device buffers (tq_vcycle).
 template <class T>

@@ -1,0 +1,1358 @@
+// pcg_fundido.cu — FUSED engine of the MGPCG pressure projection: the whole solve of
+// resolverPCG (js/pressao-cpu.js:296-402) in ONE persistent cooperative launch.
+//
+// One CTA of 512 threads per SM; phases are separated by a grid barrier (monotonic arrival
+// counter, release-add / acquire-poll) whose waits are bounded: a wait that exceeds ~1 s sets
+// an error flag, every CTA returns, and the host reports TQ_E_TIMEOUT.
+// Per PCG iteration: [DA] p = z + beta p fused with A p and p.Ap, [B] the q/r/bubble updates
+// with r.r, [C] the convergence test fused with spreading the residual into the V-cycle's
+// right-hand side, the V-cycle, and the gather of z with r.z and r.zOld.
+// The V-cycle is the reference's preconditioner (cicloV, js/pressao-cpu.js:241-255):
+//   - grid levels: the snapshot block smoother with one WARP per 16x16 block (8 cells per
+//     lane, warp-synchronous red-black sweeps in a per-warp shared tile); the prolongation of
+//     the coarse correction is folded into the tile load of the first smoother pass on the way
+//     up; the restriction is a per-warp tile (a 32-cell coarse row segment and its fine
+//     footprint staged in shared memory);
+//   - the coarse levels (the largest suffix of levels fitting in ~200 KB) run inside CTA 0's
+//     shared memory, warps mapped to rows, while the other CTAs wait at the barrier.
+// Scalars (alpha, beta, norms) are FP64 sums of per-CTA partials in a fixed order, computed
+// redundantly by every CTA after the barrier, so all CTAs hold the same bits without another
+// barrier; per-bubble sums are 64-bit fixed point as in the plain engine.
+#include <cstdio>
+#include <type_traits>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "pcg_interno.cuh"
+
+namespace tq {
+
+constexpr int TF = 512;
+constexpr int WARPS = TF / 32;
+constexpr long long LIMITE_CICLOS = 2000000000LL;  // ~1 s at 1.9 GHz
+constexpr double ESC = 1099511627776.0;            // 2^40, per-bubble fixed point
+constexpr size_t SMEM_GROSSO_MAX = 200 * 1024;
+constexpr int NPARC = 4;                           // partial slots per CTA
+constexpr int PERFIL_MAX = 1 << 16;                // phase-trace capacity
+constexpr int PERFIL_SECAO = 1 << 14;              // coarse-section stamps (after the phase trace)
+// per-warp shared-memory areas (floats)
+constexpr int TILE = 324;                          // 18x18 smoother tile
+constexpr int CT = 121;                            // 11x11 coarse tile for the folded prolongation
+constexpr int SUAV_W = TILE + CT + 32;             // + coarse water flags (bytes, rounded)
+constexpr int RX = 6 * 68, RB = 4 * 66;            // restriction staging: x rows, b/viz/residual rows
+constexpr int REST_W = RX + 3 * RB;                // x, b, residual (floats) + viz (bytes in one RB)
+constexpr size_t TILES_SECAO = (size_t)(512 / 32) * TILE * 4;  // per-warp tiles of the coarse section
+
+struct NivelF {
+  int nx, ny, meia, pad;
+  uint8_t* viz;
+  uint8_t* tipo;
+  void *b, *x, *tmp;
+};
+
+struct Fundido {
+  int G = 0, Lc = 0;
+  size_t smem = 0;
+  NivelF* niveis = nullptr;  // level table (device)
+  double* parc = nullptr;
+  unsigned* bar = nullptr;
+  int* erro = nullptr;
+  long long* accZ = nullptr;
+  double *zb2 = nullptr, *pb2 = nullptr;
+  int* ativos = nullptr;
+  int* nAtivos = nullptr;
+  float *p2 = nullptr, *z2 = nullptr;
+  float *xc = nullptr, *bc = nullptr;
+  void* kern = nullptr;
+  unsigned long long* perfil = nullptr;
+  bool perfilar = false;
+};
+
+struct Args {
+  Dev d;
+  int L, Lc;
+  const NivelF* niv;
+  uint8_t* vizOp;
+  int iteracoes;
+  double tol;
+  int bolhas, escalar;
+  double* parc;
+  unsigned* bar;
+  int* erro;
+  long long* accZ;
+  double *zb2, *pb2;
+  int* ativos;
+  int* nAtivos;
+  float *p2, *z2;
+  float *xc, *bc;
+  unsigned long long* perfil;  // [0] count, [1..] %globaltimer at each barrier (null: off)
+};
+
+// Phase trace of the fused solve (the %globaltimer at every grid barrier of the last solve).
+void perfilFundido(Fundido* f, bool ligar) {
+  if (!f) return;
+  f->perfilar = ligar;
+  if (ligar && !f->perfil) {
+    if (cudaMalloc(&f->perfil, (PERFIL_MAX + 2 + PERFIL_SECAO) * sizeof(unsigned long long)) != cudaSuccess) {
+      f->perfil = nullptr;
+      f->perfilar = false;
+    }
+  }
+}
+int lerPerfilFundido(Fundido* f, unsigned long long* out, int cap) {
+  if (!f || !f->perfil) return 0;
+  if (cap < 0) {  // the coarse-section stamps instead of the phase trace
+    unsigned long long n = 0;
+    if (cudaMemcpy(&n, f->perfil + PERFIL_MAX + 1, sizeof n, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+    if (n > PERFIL_SECAO) n = PERFIL_SECAO;
+    int k = (int)(n < (unsigned long long)(-cap) ? n : (unsigned long long)(-cap));
+    if (k > 0 && cudaMemcpy(out, f->perfil + PERFIL_MAX + 2, k * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+    return k;
+  }
+  unsigned long long n = 0;
+  if (cudaMemcpy(&n, f->perfil, sizeof n, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+  if (n > PERFIL_MAX) n = PERFIL_MAX;
+  int k = (int)(n < (unsigned long long)cap ? n : (unsigned long long)cap);
+  if (k > 0 && cudaMemcpy(out, f->perfil + 1, k * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return 0;
+  return k;
+}
+
+// ---------------------------------------------------------------- small helpers
+template <class T>
+__device__ __forceinline__ T ldcg(const T* p) { return __ldcg(p); }
+template <>
+__device__ __forceinline__ __half ldcg<__half>(const __half* p) {
+  return __ushort_as_half(__ldcg((const unsigned short*)p));
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 ldcg<__nv_bfloat16>(const __nv_bfloat16* p) {
+  return __ushort_as_bfloat16(__ldcg((const unsigned short*)p));
+}
+__device__ __forceinline__ int ldcg8(const uint8_t* p) { return (int)__ldcg((const unsigned char*)p); }
+
+__device__ __forceinline__ float lerN(int meia, const void* v, int c) {
+  return meia == 0 ? __ldcg((const float*)v + c)
+                   : (meia == 1 ? __half2float(ldcg((const __half*)v + c))
+                                : __bfloat162float(ldcg((const __nv_bfloat16*)v + c)));
+}
+__device__ __forceinline__ void gravarN(int meia, void* v, int c, float x) {
+  if (meia == 0) ((float*)v)[c] = x;
+  else if (meia == 1) ((__half*)v)[c] = __float2half_rn(x);
+  else ((__nv_bfloat16*)v)[c] = __float2bfloat16_rn(x);
+}
+
+__device__ __forceinline__ unsigned lerAdquirir(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void somarLiberar(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid barrier: every CTA adds 1 (release) to a counter that only grows during the solve and
+// waits (acquire) until it reaches epoch * gridDim.  The wait is bounded.  Returns false when
+// this CTA gave up (its wait ran out, or it saw another CTA's error flag while waiting); a CTA
+// that gave up returns, so the others give up at their next barrier.
+__device__ bool barreira(const Args& a, unsigned& epoca) {
+  __shared__ int falhou;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    epoca++;
+    const unsigned alvo = epoca * gridDim.x;
+    somarLiberar(a.bar, 1u);
+    long long t0 = clock64();
+    int f = 0;
+    for (unsigned voltas = 0;; voltas++) {
+      if (lerAdquirir(a.bar) >= alvo) break;
+      if ((voltas & 255u) == 255u) {
+        if (*(volatile int*)a.erro) {
+          f = 1;
+          break;
+        }
+        if (clock64() - t0 > LIMITE_CICLOS) {
+          atomicExch(a.erro, 1);
+          f = 1;
+          break;
+        }
+      }
+    }
+    falhou = f;
+    if (a.perfil && blockIdx.x == 0) {
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      unsigned long long k = a.perfil[0]++;
+      if (k < PERFIL_MAX) a.perfil[1 + k] = t;
+    }
+  }
+  __syncthreads();
+  return falhou == 0;
+}
+
+// Block sum of a double (valid in thread 0).
+__device__ double somaBloco(double v, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0;
+  if (w == 0) {
+    t = sh[lane];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  }
+  return t;
+}
+
+// Sums, in CTA order, of the per-CTA partials of channels 0 and 1, plus up to two sums over
+// the active bubbles (ascending labels).  Warp 0 of every CTA does the same work on the same
+// data, so every CTA obtains the same bits.
+template <class F0, class F1>
+__device__ void somasGlobais(const Args& a, int nAt, F0 f0, F1 f1, double* sh, double out[4]) {
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v0 = 0, v1 = 0, b0 = 0, b1 = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) {
+      v0 += __ldcg(&a.parc[k * NPARC + 0]);
+      v1 += __ldcg(&a.parc[k * NPARC + 1]);
+    }
+    for (int k = threadIdx.x; k < nAt; k += 32) {
+      int b = __ldcg(&a.ativos[k]);
+      b0 += f0(b);
+      b1 += f1(b);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      v0 += __shfl_down_sync(0xffffffffu, v0, o);
+      v1 += __shfl_down_sync(0xffffffffu, v1, o);
+      b0 += __shfl_down_sync(0xffffffffu, b0, o);
+      b1 += __shfl_down_sync(0xffffffffu, b1, o);
+    }
+    if (threadIdx.x == 0) {
+      sh[0] = v0;
+      sh[1] = v1;
+      sh[2] = b0;
+      sh[3] = b1;
+    }
+  }
+  __syncthreads();
+  out[0] = sh[0];
+  out[1] = sh[1];
+  out[2] = sh[2];
+  out[3] = sh[3];
+  __syncthreads();
+}
+
+__device__ __forceinline__ bool bolhaAtiva(const Args& a, uint32_t r) {
+  return r >= 2 && r < (uint32_t)MAX_BOLHAS && __ldcg(&a.d.facesB[r]) > 0;
+}
+
+__device__ __forceinline__ int grossoBaseF(int i) { return (i & 1) == 0 ? (i >> 1) - 1 : (i - 1) >> 1; }
+__device__ __forceinline__ float pesoBaseF(int i) { return (i & 1) == 0 ? 0.25f : 0.75f; }
+
+// ---------------------------------------------------------------- block sweeps
+// Cell m (0..7) of lane l in a 16x16 block whose origin has even x + y (every block origin is
+// a multiple of 8): m < 4 are the lane's cells of colour 0, m >= 4 of colour 1, in rows
+// (l >> 3) + 4(m & 3) and the column pair 2(l & 7), 2(l & 7) + 1.  The colour of a cell is
+// (x + y + 1) & 1 (js/pressao-cpu.js:120), so every lane updates four cells in each half-sweep.
+// Returns row * 16 + column.
+__device__ __forceinline__ int celulaBloco(int lane, int m) {
+  const int row = (lane >> 3) + 4 * (m & 3);
+  const int col = 2 * (lane & 7) + (((m >> 2) + 1 + (lane >> 3)) & 1);
+  return row * 16 + col;
+}
+
+// 1/k for k free neighbours (k = 1..4), the correctly rounded float constants.
+__device__ __forceinline__ float inversoVizinhos(int k) {
+  return k == 1 ? 1.0f : k == 2 ? 0.5f : k == 3 ? (1.0f / 3.0f) : 0.25f;
+}
+
+// The VARREDURAS red-black sweeps of one 16x16 block on its 18x18 shared tile
+// (js/pressao-cpu.js:114-137), by one warp, cells as in celulaBloco; vz = neighbour mask |
+// 16 water | 128 in grid, bv = right side.  Within a half-sweep a cell reads only cells of the
+// other colour and itself, so each lane issues all its loads before its stores.
+__device__ __forceinline__ void varrerTile(float* tile, const int (&vz)[8], const float (&bv)[8], int ordem) {
+  const int lane = threadIdx.x & 31;
+  int li[4];
+#pragma unroll
+  for (int mm = 0; mm < 4; mm++) li[mm] = ((lane >> 3) + 4 * mm + 1) * 18 + 2 * (lane & 7) + 1;
+  const int par = (1 + (lane >> 3)) & 1;  // column offset of colour 0; colour 1 is the other one
+  float inv[8];
+#pragma unroll
+  for (int m = 0; m < 8; m++) inv[m] = inversoVizinhos(__popc(vz[m] & 15));
+#pragma unroll
+  for (int it = 0; it < VARREDURAS; it++) {
+#pragma unroll
+    for (int o = 0; o < 2; o++) {
+      const int cor = o ^ ordem;
+      const int dc = cor ? par ^ 1 : par;
+      float nb[4][5];
+#pragma unroll
+      for (int mm = 0; mm < 4; mm++) {
+        const int p = li[mm] + dc;
+        nb[mm][0] = tile[p - 1];
+        nb[mm][1] = tile[p + 1];
+        nb[mm][2] = tile[p - 18];
+        nb[mm][3] = tile[p + 18];
+        nb[mm][4] = tile[p];
+      }
+#pragma unroll
+      for (int mm = 0; mm < 4; mm++) {
+        const int v = cor ? vz[4 + mm] : vz[mm];
+        const int mk = v & 15;
+        if ((v & 16) && mk) {
+          float s = 0.0f;
+          s += (mk & 1) ? nb[mm][0] : 0.0f;
+          s += (mk & 2) ? nb[mm][1] : 0.0f;
+          s += (mk & 4) ? nb[mm][2] : 0.0f;
+          s += (mk & 8) ? nb[mm][3] : 0.0f;
+          const float q = nb[mm][4];
+          const float b = cor ? bv[4 + mm] : bv[mm];
+          const float iv = cor ? inv[4 + mm] : inv[mm];
+          tile[li[mm] + dc] = q + ((s + b) * iv - q);
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// ---------------------------------------------------------------- grid-level smoother
+// suavizar (js/pressao-cpu.js:99-150) for one 16x16 block, by one warp.  Lane l owns the
+// cells t = l + 32m (m = 0..7) of the block: column t & 15, row t >> 4.  With PROL the
+// snapshot is x + P(x_coarse) (prolongar, js/pressao-cpu.js:191-214) built while loading.
+template <class T, bool PROL>
+__device__ __forceinline__ void suavizarBloco(const NivelF n, int blk, int nbx, int desl, int ordem, const T* src,
+                                              T* dst, float* area, const NivelF g, const float* xcSecao) {
+  const int lane = threadIdx.x & 31;
+  const int bx = blk % nbx, by = blk / nbx;
+  const int ox = bx * 16 - desl, oy = by * 16 - desl;
+  const int nx = n.nx, ny = n.ny;
+  float* tile = area;
+  // The tile's loads go out as one batch (registers first, shared memory after): a
+  // load-then-store loop would wait for each L2 round trip in turn.
+  float tv[11];
+  int tz[11];
+#pragma unroll
+  for (int k = 0; k < 11; k++) {
+    const int s = lane + 32 * k;
+    const int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
+    const bool ok = s < TILE && sx >= 0 && sy >= 0 && sx < nx && sy < ny;
+    tv[k] = ok ? carregar(ldcg(src + sx + sy * nx)) : 0.0f;
+    if (PROL) tz[k] = ok ? ldcg8(n.viz + sx + sy * nx) : 0;
+  }
+  if (PROL) {
+    // coarse tile: columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11, water x or 0
+    float* ct = area + TILE;
+    const int cx0 = (ox - 2) >> 1, cy0 = (oy - 2) >> 1;
+    float cv[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int s = lane + 32 * k;
+      const int I = cx0 + s % 11, J = cy0 + s / 11;
+      float v = 0.0f;
+      if (s < CT && I >= 0 && J >= 0 && I < g.nx && J < g.ny) {
+        const int C = I + J * g.nx;
+        const int gv = ldcg8(g.viz + C);
+        const float xv = xcSecao ? __ldcg(xcSecao + C) : lerN(g.meia, g.x, C);
+        v = (gv & 16) ? xv : 0.0f;
+      }
+      cv[k] = v;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int s = lane + 32 * k;
+      if (s < CT) ct[s] = cv[k];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 11; k++) {
+      const int s = lane + 32 * k;
+      if (s < TILE && (tz[k] & 16)) {
+        const int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
+        const int I0 = grossoBaseF(sx) - cx0, J0 = grossoBaseF(sy) - cy0;
+        const float wx0 = pesoBaseF(sx), wy0 = pesoBaseF(sy);
+        float e = 0.0f;
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+          const float wy = b ? 1.0f - wy0 : wy0;
+#pragma unroll
+          for (int aa = 0; aa < 2; aa++) e += ct[(J0 + b) * 11 + I0 + aa] * ((aa ? 1.0f - wx0 : wx0) * wy);
+        }
+        tv[k] = tv[k] + e;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 11; k++) {
+    const int s = lane + 32 * k;
+    if (s < TILE) tile[s] = tv[k];
+  }
+  int vz[8];
+  float bv[8];
+  const T* b = (const T*)n.b;
+#pragma unroll
+  for (int m = 0; m < 8; m++) {
+    int t = celulaBloco(lane, m);
+    int gx = ox + (t & 15), gy = oy + (t >> 4);
+    bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
+    int c = gx + gy * nx;
+    vz[m] = dentro ? (ldcg8(n.viz + c) | 128) : 0;
+    bv[m] = dentro ? carregar(ldcg(b + c)) : 0.0f;
+  }
+  __syncwarp();
+  varrerTile(tile, vz, bv, ordem);
+#pragma unroll
+  for (int m = 0; m < 8; m++) {
+    if (!(vz[m] & 128)) continue;
+    int t = celulaBloco(lane, m);
+    int gx = ox + (t & 15), gy = oy + (t >> 4);
+    int li = ((t >> 4) + 1) * 18 + (t & 15) + 1;
+    dst[gx + gy * nx] = guardar<T>((vz[m] & 16) ? tile[li] : 0.0f);
+  }
+  __syncwarp();
+}
+
+template <class T, bool PROL>
+__device__ void faseSuavizarT(const Args& a, int l, int desl, int ordem, bool paraTmp, float* areas) {
+  const NivelF n = a.niv[l];
+  const int nbx = (n.nx + desl + 15) >> 4, nby = (n.ny + desl + 15) >> 4;
+  const int nb = nbx * nby;
+  const int w = threadIdx.x >> 5;
+  float* area = areas + w * SUAV_W;
+  const T* src = (const T*)(paraTmp ? n.x : n.tmp);
+  T* dst = (T*)(paraTmp ? n.tmp : n.x);
+  NivelF g{};
+  if (PROL) g = a.niv[l + 1];
+  const float* xcSecao = (PROL && l + 1 == a.Lc) ? a.xc : nullptr;
+  for (int blk = w * gridDim.x + blockIdx.x; blk < nb; blk += WARPS * gridDim.x)
+    suavizarBloco<T, PROL>(n, blk, nbx, desl, ordem, src, dst, area, g, xcSecao);
+}
+
+template <class T>
+__device__ void faseSuavizar(const Args& a, int l, int desl, int ordem, bool paraTmp, bool prol, float* areas,
+                             int meia) {
+  if (meia) {
+    if (prol) faseSuavizarT<T, true>(a, l, desl, ordem, paraTmp, areas);
+    else faseSuavizarT<T, false>(a, l, desl, ordem, paraTmp, areas);
+  } else {
+    if (prol) faseSuavizarT<float, true>(a, l, desl, ordem, paraTmp, areas);
+    else faseSuavizarT<float, false>(a, l, desl, ordem, paraTmp, areas);
+  }
+}
+
+// ---------------------------------------------------------------- restriction
+// restringir (js/pressao-cpu.js:159-188) as a gather, one warp per 32-cell coarse row
+// segment: the fine footprint (x on 6 rows x 68 columns; b and flags on 4 x 66) is staged in
+// the warp's shared area, residuals computed once, then each lane sums its 4x4 window.
+__device__ void faseRestringir(const Args& a, int l, float* areas) {
+  const NivelF f = a.niv[l];
+  const NivelF g = a.niv[l + 1];
+  const bool secao = l + 1 == a.Lc;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float* xs = areas + w * REST_W;
+  float* bs = xs + RX;
+  float* rs = bs + RB;
+  uint8_t* vs = (uint8_t*)(rs + RB);
+  const float pes[4] = {0.25f, 0.75f, 0.75f, 0.25f};
+  const int nseg = (g.nx + 31) >> 5;
+  const int total = nseg * g.ny;
+  for (int seg = w * gridDim.x + blockIdx.x; seg < total; seg += WARPS * gridDim.x) {
+    const int J = seg / nseg, I0 = (seg % nseg) * 32;
+    const int fi0 = 2 * I0 - 2, fj0 = 2 * J - 2;  // x window origin (fine)
+    const int I = I0 + lane;
+    const int gvz = I < g.nx ? ldcg8(g.viz + I + J * g.nx) : 0;
+    // staging loads issued as one batch per array (registers, then shared memory)
+    {
+      float xv[13];
+#pragma unroll
+      for (int k = 0; k < 13; k++) {
+        const int s = lane + 32 * k;
+        const int i = fi0 + s % 68, j = fj0 + s / 68;
+        xv[k] = (s < RX && i >= 0 && j >= 0 && i < f.nx && j < f.ny) ? lerN(f.meia, f.x, i + j * f.nx) : 0.0f;
+      }
+      float bv[9];
+      int vv[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        const int s = lane + 32 * k;
+        const int i = fi0 + 1 + s % 66, j = fj0 + 1 + s / 66;
+        const bool d = s < RB && i >= 0 && j >= 0 && i < f.nx && j < f.ny;
+        const int c = i + j * f.nx;
+        vv[k] = d ? ldcg8(f.viz + c) : 0;
+        bv[k] = d ? lerN(f.meia, f.b, c) : 0.0f;
+      }
+#pragma unroll
+      for (int k = 0; k < 13; k++) {
+        const int s = lane + 32 * k;
+        if (s < RX) xs[s] = xv[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        const int s = lane + 32 * k;
+        if (s < RB) {
+          vs[s] = (uint8_t)vv[k];
+          bs[s] = bv[k];
+        }
+      }
+    }
+    __syncwarp();
+    for (int s = lane; s < RB; s += 32) {
+      int rr = s / 66, cc = s % 66;
+      int vz = vs[s];
+      float r = 0.0f;
+      if (vz & 16) {
+        const float* xc = xs + (rr + 1) * 68 + cc + 1;
+        float t = 0.0f;
+        if (vz & 1) t += xc[-1];
+        if (vz & 2) t += xc[1];
+        if (vz & 4) t += xc[-68];
+        if (vz & 8) t += xc[68];
+        r = bs[s] - ((float)__popc(vz & 15) * xc[0] - t);
+      }
+      rs[s] = r;
+    }
+    __syncwarp();
+    if (I < g.nx) {
+      const int C = I + J * g.nx;
+      float soma = 0.0f;
+      if (gvz & 16) {
+#pragma unroll
+        for (int bb = 0; bb < 4; bb++)
+#pragma unroll
+          for (int aa = 0; aa < 4; aa++) soma += rs[bb * 66 + 2 * lane + aa] * (pes[aa] * pes[bb]);
+      }
+      if (secao) a.bc[C] = soma;
+      else {
+        gravarN(g.meia, g.b, C, soma);
+        gravarN(g.meia, g.x, C, 0.0f);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- coarse section (CTA 0)
+// Level arrays live in CTA 0's dynamic shared memory and are addressed by offsets from the
+// `extern __shared__` array, so every access compiles to a shared-memory access.
+struct NivelS {
+  int nx, ny;
+  int xa, xb, b;  // float offsets
+  int v;          // byte offset
+};
+
+// One smoother pass over a level held in shared memory: the level's 16x16 blocks are taken in
+// turn by the CTA's warps, each sweeping a tile read from `src` (varrerTile) and writing `dst`.
+__device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int ordem, int src, int dst,
+                       float* tile) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nx = n.nx, ny = n.ny;
+  const int nbx = (nx + desl + 15) >> 4, nby = (ny + desl + 15) >> 4;
+  for (int blk = w; blk < nbx * nby; blk += WARPS) {
+    const int ox = (blk % nbx) * 16 - desl, oy = (blk / nbx) * 16 - desl;
+#pragma unroll
+    for (int k = 0; k < 11; k++) {
+      const int s = lane + 32 * k;
+      if (s < TILE) {
+        const int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
+        tile[s] = (sx >= 0 && sy >= 0 && sx < nx && sy < ny) ? F[src + sx + sy * nx] : 0.0f;
+      }
+    }
+    int vz[8];
+    float bv[8];
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      const int t = celulaBloco(lane, m);
+      const int gx = ox + (t & 15), gy = oy + (t >> 4);
+      const bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
+      const int c = gx + gy * nx;
+      vz[m] = dentro ? (U[n.v + c] | 128) : 0;
+      bv[m] = dentro ? F[n.b + c] : 0.0f;
+    }
+    __syncwarp();
+    varrerTile(tile, vz, bv, ordem);
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      if (!(vz[m] & 128)) continue;
+      const int t = celulaBloco(lane, m);
+      const int gx = ox + (t & 15), gy = oy + (t >> 4);
+      F[dst + gx + gy * nx] = (vz[m] & 16) ? tile[((t >> 4) + 1) * 18 + (t & 15) + 1] : 0.0f;
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+}
+
+// Stamp of the coarse-section trace (CTA 0, thread 0, when tracing).
+__device__ __forceinline__ void marcaSecao(const Args& a) {
+  if (a.perfil && threadIdx.x == 0) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    unsigned long long* base = a.perfil + PERFIL_MAX + 1;
+    unsigned long long k = base[0]++;
+    if (k < PERFIL_SECAO) base[1 + k] = t;
+  }
+}
+
+// Levels Lc..L-1 of the V-cycle inside CTA 0: loads b of level Lc (a.bc), runs the down
+// passes and restrictions, the coarsest red-black solve (one warp), the prolongations and up
+// passes, and stores x of level Lc (a.xc).
+__device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, NivelS* s, int* tileOff) {
+  float* F = (float*)smem;
+  uint8_t* U = smem;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  marcaSecao(a);
+  if (threadIdx.x == 0) {
+    int off = 0;  // bytes
+    for (int l = a.Lc; l < a.L; l++) {
+      const NivelF n = a.niv[l];
+      const int N = n.nx * n.ny;
+      NivelS& t = s[l];
+      t.nx = n.nx;
+      t.ny = n.ny;
+      t.xa = off / 4;
+      off += (N * 4 + 15) & ~15;
+      t.xb = off / 4;
+      off += (N * 4 + 15) & ~15;
+      t.b = off / 4;
+      off += (N * 4 + 15) & ~15;
+      t.v = off;
+      off += (N + 15) & ~15;
+    }
+    *tileOff = off;
+  }
+  __syncthreads();
+  float* tile = (float*)(smem + *tileOff) + w * TILE;
+  for (int l = a.Lc; l < a.L; l++) {
+    const NivelS t = s[l];
+    const uint8_t* viz = a.niv[l].viz;
+    const int N = t.nx * t.ny;
+    for (int c0 = 0; c0 < N; c0 += 4 * TF) {  // loads in batches of 4 per thread
+      int vv[4];
+      float bb[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int c = c0 + threadIdx.x + k * TF;
+        vv[k] = c < N ? ldcg8(viz + c) : 0;
+        bb[k] = (c < N && l == a.Lc) ? __ldcg(a.bc + c) : 0.0f;
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int c = c0 + threadIdx.x + k * TF;
+        if (c < N) {
+          U[t.v + c] = (uint8_t)vv[k];
+          F[t.xa + c] = 0.0f;
+          if (l == a.Lc) F[t.b + c] = bb[k];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  marcaSecao(a);
+  const float pes[4] = {0.25f, 0.75f, 0.75f, 0.25f};
+  for (int l = a.Lc; l < a.L - 1; l++) {
+    const NivelS f = s[l];
+    const NivelS g = s[l + 1];
+    passoS(F, U, f, 0, 0, f.xa, f.xb, tile);
+    marcaSecao(a);
+    passoS(F, U, f, 8, 0, f.xb, f.xa, tile);
+    marcaSecao(a);
+    // restringir: residuals of the fine level into its free x buffer, then the 4x4 gathers.
+    // Out-of-range and dry neighbours enter with weight or value 0, which adds +0 to a sum.
+    {
+      const int Nf = f.nx * f.ny;
+      const float* x = F + f.xa;
+      for (int c = threadIdx.x; c < Nf; c += TF) {
+        const int vz = U[f.v + c];
+        const float a0 = x[(vz & 1) ? c - 1 : c], a1 = x[(vz & 2) ? c + 1 : c];
+        const float a2 = x[(vz & 4) ? c - f.nx : c], a3 = x[(vz & 8) ? c + f.nx : c];
+        const float xc = x[c], bc = F[f.b + c];
+        float t = 0.0f;
+        t += (vz & 1) ? a0 : 0.0f;
+        t += (vz & 2) ? a1 : 0.0f;
+        t += (vz & 4) ? a2 : 0.0f;
+        t += (vz & 8) ? a3 : 0.0f;
+        F[f.xb + c] = (vz & 16) ? bc - ((float)__popc(vz & 15) * xc - t) : 0.0f;
+      }
+      __syncthreads();
+      const float* r = F + f.xb;
+      for (int C = threadIdx.x; C < g.nx * g.ny; C += TF) {
+        const int I = C % g.nx, J = C / g.nx;
+        float rv[16];
+#pragma unroll
+        for (int bb = 0; bb < 4; bb++) {
+          const int j = min(max(2 * J - 1 + bb, 0), f.ny - 1);
+#pragma unroll
+          for (int aa = 0; aa < 4; aa++) rv[bb * 4 + aa] = r[min(max(2 * I - 1 + aa, 0), f.nx - 1) + j * f.nx];
+        }
+        float sum = 0.0f;
+#pragma unroll
+        for (int bb = 0; bb < 4; bb++) {
+          const int j = 2 * J - 1 + bb;
+#pragma unroll
+          for (int aa = 0; aa < 4; aa++) {
+            const int i = 2 * I - 1 + aa;
+            const bool dentro = i >= 0 && j >= 0 && i < f.nx && j < f.ny;
+            sum += dentro ? rv[bb * 4 + aa] * (pes[aa] * pes[bb]) : 0.0f;
+          }
+        }
+        F[g.b + C] = (U[g.v + C] & 16) ? sum : 0.0f;
+        F[g.xa + C] = 0.0f;
+      }
+    }
+    __syncthreads();
+    marcaSecao(a);
+  }
+  if (w == 0) {  // resolverGrosso (js/pressao-cpu.js:217-238), one warp
+    const NivelS n = s[a.L - 1];
+    const int nx = n.nx, N = n.nx * n.ny;
+    float* x = F + n.xa;
+    // The cells that change (water with a free neighbour), listed per colour in the free x
+    // buffer as cell | mask << 24, colour 0 first.
+    int* lista = (int*)(F + n.xb);
+    int cont[2];
+#pragma unroll
+    for (int cor = 0; cor < 2; cor++) {
+      int base = cor ? cont[0] : 0;
+      for (int c0 = 0; c0 < N; c0 += 32) {
+        const int c = c0 + lane;
+        const int vz = c < N ? U[n.v + c] : 0;
+        const bool ok = c < N && (vz & 16) && (vz & 15) && ((((c % nx) + (c / nx) + 1) & 1) == cor);
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (ok) lista[base + __popc(m & ((1u << lane) - 1u))] = c | ((vz & 15) << 24);
+        base += __popc(m);
+      }
+      cont[cor] = base - (cor ? cont[0] : 0);
+    }
+    __syncwarp();
+    for (int k = 0; k < VARREDURAS_GROSSO; k++)
+      for (int o = 0; o < 2; o++) {
+        const int cor = (k & 1) ? 1 - o : o;
+        const int ini = cor ? cont[0] : 0, n_ = cor ? cont[1] : cont[0];
+        for (int e0 = 0; e0 < n_; e0 += 64) {
+          const int eA = e0 + lane, eB = e0 + 32 + lane;
+          const int EA = eA < n_ ? lista[ini + eA] : -1, EB = eB < n_ ? lista[ini + eB] : -1;
+          float va[5], vb[5];
+          {  // an idle lane (entry -1) reads cell 0
+            const int c = EA < 0 ? 0 : EA & 0xffffff, mk = EA < 0 ? 0 : EA >> 24;
+            va[0] = x[(mk & 1) ? c - 1 : c];
+            va[1] = x[(mk & 2) ? c + 1 : c];
+            va[2] = x[(mk & 4) ? c - nx : c];
+            va[3] = x[(mk & 8) ? c + nx : c];
+            va[4] = F[n.b + c];
+          }
+          {
+            const int c = EB < 0 ? 0 : EB & 0xffffff, mk = EB < 0 ? 0 : EB >> 24;
+            vb[0] = x[(mk & 1) ? c - 1 : c];
+            vb[1] = x[(mk & 2) ? c + 1 : c];
+            vb[2] = x[(mk & 4) ? c - nx : c];
+            vb[3] = x[(mk & 8) ? c + nx : c];
+            vb[4] = F[n.b + c];
+          }
+          if (EA >= 0) {
+            const int mk = EA >> 24;
+            float t = 0.0f;
+            t += (mk & 1) ? va[0] : 0.0f;
+            t += (mk & 2) ? va[1] : 0.0f;
+            t += (mk & 4) ? va[2] : 0.0f;
+            t += (mk & 8) ? va[3] : 0.0f;
+            x[EA & 0xffffff] = (t + va[4]) * inversoVizinhos(__popc(mk));
+          }
+          if (EB >= 0) {
+            const int mk = EB >> 24;
+            float t = 0.0f;
+            t += (mk & 1) ? vb[0] : 0.0f;
+            t += (mk & 2) ? vb[1] : 0.0f;
+            t += (mk & 4) ? vb[2] : 0.0f;
+            t += (mk & 8) ? vb[3] : 0.0f;
+            x[EB & 0xffffff] = (t + vb[4]) * inversoVizinhos(__popc(mk));
+          }
+        }
+        __syncwarp();
+      }
+  }
+  __syncthreads();
+  marcaSecao(a);
+  for (int l = a.L - 2; l >= a.Lc; l--) {
+    const NivelS g = s[l + 1];
+    const NivelS f = s[l];
+    // prolongar: coarse x is 0 on every dry coarse cell, out-of-range corners get weight 0
+    for (int c = threadIdx.x; c < f.nx * f.ny; c += TF) {
+      const int i = c % f.nx, j = c / f.nx;
+      const int I0 = grossoBaseF(i), J0 = grossoBaseF(j);
+      const float wx0 = pesoBaseF(i), wy0 = pesoBaseF(j);
+      float gv[4];
+#pragma unroll
+      for (int b = 0; b < 2; b++) {
+        const int J = min(max(J0 + b, 0), g.ny - 1);
+#pragma unroll
+        for (int aa = 0; aa < 2; aa++) gv[b * 2 + aa] = F[g.xa + min(max(I0 + aa, 0), g.nx - 1) + J * g.nx];
+      }
+      const float xf = F[f.xa + c];
+      float e = 0.0f;
+#pragma unroll
+      for (int b = 0; b < 2; b++) {
+        const int J = J0 + b;
+        const float wy = b ? 1.0f - wy0 : wy0;
+#pragma unroll
+        for (int aa = 0; aa < 2; aa++) {
+          const int I = I0 + aa;
+          const bool dentro = I >= 0 && J >= 0 && I < g.nx && J < g.ny;
+          e += dentro ? gv[b * 2 + aa] * ((aa ? 1.0f - wx0 : wx0) * wy) : 0.0f;
+        }
+      }
+      if (U[f.v + c] & 16) F[f.xa + c] = xf + e;
+    }
+    __syncthreads();
+    marcaSecao(a);
+    passoS(F, U, f, 8, 1, f.xa, f.xb, tile);
+    marcaSecao(a);
+    passoS(F, U, f, 0, 1, f.xb, f.xa, tile);
+    marcaSecao(a);
+  }
+  const NivelS t = s[a.Lc];
+  const int Nc = t.nx * t.ny;
+  for (int c = threadIdx.x; c < Nc; c += TF) a.xc[c] = F[t.xa + c];
+}
+
+// ---------------------------------------------------------------- the V-cycle
+template <class T>
+__device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char* smem, NivelS* tabS, int* tileOff) {
+  for (int l = 0; l < a.Lc; l++) {
+    const int meia = a.niv[l].meia;
+    faseSuavizar<T>(a, l, 0, 0, true, false, areas, meia);
+    if (!barreira(a, ep)) return false;
+    faseSuavizar<T>(a, l, 8, 0, false, false, areas, meia);
+    if (!barreira(a, ep)) return false;
+    faseRestringir(a, l, areas);
+    if (!barreira(a, ep)) return false;
+  }
+  if (blockIdx.x == 0) secaoGrossa(a, smem, tabS, tileOff);
+  if (!barreira(a, ep)) return false;
+  for (int l = a.Lc - 1; l >= 0; l--) {
+    const int meia = a.niv[l].meia;
+    faseSuavizar<T>(a, l, 8, 1, true, true, areas, meia);  // prolongation folded in
+    if (!barreira(a, ep)) return false;
+    faseSuavizar<T>(a, l, 0, 1, false, false, areas, meia);
+    if (!barreira(a, ep)) return false;
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------- PCG pieces
+// A*v at water cell c (js/pressao-cpu.js:84-93 after difundir): neighbours that are water give
+// val(n), active-bubble air gives valB(label), anything else 0.
+template <class FV, class FB>
+__device__ __forceinline__ float aplicarF(const Args& a, int c, FV val, FB valB) {
+  const Dev& d = a.d;
+  const int vz = ldcg8(a.vizOp + c);
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (!(vz & (1 << k))) continue;
+    const int n = k == 0 ? c - 1 : k == 1 ? c + 1 : k == 2 ? c - d.nx : c + d.nx;
+    const int t = ldcg8(d.tipo + n);
+    if (t == AGUA) s += val(n);
+    else if (a.bolhas && t == AR) {
+      uint32_t r = __ldcg(d.rotulo + n);
+      if (bolhaAtiva(a, r)) s += valB(r);
+    }
+  }
+  return (float)__popc(vz & 15) * val(c) - s;
+}
+
+// Spreads the residual into the V-cycle's level-0 right-hand side (precondicionar,
+// js/pressao-cpu.js:353-355) and zeroes level-0 x.  rb is read from d.rb.
+__device__ void faseEspalhar(const Args& a, const NivelF& n0, float escala) {
+  const Dev& d = a.d;
+  for (int c = blockIdx.x * TF + threadIdx.x; c < d.N; c += gridDim.x * TF) {
+    float v = __ldcg(d.r + c);
+    if (a.bolhas && ldcg8(d.tipo + c) == AR) {
+      uint32_t b = __ldcg(d.rotulo + c);
+      if (b >= 2 && b < (uint32_t)MAX_BOLHAS) {
+        unsigned cels = __ldcg(d.celsB + b);
+        if (cels > 0) v = (float)(__ldcg(d.rb + b) / cels);
+      }
+    }
+    gravarN(n0.meia, n0.b, c, v * escala);
+    gravarN(n0.meia, n0.x, c, 0.0f);
+  }
+}
+
+// Gathers z from the V-cycle (precondicionar, js/pressao-cpu.js:357-361): z = x/escala except
+// active bubble cells (zeroed; their mean correction accumulates into accZ); partials of r.z
+// (channel 0) and r.zOld (channel 1).
+__device__ void faseJuntar(const Args& a, const NivelF& n0, float invEscala, float* zNovo, const float* zVelho,
+                           double* sh) {
+  const Dev& d = a.d;
+  double s0 = 0, s1 = 0;
+  for (int c = blockIdx.x * TF + threadIdx.x; c < d.N; c += gridDim.x * TF) {
+    float x = lerN(n0.meia, n0.x, c) * invEscala;
+    const int t = ldcg8(d.tipo + c);
+    if (a.bolhas && t == AR) {
+      uint32_t b = __ldcg(d.rotulo + c);
+      if (b >= 2 && b < (uint32_t)MAX_BOLHAS) {
+        unsigned cels = __ldcg(d.celsB + b);
+        if (cels > 0) {
+          somaFixa(&a.accZ[b], (double)x / cels, ESC);
+          zNovo[c] = 0.0f;
+          continue;
+        }
+      }
+    }
+    zNovo[c] = x;
+    if (t == AGUA) {
+      double r = __ldcg(d.r + c);
+      s0 += r * (double)x;
+      if (zVelho) s1 += r * (double)__ldcg(zVelho + c);
+    }
+  }
+  double t0 = somaBloco(s0, sh);
+  double t1 = somaBloco(s1, sh);
+  if (threadIdx.x == 0) {
+    a.parc[blockIdx.x * NPARC + 0] = t0;
+    a.parc[blockIdx.x * NPARC + 1] = t1;
+  }
+}
+
+// ---------------------------------------------------------------- the kernel
+template <class T>
+__global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a) {
+  extern __shared__ __align__(16) unsigned char dyn[];
+  __shared__ double sh[32];
+  __shared__ NivelS tabS[MAX_NIVEIS];
+  __shared__ int tileOff;
+  float* areas = (float*)dyn;
+  const Dev& d = a.d;
+  const int N = d.N, nx = d.nx, ny = d.ny;
+  const int gt0 = blockIdx.x * TF + threadIdx.x;
+  const int GT = gridDim.x * TF;
+  unsigned ep = 0;
+  double somas[4];
+
+  // ---- setup: level-0 preconditioner types, operator masks, bubble faces
+  {
+    uint8_t* t0 = a.niv[0].tipo;
+    for (int c = gt0; c < N; c += GT) {
+      const int t = d.tipo[c];
+      const uint32_t rot = d.rotulo[c];
+      t0[c] = (a.bolhas && t == AR && rot >= 2) ? AGUA : (uint8_t)t;
+      const int i = c % nx, j = c / nx;
+      int m = 0;
+      if (i > 0 && d.tipo[c - 1] != SOLIDO) m |= 1;
+      if (i < nx - 1 && d.tipo[c + 1] != SOLIDO) m |= 2;
+      if (j > 0 && d.tipo[c - nx] != SOLIDO) m |= 4;
+      if (j < ny - 1 && d.tipo[c + nx] != SOLIDO) m |= 8;
+      if (t == AGUA) m |= 16;
+      a.vizOp[c] = (uint8_t)m;
+      if (a.bolhas && t == AR && rot >= 2 && rot < (uint32_t)MAX_BOLHAS && i >= 1 && j >= 1 && i < nx - 1 &&
+          j < ny - 1) {
+        unsigned k = (d.tipo[c - 1] == AGUA) + (d.tipo[c + 1] == AGUA) + (d.tipo[c - nx] == AGUA) +
+                     (d.tipo[c + nx] == AGUA);
+        if (k) atomicAdd(&d.facesB[rot], k);
+      }
+    }
+  }
+  if (!barreira(a, ep)) return;
+  // ---- coarse types (tiposGrossos, js/pressao-cpu.js:63-81), one level per phase
+  for (int l = 1; l < a.L; l++) {
+    const NivelF f = a.niv[l - 1];
+    const NivelF g = a.niv[l];
+    for (int C = gt0; C < g.nx * g.ny; C += GT) {
+      const int I = C % g.nx, J = C / g.nx;
+      bool ar = false, agua = false;
+      for (int b = 0; b < 2; b++)
+        for (int aa = 0; aa < 2; aa++) {
+          int i = 2 * I + aa, j = 2 * J + b;
+          if (i >= f.nx || j >= f.ny) continue;
+          int t = ldcg8(f.tipo + i + j * f.nx);
+          if (t == AR) ar = true;
+          else if (t == AGUA) agua = true;
+        }
+      g.tipo[C] = ar ? AR : agua ? AGUA : SOLIDO;
+    }
+    if (!barreira(a, ep)) return;
+  }
+  // ---- neighbour masks of every level, bubble cell counts, active list, initial y
+  for (int l = 0; l < a.L; l++) {
+    const NivelF n = a.niv[l];
+    for (int c = gt0; c < n.nx * n.ny; c += GT) {
+      const int i = c % n.nx, j = c / n.nx;
+      const uint8_t* tp = n.tipo;
+      int m = 0;
+      if (i > 0 && ldcg8(tp + c - 1) != SOLIDO) m |= 1;
+      if (i < n.nx - 1 && ldcg8(tp + c + 1) != SOLIDO) m |= 2;
+      if (j > 0 && ldcg8(tp + c - n.nx) != SOLIDO) m |= 4;
+      if (j < n.ny - 1 && ldcg8(tp + c + n.nx) != SOLIDO) m |= 8;
+      if (ldcg8(tp + c) == AGUA) m |= 16;
+      n.viz[c] = (uint8_t)m;
+    }
+  }
+  if (a.bolhas) {
+    for (int c = gt0; c < N; c += GT) {
+      uint32_t b = d.rotulo[c];
+      if (b >= 2 && b < (uint32_t)MAX_BOLHAS && d.tipo[c] == AR && __ldcg(&d.facesB[b]) > 0)
+        atomicAdd(&d.celsB[b], 1u);
+    }
+    if (blockIdx.x == 0) {
+      if (threadIdx.x < 32) {  // active labels in ascending order (one warp, ballot-compacted)
+        int base = 0;
+        for (int b0 = 0; b0 < MAX_BOLHAS; b0 += 32) {
+          int b = b0 + threadIdx.x;
+          bool at = b >= 2 && __ldcg(&d.facesB[b]) > 0;
+          unsigned m = __ballot_sync(0xffffffffu, at);
+          if (at) a.ativos[base + __popc(m & ((1u << threadIdx.x) - 1u))] = b;
+          base += __popc(m);
+        }
+        if (threadIdx.x == 0) *a.nAtivos = base;
+      }
+      for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) {
+        bool at = b >= 2 && __ldcg(&d.facesB[b]) > 0;
+        d.yB[b] = at ? (double)d.yBolhaF[b] : 0.0;
+        d.rb[b] = 0.0;
+        d.zb[b] = a.zb2[b] = 0.0;
+        d.pb[b] = a.pb2[b] = 0.0;
+      }
+    }
+  } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *a.nAtivos = 0;
+  }
+  if (!barreira(a, ep)) return;
+  const int nAt = a.bolhas ? __ldcg(a.nAtivos) : 0;
+  const NivelF n0 = a.niv[0];
+
+  // ---- r = -div - A q (js/pressao-cpu.js:331-338), bubble aq sums
+  {
+    double s = 0;
+    for (int c = gt0; c < N; c += GT) {
+      if (d.tipo[c] != AGUA) {
+        d.q[c] = 0.0f;
+        d.r[c] = 0.0f;
+        continue;
+      }
+      float ar = aplicarF(a, c, [&](int n) { return __ldcg(d.q + n); },
+                          [&](uint32_t r) { return (float)__ldcg(d.yB + r); });
+      float rv = -d.div[c] - ar;
+      d.r[c] = rv;
+      s += (double)rv * rv;
+    }
+    if (a.bolhas)
+      for (int c = gt0; c < N; c += GT) {
+        const int i = c % nx, j = c / nx;
+        if (i < 1 || j < 1 || i >= nx - 1 || j >= ny - 1) continue;
+        uint32_t b = d.rotulo[c];
+        if (d.tipo[c] != AR || !bolhaAtiva(a, b)) continue;
+        double t = 0;
+        if (d.tipo[c - 1] == AGUA) t += (double)__ldcg(d.q + c - 1);
+        if (d.tipo[c + 1] == AGUA) t += (double)__ldcg(d.q + c + 1);
+        if (d.tipo[c - nx] == AGUA) t += (double)__ldcg(d.q + c - nx);
+        if (d.tipo[c + nx] == AGUA) t += (double)__ldcg(d.q + c + nx);
+        if (t != 0) somaFixa(&d.accB[b], t, ESC);
+      }
+    double tb = somaBloco(s, sh);
+    if (threadIdx.x == 0) {
+      a.parc[blockIdx.x * NPARC + 0] = tb;
+      a.parc[blockIdx.x * NPARC + 1] = 0.0;
+    }
+  }
+  if (!barreira(a, ep)) return;
+  // rb = rhs - (faces*y - sum) (js/pressao-cpu.js:339-341); norm0
+  auto rbInicial = [&](int b) {
+    return (double)d.rhsBolhaF[b] - (__ldcg(&d.facesB[b]) * __ldcg(&d.yB[b]) - (double)__ldcg(&d.accB[b]) / ESC);
+  };
+  somasGlobais(a, nAt, [&](int b) { double v = rbInicial(b); return v * v; }, [](int) { return 0.0; }, sh, somas);
+  const double norma0 = sqrt(somas[0] + somas[2]);
+  if (blockIdx.x == 0) {
+    for (int k = threadIdx.x; k < nAt; k += TF) {
+      int b = __ldcg(&a.ativos[k]);
+      d.rb[b] = rbInicial(b);
+    }
+    if (threadIdx.x == 0) {
+      d.esc->norma0 = d.esc->norma = norma0;
+      d.esc->normas[0] = norma0;
+      d.esc->iters = 0;
+      d.esc->pronto = 0;
+    }
+  }
+  if (!barreira(a, ep)) return;  // rb visible before spreading
+  float escala = (a.escalar && norma0 > 0) ? (float)(1.0 / norma0) : 1.0f;
+  faseEspalhar(a, n0, escala);
+  if (blockIdx.x == 0)
+    for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) {
+      a.accZ[b] = 0;
+      d.accB[b] = 0;
+    }
+  if (!barreira(a, ep)) return;
+  if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff)) return;
+  int cz = 0, cp = 0;  // which of the two z / p buffers holds the latest values
+  faseJuntar(a, n0, 1.0f / escala, d.z, nullptr, sh);
+  if (!barreira(a, ep)) return;
+  auto zbAtual = [&](int b) { return (double)__ldcg(&a.accZ[b]) / ESC; };
+  somasGlobais(a, nAt, [&](int b) { return __ldcg(&d.rb[b]) * zbAtual(b); }, [](int) { return 0.0; }, sh, somas);
+  double rz = somas[0] + somas[2];
+  double beta = 0.0;
+  bool primeira = true;
+
+  for (int it = 0; it < a.iteracoes; it++) {
+    float* zc = cz ? a.z2 : d.z;
+    float* zo = cz ? d.z : a.z2;
+    const float* pv = cp ? a.p2 : d.p;
+    float* pn = cp ? d.p : a.p2;
+    const double* zbOld = cz ? d.zb : a.zb2;
+    double* zbCur = cz ? a.zb2 : d.zb;
+    const double* pbVelho = cp ? a.pb2 : d.pb;
+    double* pbNovo = cp ? d.pb : a.pb2;
+    // ---- [DA] beta, p = z + beta p, A p, p.Ap, bubble rows
+    if (!primeira) {
+      somasGlobais(a, nAt, [&](int b) { return __ldcg(&d.rb[b]) * zbAtual(b); },
+                   [&](int b) { return __ldcg(&d.rb[b]) * __ldcg(&zbOld[b]); }, sh, somas);
+      const double rzNovo = somas[0] + somas[2], cruz = somas[1] + somas[3];
+      beta = fabs(rz) < 1e-30 ? 0.0 : fmax(0.0, (rzNovo - cruz) / rz);
+      rz = rzNovo;
+    }
+    const float betaf = (float)beta;
+    const bool prim = primeira;
+    auto pNovo = [&](int n) { return prim ? __ldcg(zc + n) : __ldcg(zc + n) + betaf * __ldcg(pv + n); };
+    auto pbNovoV = [&](int b) { return prim ? zbAtual(b) : zbAtual(b) + beta * __ldcg(&pbVelho[b]); };
+    if (blockIdx.x == 0)
+      for (int k = threadIdx.x; k < nAt; k += TF) {
+        int b = __ldcg(&a.ativos[k]);
+        zbCur[b] = zbAtual(b);
+        pbNovo[b] = pbNovoV(b);
+      }
+    {
+      double s = 0;
+      for (int c = gt0; c < N; c += GT) {
+        if (d.tipo[c] != AGUA) {
+          pn[c] = 0.0f;
+          d.ap[c] = 0.0f;
+          continue;
+        }
+        const float pc = pNovo(c);
+        pn[c] = pc;
+        const float apc = aplicarF(a, c, pNovo, [&](uint32_t r) { return (float)pbNovoV((int)r); });
+        d.ap[c] = apc;
+        s += (double)pc * apc;
+      }
+      if (a.bolhas)
+        for (int c = gt0; c < N; c += GT) {
+          const int i = c % nx, j = c / nx;
+          if (i < 1 || j < 1 || i >= nx - 1 || j >= ny - 1) continue;
+          uint32_t b = d.rotulo[c];
+          if (d.tipo[c] != AR || !bolhaAtiva(a, b)) continue;
+          double t = 0;
+          if (d.tipo[c - 1] == AGUA) t += (double)pNovo(c - 1);
+          if (d.tipo[c + 1] == AGUA) t += (double)pNovo(c + 1);
+          if (d.tipo[c - nx] == AGUA) t += (double)pNovo(c - nx);
+          if (d.tipo[c + nx] == AGUA) t += (double)pNovo(c + nx);
+          if (t != 0) somaFixa(&d.accB[b], t, ESC);
+        }
+      double tb = somaBloco(s, sh);
+      if (threadIdx.x == 0) a.parc[blockIdx.x * NPARC + 0] = tb;
+    }
+    if (!barreira(a, ep)) return;
+    // ---- [B] alpha; q += alpha p, r -= alpha Ap; bubbles; r.r
+    auto apbV = [&](int b) {
+      return __ldcg(&d.facesB[b]) * __ldcg(&pbNovo[b]) - (double)__ldcg(&d.accB[b]) / ESC;
+    };
+    somasGlobais(a, nAt, [&](int b) { return __ldcg(&pbNovo[b]) * apbV(b); }, [](int) { return 0.0; }, sh, somas);
+    const double pap = somas[0] + somas[2];
+    const double alfa = fabs(pap) < 1e-30 ? 0.0 : rz / pap;
+    {
+      const float af = (float)alfa;
+      double s = 0;
+      for (int c = gt0; c < N; c += GT) {
+        if (d.tipo[c] != AGUA) continue;
+        d.q[c] = d.q[c] + af * __ldcg(pn + c);
+        const float rv = d.r[c] - af * __ldcg(d.ap + c);
+        d.r[c] = rv;
+        s += (double)rv * rv;
+      }
+      if (blockIdx.x == 0) {
+        double sb = 0;
+        for (int k = threadIdx.x; k < nAt; k += TF) {
+          int b = __ldcg(&a.ativos[k]);
+          d.yB[b] += alfa * __ldcg(&pbNovo[b]);
+          double rbn = __ldcg(&d.rb[b]) - alfa * apbV(b);
+          d.rb[b] = rbn;
+          sb += rbn * rbn;
+        }
+        s += sb;
+        for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) a.accZ[b] = 0;
+      }
+      double tb = somaBloco(s, sh);
+      if (threadIdx.x == 0) a.parc[blockIdx.x * NPARC + 0] = tb;
+    }
+    if (!barreira(a, ep)) return;
+    // ---- [C] norm, convergence, spread the residual
+    somasGlobais(a, 0, [](int) { return 0.0; }, [](int) { return 0.0; }, sh, somas);
+    const double norma = sqrt(somas[0]);
+    const bool fim = it == a.iteracoes - 1 || (a.tol > 0 && norma <= a.tol * norma0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (it + 1 < 1024) d.esc->normas[it + 1] = norma;
+      d.esc->iters = it + 1;
+      d.esc->norma = norma;
+      d.esc->pronto = fim ? 1 : 0;
+    }
+    if (fim) break;
+    escala = (a.escalar && norma > 0) ? (float)(1.0 / norma) : 1.0f;
+    faseEspalhar(a, n0, escala);
+    if (blockIdx.x == 0)
+      for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) d.accB[b] = 0;
+    if (!barreira(a, ep)) return;
+    if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff)) return;
+    faseJuntar(a, n0, 1.0f / escala, zo, zc, sh);
+    if (!barreira(a, ep)) return;
+    cz ^= 1;
+    cp ^= 1;
+    primeira = false;
+  }
+  // ---- end: q = 0 off water; bubbles hand back their pressure
+  if (!barreira(a, ep)) return;
+  for (int c = gt0; c < N; c += GT)
+    if (d.tipo[c] != AGUA) d.q[c] = 0.0f;
+  if (blockIdx.x == 0)
+    for (int k = threadIdx.x; k < nAt; k += TF) {
+      int b = __ldcg(&a.ativos[k]);
+      d.yBolhaF[b] = (float)__ldcg(&d.yB[b]);
+    }
+}
+
+// ---------------------------------------------------------------- host side
+template <class T>
+static void* kernelDe() { return (void*)k_mgpcg<T>; }
+
+Fundido* criarFundido(Pcg* p) {
+  if (p->L < 2) return nullptr;  // no coarse level to hand to the coarse section
+  Fundido* f = new Fundido();
+  // coarse section: the longest suffix of levels (not level 0) fitting the shared budget
+  int Lc = p->L;
+  size_t bytes = 0;
+  for (int l = p->L - 1; l >= 1; l--) {
+    size_t n = (size_t)p->nxL[l] * p->nyL[l];
+    size_t b = 3 * ((n * 4 + 15) & ~(size_t)15) + ((n + 15) & ~(size_t)15);
+    if (bytes + b + TILES_SECAO > SMEM_GROSSO_MAX) break;
+    bytes += b;
+    Lc = l;
+  }
+  if (Lc >= p->L) {  // even the coarsest level does not fit
+    delete f;
+    return nullptr;
+  }
+  f->Lc = Lc;
+  size_t porWarp = (size_t)(SUAV_W > REST_W ? SUAV_W : REST_W) * 4;
+  size_t areas = (size_t)WARPS * porWarp;
+  f->smem = bytes + TILES_SECAO > areas ? bytes + TILES_SECAO : areas;
+  f->kern = p->precisao == TQ_PREC_FP16   ? kernelDe<__half>()
+            : p->precisao == TQ_PREC_BF16 ? kernelDe<__nv_bfloat16>()
+                                          : kernelDe<float>();
+  int dev = 0, sms = 0, porSM = 0;
+  bool ok = cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaFuncSetAttribute(f->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f->smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&porSM, f->kern, TF, f->smem) == cudaSuccess && porSM >= 1;
+  if (ok) {
+    f->G = sms;  // one CTA per SM: co-resident, as the grid barrier needs
+    const size_t N = p->N;
+    const size_t nLc = (size_t)p->nxL[Lc] * p->nyL[Lc];
+    ok = cudaMalloc(&f->niveis, MAX_NIVEIS * sizeof(NivelF)) == cudaSuccess &&
+         cudaMalloc(&f->parc, (size_t)f->G * NPARC * sizeof(double)) == cudaSuccess &&
+         cudaMalloc(&f->bar, 2 * sizeof(unsigned)) == cudaSuccess && cudaMalloc(&f->erro, sizeof(int)) == cudaSuccess &&
+         cudaMalloc(&f->accZ, MAX_BOLHAS * sizeof(long long)) == cudaSuccess &&
+         cudaMalloc(&f->zb2, MAX_BOLHAS * sizeof(double)) == cudaSuccess &&
+         cudaMalloc(&f->pb2, MAX_BOLHAS * sizeof(double)) == cudaSuccess &&
+         cudaMalloc(&f->ativos, MAX_BOLHAS * sizeof(int)) == cudaSuccess &&
+         cudaMalloc(&f->nAtivos, sizeof(int)) == cudaSuccess && cudaMalloc(&f->p2, N * 4) == cudaSuccess &&
+         cudaMalloc(&f->z2, N * 4) == cudaSuccess && cudaMalloc(&f->xc, nLc * 4) == cudaSuccess &&
+         cudaMalloc(&f->bc, nLc * 4) == cudaSuccess;
+  }
+  if (ok) {
+    NivelF tab[MAX_NIVEIS] = {};
+    for (int l = 0; l < p->L; l++) {
+      NivelF& n = tab[l];
+      n.nx = p->nxL[l];
+      n.ny = p->nyL[l];
+      n.meia = (l < Lc && p->meia[l]) ? (p->precisao == TQ_PREC_FP16 ? 1 : 2) : 0;
+      n.viz = p->vizL[l];
+      n.tipo = p->tipoL[l];
+      n.b = p->bL[l];
+      n.x = p->xL[l];
+      n.tmp = p->tmpL[l];
+    }
+    ok = cudaMemcpy(f->niveis, tab, sizeof tab, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(f->bar, 0, 2 * sizeof(unsigned)) == cudaSuccess && cudaMemset(f->erro, 0, sizeof(int)) == cudaSuccess;
+  }
+  if (!ok) {
+    cudaGetLastError();
+    destruirFundido(f);
+    return nullptr;
+  }
+  return f;
+}
+
+void destruirFundido(Fundido* f) {
+  if (!f) return;
+  void* ps[] = {f->niveis, f->parc, f->bar, f->erro, f->accZ, f->zb2, f->pb2, f->ativos,
+                f->nAtivos, f->p2, f->z2, f->xc, f->bc, f->perfil};
+  for (void* q : ps)
+    if (q) cudaFree(q);
+  delete f;
+}
+
+int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s) {
+  Fundido* f = p->fundido;
+  Args a{};
+  a.d = d;
+  a.L = p->L;
+  a.Lc = f->Lc;
+  a.niv = f->niveis;
+  a.vizOp = p->vizOp;
+  a.iteracoes = iteracoes;
+  a.tol = tol;
+  a.bolhas = bolhas ? 1 : 0;
+  a.escalar = p->precisao != TQ_PREC_FP32 ? 1 : 0;
+  a.parc = f->parc;
+  a.bar = f->bar;
+  a.erro = f->erro;
+  a.accZ = f->accZ;
+  a.zb2 = f->zb2;
+  a.pb2 = f->pb2;
+  a.ativos = f->ativos;
+  a.nAtivos = f->nAtivos;
+  a.p2 = f->p2;
+  a.z2 = f->z2;
+  a.xc = f->xc;
+  a.bc = f->bc;
+  a.perfil = f->perfilar ? f->perfil : nullptr;
+  if (a.perfil) {
+    cudaMemsetAsync(f->perfil, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(f->perfil + PERFIL_MAX + 1, 0, sizeof(unsigned long long), s);
+  }
+  cudaMemsetAsync(d.facesB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
+  cudaMemsetAsync(d.celsB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
+  cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
+  cudaMemsetAsync(f->bar, 0, 2 * sizeof(unsigned), s);
+  cudaMemsetAsync(f->erro, 0, sizeof(int), s);
+  void* args[] = {&a};
+  contarLancamento();
+  cudaError_t e = cudaLaunchCooperativeKernel(f->kern, dim3(f->G), dim3(TF), args, f->smem, s);
+  if (e != cudaSuccess) return TQ_E_CUDA;
+  int h[2] = {0, 0};
+  if (cudaMemcpyAsync(&h[0], f->erro, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(&h[1], &d.esc->iters, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return TQ_E_CUDA;
+  if (h[0]) return TQ_E_TIMEOUT;
+  p->iters = h[1];
+  p->normas.resize(h[1] + 1);
+  if (cudaMemcpyAsync(p->normas.data(), d.esc->normas, sizeof(double) * (h[1] + 1), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return TQ_E_CUDA;
+  return TQ_OK;
+}
+
+}  // namespace tq

@@ -282,7 +282,6 @@ int tq_create(const tq_options* o, tq_sim** out) {
   if (o->p2g_mode != TQ_P2G_FIXED) return falha(TQ_E_ARG, "the CUDA library implements TQ_P2G_FIXED only");
   if (o->precision < TQ_PREC_FP32 || o->precision > TQ_PREC_BF16) return falha(TQ_E_ARG, "bad precision");
   if (o->engine != TQ_ENGINE_PLAIN && o->engine != TQ_ENGINE_FUSED) return falha(TQ_E_ARG, "bad engine");
-  if (o->engine == TQ_ENGINE_FUSED) return falha(TQ_E_ARG, "fused engine not available in this build");
   int st = iniciarCuda(o->device);
   if (st) return st;
   tq_sim* s = new (std::nothrow) tq_sim();
@@ -683,6 +682,7 @@ int tq_set_timing(tq_sim* s, int32_t on) {
   if (!s) return falha(TQ_E_ARG, "null handle");
   CK(cudaStreamSynchronize(s->s));
   s->timing = on != 0;
+  perfilPcg(s->pcg, on >= 2);
   s->usados = 0;
   s->regSub.clear();
   s->regAr.clear();
@@ -719,6 +719,17 @@ int tq_get_timing(tq_sim* s, double* ms, int32_t cap, int32_t* n) {
   if (n) *n = 11;
   if (ms)
     for (int i = 0; i < 11 && i < cap; i++) ms[i] = v[i];
+  return TQ_OK;
+}
+
+int tq_get_phase_trace(tq_sim* s, uint64_t* out, int32_t cap, int32_t* n) {
+  if (!s) return falha(TQ_E_ARG, "null handle");
+  CK(cudaStreamSynchronize(s->s));
+  std::vector<unsigned long long> tmp(cap > 0 ? cap : -cap);
+  int k = cap != 0 ? lerPerfilPcg(s->pcg, tmp.data(), cap) : 0;
+  if (n) *n = k;
+  if (out)
+    for (int i = 0; i < k; i++) out[i] = tmp[i];
   return TQ_OK;
 }
 

@@ -78,9 +78,13 @@ def test_ciclo_v_tamanhos(lib_gpu, nx, ny):
 
 
 # ------------------------------------------------------------------ PCG
+MOTORES = [pytest.param(_abi.TQ_ENGINE_PLAIN, id="plain"), pytest.param(_abi.TQ_ENGINE_FUSED, id="fused")]
+
+
+@pytest.mark.parametrize("motor", MOTORES)
 @pytest.mark.parametrize("nome", ["barragem", "bolha", "copo"])
 @pytest.mark.parametrize("com_bolhas", [False, True], ids=["sem-bolhas", "com-bolhas"])
-def test_pcg_iteracoes_fixas(lib_gpu, nome, com_bolhas):
+def test_pcg_iteracoes_fixas(lib_gpu, nome, com_bolhas, motor):
     tipo, div, rot, o = problema_de_pressao(nome)
     q0 = np.zeros(tipo.size, np.float32)
     bol_o = bol_g = None
@@ -91,7 +95,7 @@ def test_pcg_iteracoes_fixas(lib_gpu, nome, com_bolhas):
         bol_g = dict(rotulo=rot.copy(), rhs=rhs.copy(), y=y.copy())
     q_o, q_g = q0.copy(), q0.copy()
     n_o = resolver_pressao_oraculo(tipo, div, q_o, 3, 0.0, bol_o)
-    n_g = resolver_pressao(tipo, div, q_g, 3, 0.0, bol_g)
+    n_g = resolver_pressao(tipo, div, q_g, 3, 0.0, bol_g, motor=motor)
     assert len(n_o) == len(n_g) == 4
     # FP32 CG with FP64 dots vs the oracle's double-then-round: 1e-4 relative on q and on the
     # residual history (the fixed three iterations amplify rounding differences a little).
@@ -101,14 +105,15 @@ def test_pcg_iteracoes_fixas(lib_gpu, nome, com_bolhas):
         assert erro_relativo(bol_g["y"], bol_o["y"]) < 1e-3
 
 
+@pytest.mark.parametrize("motor", MOTORES)
 @pytest.mark.parametrize("prec", [_abi.TQ_PREC_FP32, _abi.TQ_PREC_FP16, _abi.TQ_PREC_BF16], ids=["fp32", "fp16", "bf16"])
-def test_pcg_tolerancia(lib_gpu, prec):
+def test_pcg_tolerancia(lib_gpu, prec, motor):
     """With a tolerance the solve runs to ||r|| <= 1e-6 ||r0|| (the oracle agrees on q)."""
     tipo, div, rot, o = problema_de_pressao("copo")
     q_o = np.zeros(tipo.size, np.float32)
     q_g = q_o.copy()
     n_o = resolver_pressao_oraculo(tipo, div, q_o, 200, 1e-6)
-    n_g = resolver_pressao(tipo, div, q_g, 200, 1e-6, precisao=prec)
+    n_g = resolver_pressao(tipo, div, q_g, 200, 1e-6, precisao=prec, motor=motor)
     assert n_g[-1] <= 1e-6 * n_g[0]
     assert n_o[-1] <= 1e-6 * n_o[0]
     assert erro_relativo(q_g, q_o) < 1e-4
@@ -167,9 +172,10 @@ FLUTUANTES = {"u": 1e-4, "v": 1e-4, "q": 1e-4, "div": 1e-5, "fase": 1e-6, "curva
               "pressaoBolha": 1e-3, "volumeAlvo": 0.0}
 
 
+@pytest.mark.parametrize("motor", MOTORES)
 @pytest.mark.parametrize("nome", ["barragem", "bolha", "copo"])
-def test_subpasso_paridade(lib_gpu, nome):
-    o, g = par(nome)
+def test_subpasso_paridade(lib_gpu, nome, motor):
+    o, g = par(nome, {"engine": motor})
     dt = passo_maximo(o.h, o.cena.altura, None)
     for quadro in range(8):
         copiar_estado(o, g)
@@ -191,10 +197,11 @@ def test_subpasso_paridade(lib_gpu, nome):
     del dt
 
 
-def test_deterministico(lib_gpu):
+@pytest.mark.parametrize("motor", MOTORES)
+def test_deterministico(lib_gpu, motor):
     """Two runs of the same scene produce identical bits."""
     def rodar():
-        _, g = par("bolha")
+        _, g = par("bolha", {"engine": motor})
         for _ in range(6):
             g.avancar(1 / 60, 3)
         return g.p.copy(), g.campo("q")
