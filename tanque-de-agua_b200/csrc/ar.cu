@@ -150,8 +150,9 @@ __device__ int rankBloco1024(bool keep, int* total) {
   __syncthreads();
   if (lane == 0) somas[w] = __popc(m);
   __syncthreads();
+  const int nw = (int)(blockDim.x >> 5);
   if (w == 0) {
-    int v = somas[lane];
+    int v = lane < nw ? somas[lane] : 0;  // slots of absent warps were never written
     for (int o = 1; o < 32; o <<= 1) {
       int t = __shfl_up_sync(0xffffffffu, v, o);
       if (lane >= o) v += t;
@@ -160,7 +161,7 @@ __device__ int rankBloco1024(bool keep, int* total) {
   }
   __syncthreads();
   int base = w ? somas[w - 1] : 0;
-  *total = somas[31];
+  *total = somas[nw - 1];
   return base + rank;
 }
 __device__ int scanBlocoUnico(const int* cont, int* offs, int n) {

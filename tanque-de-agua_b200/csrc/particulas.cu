@@ -247,8 +247,9 @@ __device__ int rankNoBloco(bool keep, int* total) {
   __syncthreads();
   if (lane == 0) somas[w] = __popc(m);
   __syncthreads();
+  const int nw = (int)(blockDim.x >> 5);
   if (w == 0) {
-    int v = somas[lane];
+    int v = lane < nw ? somas[lane] : 0;  // slots of absent warps were never written
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       int t = __shfl_up_sync(0xffffffffu, v, o);
@@ -258,7 +259,7 @@ __device__ int rankNoBloco(bool keep, int* total) {
   }
   __syncthreads();
   int base = w ? somas[w - 1] : 0;
-  *total = somas[31];
+  *total = somas[nw - 1];
   return base + rank;
 }
 

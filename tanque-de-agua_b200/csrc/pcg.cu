@@ -550,7 +550,10 @@ Pcg* criarPcg(int nx, int ny, int precisao, int motor) {
   size_t nc = (size_t)p->nxL[L - 1] * p->nyL[L - 1];
   p->smemGrosso = nc * 9 <= 200 * 1024 ? nc * 9 : 0;
   if (p->smemGrosso) {
-    if (cudaFuncSetAttribute(k_grosso, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smemGrosso) != cudaSuccess)
+    // The attribute is per kernel, shared by every solver in the process: it is always raised
+    // to the 200 KB cap, never set to this grid's size, which would fail the launches of a
+    // solver on a grid with a larger coarsest level.
+    if (cudaFuncSetAttribute(k_grosso, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
       p->smemGrosso = 0;
   }
   if (ok && motor == TQ_ENGINE_FUSED) {

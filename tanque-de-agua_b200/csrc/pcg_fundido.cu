@@ -200,7 +200,7 @@ __device__ double somaBloco(double v, double* sh) {
   __syncthreads();
   double t = 0;
   if (w == 0) {
-    t = sh[lane];
+    t = lane < WARPS ? sh[lane] : 0.0;  // only WARPS slots were written
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
   }
@@ -1250,9 +1250,12 @@ Fundido* criarFundido(Pcg* p) {
             : p->precisao == TQ_PREC_BF16 ? kernelDe<__nv_bfloat16>()
                                           : kernelDe<float>();
   int dev = 0, sms = 0, porSM = 0;
+  // The attribute is per kernel and shared by every solver in the process: raise it to the
+  // largest size any grid uses (f->smem <= SMEM_GROSSO_MAX), never lower it to this grid's.
+  const size_t smemMax = SMEM_GROSSO_MAX > areas ? SMEM_GROSSO_MAX : areas;
   bool ok = cudaGetDevice(&dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-            cudaFuncSetAttribute(f->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f->smem) == cudaSuccess &&
+            cudaFuncSetAttribute(f->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemMax) == cudaSuccess &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&porSM, f->kern, TF, f->smem) == cudaSuccess && porSM >= 1;
   if (ok) {
     f->G = sms;  // one CTA per SM: co-resident, as the grid barrier needs

@@ -209,3 +209,24 @@ def test_deterministico(lib_gpu, motor):
     p2, q2 = rodar()
     assert np.array_equal(p1.view(np.uint32), p2.view(np.uint32))
     assert np.array_equal(q1.view(np.uint32), q2.view(np.uint32))
+
+
+@pytest.mark.parametrize("motor", MOTORES)
+def test_solvers_vivos_de_tamanhos_diferentes(lib_gpu, motor):
+    """Two live tanks whose coarsest levels need different shared memory: the one created
+    first (the larger coarsest level) still launches after the second one is created."""
+    from tanque.cenarios import semear_retangulo_rapido
+
+    def tanque(nx, ny, h):
+        cena = Cena(nx, ny, h)
+        g = SimulacaoGPU(cena, {"engine": motor, "tolerance": 1e-6, "iterations": 50})
+        g.adicionar(semear_retangulo_rapido(3 * h, 3 * h, 0.5 * cena.largura, 0.6 * cena.altura, h), False)
+        return g
+
+    a = tanque(100, 60, 0.01)   # coarsest level 13x8
+    b = tanque(300, 200, 0.004)  # coarsest level 10x7
+    for _ in range(2):
+        a.avancar(1 / 120, 2)
+        b.avancar(1 / 120, 2)
+    assert a.n > 0 and b.n > 0
+    assert np.all(np.isfinite(a.campo("q"))) and np.all(np.isfinite(b.campo("q")))
