@@ -241,6 +241,27 @@ int tq_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float* 
 int tq_vcycle(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float* x,
               int32_t precision);
 
+/* The same V-cycle as tq_vcycle, for callers that must not allocate device memory while
+ * they run (no counterpart in the reference).  A host engine whose allocator already holds
+ * the device memory it is allowed to use, or that cannot afford cudaFree's device-wide
+ * synchronisation or an allocation failing in the middle of a frame, gets the V-cycle's
+ * level hierarchy from a static device array instead: nothing is allocated or freed.
+ *
+ * tipo, b and x are DEVICE pointers on the current device (N = nx*ny bytes, floats, floats;
+ * x is written, b and tipo only read); the work is queued on `stream` (a cudaStream_t, NULL
+ * for the default stream) and the call returns without waiting for it.
+ * Limit: the levels of the grid must fit in 16 MiB of scratch (about 13 bytes per level-0
+ * cell plus 14 per coarse cell: roughly 900,000 cells, e.g. 1280x720); a larger grid
+ * returns TQ_E_CAPACITY, with the bytes it needs in tq_last_error, before any device work.
+ * Nothing in the scratch needs to start at zero: each call writes what it reads.
+ * The scratch is shared by every call on a device: calls whose work overlaps in time (two
+ * streams, or two host threads) race on it and corrupt each other's results, so keep the
+ * calls on one device in one stream, or wait for one before issuing the next.
+ * The first call on each device does a one-time set-up (it looks up the scratch's device
+ * address); a caller that captures streams makes that first call before capturing. */
+int tq_vcycle_noalloc(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float* x,
+                      int32_t precision, void* stream);
+
 /* ---------------------------------------------------------------- errors */
 const char* tq_status_string(int status);
 /* Last error message of the calling thread (CUDA error text or argument problem). */

@@ -41,6 +41,14 @@ void perfilPcg(Pcg* p, bool ligar);
 int lerPerfilPcg(Pcg* p, unsigned long long* out, int cap);
 // One V-cycle from device buffers (level-0 types, right-hand side, result).
 int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cudaStream_t s);
+// One V-cycle with the level hierarchy in a static device array (tq_vcycle_noalloc): its
+// capacity, the bytes a grid needs, the array's address on the current device (looked up once
+// per device) and the cycle itself.
+constexpr size_t BYTES_SCRATCH_VCICLO = (size_t)16 << 20;
+size_t bytesScratchVCiclo(int nx, int ny);
+int enderecoScratchVCiclo(void** out);
+int cicloVSemAlocar(void* scratch, int nx, int ny, const uint8_t* tipo, const float* b, float* x, int precisao,
+                    cudaStream_t s);
 
 // ar.cu — RastreadorDeAr.atualizar on the device.
 struct Rastreador;

@@ -7,6 +7,7 @@
 // __nv_bfloat16 (levels below 16k cells stay float); arithmetic is FP32; dot products and
 // norms are FP64 with a fixed reduction order (bitwise reproducible); per-bubble sums are
 // 64-bit fixed point.
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -790,6 +791,101 @@ int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cud
     lanca(k_descarregar_x<T>, nb, 256, 0, s, nivel<T>(p, 0), x);
   });
   return cudaGetLastError() == cudaSuccess ? TQ_OK : TQ_E_CUDA;
+}
+
+// ---------------------------------------------------------------- V-cycle without allocation
+// The level hierarchy of tq_vcycle_noalloc lives in this file-scope device array instead of
+// cudaMalloc'd buffers.  Level 0 reads the caller's types in place; every other array is
+// carved from the scratch on 256-byte boundaries.  The call writes every scratch byte it
+// reads before reading it (types and masks of every level, level-0 b and x = 0, the
+// restriction's b and x = 0 on each coarse level), so nothing has to start at zero and
+// nothing carries over from one call to the next.
+static __device__ __align__(256) unsigned char g_scratchVCiclo[BYTES_SCRATCH_VCICLO];
+
+namespace {
+constexpr size_t ALINHA_SCRATCH = 256;
+inline size_t alinhar(size_t n) { return (n + ALINHA_SCRATCH - 1) & ~(ALINHA_SCRATCH - 1); }
+
+// The level sizes of montarNiveis (js/pressao-cpu.js:24-41), as criarPcg builds them.
+int niveisDe(int nx, int ny, int* nxL, int* nyL) {
+  int L = 1, a = nx, b = ny;
+  nxL[0] = a;
+  nyL[0] = b;
+  while ((a < b ? a : b) > 12 && L < MAX_NIVEIS) {
+    a = (a + 1) / 2;
+    b = (b + 1) / 2;
+    nxL[L] = a;
+    nyL[L] = b;
+    L++;
+  }
+  return L;
+}
+}  // namespace
+
+size_t bytesScratchVCiclo(int nx, int ny) {
+  int nxL[MAX_NIVEIS], nyL[MAX_NIVEIS];
+  const int L = niveisDe(nx, ny, nxL, nyL);
+  size_t total = 0;
+  for (int l = 0; l < L; l++) {
+    const size_t n = (size_t)nxL[l] * nyL[l];
+    if (l > 0) total += alinhar(n);  // types (level 0 uses the caller's)
+    total += alinhar(n) + 3 * alinhar(n * 4);  // masks, b, x, tmp
+  }
+  return total;
+}
+
+// Device address of the scratch on the current device, looked up once per device.
+int enderecoScratchVCiclo(void** out) {
+  static std::mutex mtx;
+  static void* base[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return TQ_E_NODEV;
+  std::lock_guard<std::mutex> g(mtx);
+  if (!base[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_scratchVCiclo) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return TQ_E_CUDA;
+    }
+    base[dev] = p;
+  }
+  *out = base[dev];
+  return TQ_OK;
+}
+
+int cicloVSemAlocar(void* scratch, int nx, int ny, const uint8_t* tipo, const float* b, float* x, int precisao,
+                    cudaStream_t s) {
+  Pcg p{};
+  p.nx = nx;
+  p.ny = ny;
+  p.N = nx * ny;
+  p.precisao = precisao;
+  p.motor = TQ_ENGINE_PLAIN;
+  p.L = niveisDe(nx, ny, p.nxL, p.nyL);
+  unsigned char* cur = (unsigned char*)scratch;
+  for (int l = 0; l < p.L; l++) {
+    const size_t n = (size_t)p.nxL[l] * p.nyL[l];
+    p.meia[l] = precisao != TQ_PREC_FP32 && n >= (size_t)MEIA_MIN_CELULAS;
+    if (l == 0) {
+      p.tipoL[0] = const_cast<uint8_t*>(tipo);  // only read (prepararNiveis copies nothing)
+    } else {
+      p.tipoL[l] = cur;
+      cur += alinhar(n);
+    }
+    p.vizL[l] = cur;
+    cur += alinhar(n);
+    p.bL[l] = cur;
+    cur += alinhar(n * 4);
+    p.xL[l] = cur;
+    cur += alinhar(n * 4);
+    p.tmpL[l] = cur;
+    cur += alinhar(n * 4);
+  }
+  // The coarsest solve stages its level in shared memory only within the default 48 KB, which
+  // needs no function attribute.
+  const size_t nc = (size_t)p.nxL[p.L - 1] * p.nyL[p.L - 1];
+  p.smemGrosso = nc * 9 <= 48 * 1024 ? nc * 9 : 0;
+  return cicloVDispositivo(&p, tipo, b, x, s);
 }
 
 }  // namespace tq

@@ -811,4 +811,25 @@ int tq_vcycle(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float
   return r;
 }
 
+int tq_vcycle_noalloc(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float* x, int32_t precision,
+                      void* stream) {
+  if (nx < 3 || ny < 3 || !tipo || !b || !x) return falha(TQ_E_ARG, "tq_vcycle_noalloc: bad arguments");
+  if (precision < TQ_PREC_FP32 || precision > TQ_PREC_BF16) return falha(TQ_E_ARG, "tq_vcycle_noalloc: bad precision");
+  const size_t preciso = bytesScratchVCiclo(nx, ny);
+  if (preciso > BYTES_SCRATCH_VCICLO) {
+    std::snprintf(g_erro, sizeof g_erro,
+                  "tq_vcycle_noalloc: a %dx%d grid needs %zu bytes of scratch for its levels; the static scratch "
+                  "holds %zu bytes",
+                  nx, ny, preciso, BYTES_SCRATCH_VCICLO);
+    return TQ_E_CAPACITY;
+  }
+  void* scratch = nullptr;
+  int st = enderecoScratchVCiclo(&scratch);
+  if (st == TQ_E_NODEV) return falha(st, "tq_vcycle_noalloc: no current CUDA device");
+  if (st) return falha(st, "tq_vcycle_noalloc: cudaGetSymbolAddress of the scratch failed");
+  st = cicloVSemAlocar(scratch, nx, ny, tipo, b, x, precision, (cudaStream_t)stream);
+  if (st) return falha(st, "tq_vcycle_noalloc: V-cycle launch failed");
+  return TQ_OK;
+}
+
 }  // extern "C"
