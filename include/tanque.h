@@ -187,7 +187,9 @@ enum tq_scalar {
   TQ_SCALAR_PCG_RES0 = 4,       /* ||r0|| of the last solve */
   TQ_SCALAR_PCG_RES = 5,        /* final ||r|| of the last solve */
   TQ_SCALAR_LAUNCHES = 6,       /* kernels launched by this process so far (all handles) */
-  TQ_SCALAR_COUNT_ = 7
+  TQ_SCALAR_GRAVITY_X = 7,      /* sim.gravidade[0] (m/s^2) — writable, used from the next */
+  TQ_SCALAR_GRAVITY_Y = 8,      /* sim.gravidade[1]   substep (MotorCPU.gravidade, js/motor.js:96) */
+  TQ_SCALAR_COUNT_ = 9
 };
 int tq_get_scalar(tq_sim* s, int32_t which, double* out);
 int tq_set_scalar(tq_sim* s, int32_t which, double value);

@@ -1746,6 +1746,8 @@ int tqo_get_scalar(tqo_sim* s, int32_t which, double* out) {
       case TQ_SCALAR_PCG_ITERS: *out = S_.normas.empty() ? 0 : (double)(S_.normas.size() - 1); break;
       case TQ_SCALAR_PCG_RES0: *out = S_.normas.empty() ? 0 : S_.normas.front(); break;
       case TQ_SCALAR_PCG_RES: *out = S_.normas.empty() ? 0 : S_.normas.back(); break;
+      case TQ_SCALAR_GRAVITY_X: *out = S_.gravidade[0]; break;
+      case TQ_SCALAR_GRAVITY_Y: *out = S_.gravidade[1]; break;
       default: return fail(TQ_E_ARG, "unknown scalar");
     }
   });
@@ -1757,6 +1759,8 @@ int tqo_set_scalar(tqo_sim* s, int32_t which, double value) {
       case TQ_SCALAR_VMAX: S_.vMax = value; break;
       case TQ_SCALAR_PRIMEIRA: S_.rastreador.primeira = value != 0; break;
       case TQ_SCALAR_TIPOS_PRONTOS: S_.tiposProntos = value != 0; break;
+      case TQ_SCALAR_GRAVITY_X: S_.gravidade[0] = value; break;  // sim.gravidade (js/motor.js:96)
+      case TQ_SCALAR_GRAVITY_Y: S_.gravidade[1] = value; break;
       default: return fail(TQ_E_ARG, "scalar not writable");
     }
   });

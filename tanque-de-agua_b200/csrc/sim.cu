@@ -628,6 +628,8 @@ int tq_get_scalar(tq_sim* s, int32_t w, double* out) {
     case TQ_SCALAR_PRIMEIRA: *out = primeiraRastreador(s->ar); return TQ_OK;
     case TQ_SCALAR_TIPOS_PRONTOS: *out = s->tiposProntos ? 1 : 0; return TQ_OK;
     case TQ_SCALAR_PCG_ITERS: *out = itersPcg(s->pcg); return TQ_OK;
+    case TQ_SCALAR_GRAVITY_X: *out = s->o.gravity[0]; return TQ_OK;
+    case TQ_SCALAR_GRAVITY_Y: *out = s->o.gravity[1]; return TQ_OK;
     case TQ_SCALAR_PCG_RES0:
     case TQ_SCALAR_PCG_RES: {
       double v[2];
@@ -645,6 +647,8 @@ int tq_set_scalar(tq_sim* s, int32_t w, double v) {
   switch (w) {
     case TQ_SCALAR_PRIMEIRA: definirPrimeiraRastreador(s->ar, v != 0); return TQ_OK;
     case TQ_SCALAR_TIPOS_PRONTOS: s->tiposProntos = v != 0; return TQ_OK;
+    case TQ_SCALAR_GRAVITY_X: s->o.gravity[0] = v; return TQ_OK;
+    case TQ_SCALAR_GRAVITY_Y: s->o.gravity[1] = v; return TQ_OK;
     case TQ_SCALAR_VMAX: {
       unsigned long long b;
       std::memcpy(&b, &v, 8);

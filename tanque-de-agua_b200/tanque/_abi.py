@@ -37,6 +37,7 @@ CAMPOS_ENUM = {
 TQ_SCALAR_VMAX, TQ_SCALAR_PRIMEIRA, TQ_SCALAR_TIPOS_PRONTOS = 0, 1, 2
 TQ_SCALAR_PCG_ITERS, TQ_SCALAR_PCG_RES0, TQ_SCALAR_PCG_RES = 3, 4, 5
 TQ_SCALAR_LAUNCHES = 6
+TQ_SCALAR_GRAVITY_X, TQ_SCALAR_GRAVITY_Y = 7, 8
 
 
 class TqOptions(C.Structure):

@@ -76,7 +76,13 @@ class Simulacao:
     # ---------------------------------------------------------------- SimulacaoCPU surface
     @property
     def gravidade(self):
-        return (self.opcoes.gravity[0], self.opcoes.gravity[1])
+        return (self.escalar(_abi.TQ_SCALAR_GRAVITY_X), self.escalar(_abi.TQ_SCALAR_GRAVITY_Y))
+
+    @gravidade.setter
+    def gravidade(self, g):
+        """sim.gravidade = [gx, gy] (MotorCPU.gravidade, js/motor.js:96): used from the next substep."""
+        self.definirEscalar(_abi.TQ_SCALAR_GRAVITY_X, float(g[0]))
+        self.definirEscalar(_abi.TQ_SCALAR_GRAVITY_Y, float(g[1]))
 
     def atualizarParedes(self):
         """atualizarParedes (js/fisica-cpu.js:80-85) after Cena edits: upload the SDF."""

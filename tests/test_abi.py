@@ -57,3 +57,13 @@ def test_erros_de_argumento_sem_gpu():
         lig("create", C.byref(o), C.byref(h))
     assert e.value.status == _abi.TQ_E_ARG
     assert lig.lib.tq_status_string(_abi.TQ_E_TIMEOUT)
+
+
+def test_gravidade_escalar_no_oraculo():
+    """TQ_SCALAR_GRAVITY_X/Y read back what was set (oracle side of the mirrored surface)."""
+    from oraculo import CenaOraculo, SimulacaoOraculo
+    o = SimulacaoOraculo(CenaOraculo(20, 16, 0.01))
+    assert o.gravidade == (0.0, -9.81)
+    o.gravidade = (1.5, -2.0)
+    assert o.gravidade == (1.5, -2.0)
+    o.fechar()

@@ -230,3 +230,20 @@ def test_solvers_vivos_de_tamanhos_diferentes(lib_gpu, motor):
         b.avancar(1 / 120, 2)
     assert a.n > 0 and b.n > 0
     assert np.all(np.isfinite(a.campo("q"))) and np.all(np.isfinite(b.campo("q")))
+
+
+def test_gravidade_em_execucao(lib_gpu):
+    """sim.gravidade changed between frames (MotorCPU.gravidade, js/motor.js:96): the next
+    substeps use it on the GPU exactly as in the oracle."""
+    o, g = par("barragem")
+    for s in (o, g):
+        s.avancar(1 / 60 / 3, 1)
+        s.gravidade = (3.5, -4.0)
+    assert g.gravidade == (3.5, -4.0) == o.gravidade
+    copiar_estado(o, g)
+    o.avancar(1 / 60 / 3, 1)
+    g.avancar(1 / 60 / 3, 1)
+    for campo in ["accU", "accV", "tipo"]:
+        assert np.array_equal(g.campo(campo), o.campo(campo)), campo
+    assert erro_relativo(g.campo("u"), o.campo("u")) <= 1e-4
+    assert erro_relativo(g.campo("v"), o.campo("v")) <= 1e-4
