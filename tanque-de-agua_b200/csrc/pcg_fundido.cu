@@ -1,7 +1,7 @@
 // pcg_fundido.cu — FUSED engine of the MGPCG pressure projection: the whole solve of
 // resolverPCG (js/pressao-cpu.js:296-402) in ONE persistent cooperative launch.
 //
-// One CTA of 512 threads per SM; phases are separated by a grid barrier (monotonic arrival
+// One CTA of 384 threads per SM (12 warps: room for ~170 registers a thread); phases are separated by a grid barrier (monotonic arrival
 // counter, release-add / acquire-poll) whose waits are bounded: a wait that exceeds ~1 s sets
 // an error flag, every CTA returns, and the host reports TQ_E_TIMEOUT.
 // Per PCG iteration: [DA] p = z + beta p fused with A p and p.Ap, [B] the q/r/bubble updates
@@ -27,21 +27,34 @@
 
 namespace tq {
 
-constexpr int TF = 512;
+constexpr int TF = 384;
 constexpr int WARPS = TF / 32;
 constexpr long long LIMITE_CICLOS = 2000000000LL;  // ~1 s at 1.9 GHz
 constexpr double ESC = 1099511627776.0;            // 2^40, per-bubble fixed point
 constexpr size_t SMEM_GROSSO_MAX = 200 * 1024;
+// Levels up to this many cells run in CTA 0's coarse section; larger ones as grid phases,
+// where their 16x16 blocks spread over the SMs instead of queueing on one SM's warps.
+constexpr size_t SECAO_MAX_CELULAS = 2048;
+// The coarsest solve as a stored matrix: up to DENSO_MAX changing cells (water with a free
+// neighbour) on a coarsest level of at most DENSO_MAPA_MAX cells.  Layout at offDenso: the
+// matrix (DENSO_MAX^2 floats), the cells (int), their neighbours' list indices (4 int each),
+// 1/k (float), and a header (count, count of colour 0).
+constexpr int DENSO_MAX = 128;
+constexpr int DENSO_MAPA_MAX = DENSO_MAX * DENSO_MAX;
+constexpr size_t DENSO_BYTES = (size_t)DENSO_MAX * DENSO_MAX * 4 + (size_t)DENSO_MAX * 4 * 6 + 16;
+constexpr size_t SMEM_CTA_MAX = 227 * 1024 - 2048;  // dynamic shared memory cap (static share aside)
 constexpr int NPARC = 4;                           // partial slots per CTA
 constexpr int PERFIL_MAX = 1 << 16;                // phase-trace capacity
 constexpr int PERFIL_SECAO = 1 << 14;              // coarse-section stamps (after the phase trace)
 // per-warp shared-memory areas (floats)
-constexpr int TILE = 324;                          // 18x18 smoother tile
+constexpr int TILE = 324;                          // 18x18 smoother tile (cells)
+constexpr int PT = 24;                             // its row pitch in shared memory: the sweeps'
+constexpr int TILE_AREA = 18 * PT;                 // strided loads then hit 32 distinct banks
 constexpr int CT = 121;                            // 11x11 coarse tile for the folded prolongation
-constexpr int SUAV_W = TILE + CT + 32;             // + coarse water flags (bytes, rounded)
+constexpr int SUAV_W = TILE_AREA + CT + 32;
 constexpr int RX = 6 * 68, RB = 4 * 66;            // restriction staging: x rows, b/viz/residual rows
 constexpr int REST_W = RX + 3 * RB;                // x, b, residual (floats) + viz (bytes in one RB)
-constexpr size_t TILES_SECAO = (size_t)(512 / 32) * TILE * 4;  // per-warp tiles of the coarse section
+constexpr size_t TILES_SECAO = (size_t)WARPS * TILE_AREA * 4;  // per-warp tiles of the coarse section
 
 struct NivelF {
   int nx, ny, meia, pad;
@@ -63,6 +76,8 @@ struct Fundido {
   int* nAtivos = nullptr;
   float *p2 = nullptr, *z2 = nullptr;
   float *xc = nullptr, *bc = nullptr;
+  int offDenso = -1;  // byte offset of the coarsest level's matrix in CTA 0's shared memory
+  uint16_t* op = nullptr;
   void* kern = nullptr;
   unsigned long long* perfil = nullptr;
   bool perfilar = false;
@@ -85,6 +100,8 @@ struct Args {
   int* nAtivos;
   float *p2, *z2;
   float *xc, *bc;
+  int offDenso;  // coarsest-level matrix in CTA 0's dynamic shared memory (-1: sweeps)
+  uint16_t* op;  // per-cell operator descriptor of level 0 (OP_*)
   unsigned long long* perfil;  // [0] count, [1..] %globaltimer at each barrier (null: off)
 };
 
@@ -250,6 +267,13 @@ __device__ __forceinline__ bool bolhaAtiva(const Args& a, uint32_t r) {
   return r >= 2 && r < (uint32_t)MAX_BOLHAS && __ldcg(&a.d.facesB[r]) > 0;
 }
 
+// Per-cell operator descriptor of level 0 (built once per solve): bits 0-3 the left, right,
+// down and up neighbours are water; OP_AGUA the cell is water; OP_FACE interior air of an
+// active bubble (its water faces enter the bubble's row); OP_VIZ_BOLHA a free neighbour is
+// air of an active bubble; OP_BOLHA air of an active bubble; bits 8-10 the number of free
+// (non-wall) neighbours.
+constexpr int OP_AGUA = 16, OP_FACE = 32, OP_VIZ_BOLHA = 64, OP_BOLHA = 128;
+
 __device__ __forceinline__ int grossoBaseF(int i) { return (i & 1) == 0 ? (i >> 1) - 1 : (i - 1) >> 1; }
 __device__ __forceinline__ float pesoBaseF(int i) { return (i & 1) == 0 ? 0.25f : 0.75f; }
 
@@ -270,108 +294,168 @@ __device__ __forceinline__ float inversoVizinhos(int k) {
   return k == 1 ? 1.0f : k == 2 ? 0.5f : k == 3 ? (1.0f / 3.0f) : 0.25f;
 }
 
-// The VARREDURAS red-black sweeps of one 16x16 block on its 18x18 shared tile
+// One half-sweep of colour COR over the lane's four cells of that colour (tile offsets li + dc).
+// A cell reads only cells of the other colour and itself, so all loads go before the stores; a
+// cell that does not change (dry, outside the grid, or no free neighbour) stores its own value.
+template <int COR>
+__device__ __forceinline__ void meiaVarredura(float* tile, const int (&li)[4], int dc, const int (&vz)[8],
+                                              const float (&bv)[8], const float (&inv)[8]) {
+  float nb[4][5];
+#pragma unroll
+  for (int mm = 0; mm < 4; mm++) {
+    const int p = li[mm] + dc;
+    nb[mm][0] = tile[p - 1];
+    nb[mm][1] = tile[p + 1];
+    nb[mm][2] = tile[p - PT];
+    nb[mm][3] = tile[p + PT];
+    nb[mm][4] = tile[p];
+  }
+#pragma unroll
+  for (int mm = 0; mm < 4; mm++) {
+    const int v = vz[4 * COR + mm];
+    const int mk = v & 15;
+    float s = 0.0f;
+    s += (mk & 1) ? nb[mm][0] : 0.0f;
+    s += (mk & 2) ? nb[mm][1] : 0.0f;
+    s += (mk & 4) ? nb[mm][2] : 0.0f;
+    s += (mk & 8) ? nb[mm][3] : 0.0f;
+    const float q = nb[mm][4];
+    const float novo = q + ((s + bv[4 * COR + mm]) * inv[4 * COR + mm] - q);
+    tile[li[mm] + dc] = ((v & 16) && mk) ? novo : q;
+  }
+  __syncwarp();
+}
+
+// The VARREDURAS red-black sweeps of one 16x16 block on its 18x18 shared tile (row pitch PT)
 // (js/pressao-cpu.js:114-137), by one warp, cells as in celulaBloco; vz = neighbour mask |
-// 16 water | 128 in grid, bv = right side.  Within a half-sweep a cell reads only cells of the
-// other colour and itself, so each lane issues all its loads before its stores.
+// 16 water | 128 in grid, bv = right side; ordem 0 sweeps colour 0 first.
 __device__ __forceinline__ void varrerTile(float* tile, const int (&vz)[8], const float (&bv)[8], int ordem) {
   const int lane = threadIdx.x & 31;
   int li[4];
 #pragma unroll
-  for (int mm = 0; mm < 4; mm++) li[mm] = ((lane >> 3) + 4 * mm + 1) * 18 + 2 * (lane & 7) + 1;
+  for (int mm = 0; mm < 4; mm++) li[mm] = ((lane >> 3) + 4 * mm + 1) * PT + 2 * (lane & 7) + 1;
   const int par = (1 + (lane >> 3)) & 1;  // column offset of colour 0; colour 1 is the other one
   float inv[8];
 #pragma unroll
   for (int m = 0; m < 8; m++) inv[m] = inversoVizinhos(__popc(vz[m] & 15));
+  if (ordem == 0) {
 #pragma unroll
-  for (int it = 0; it < VARREDURAS; it++) {
+    for (int it = 0; it < VARREDURAS; it++) {
+      meiaVarredura<0>(tile, li, par, vz, bv, inv);
+      meiaVarredura<1>(tile, li, par ^ 1, vz, bv, inv);
+    }
+  } else {
 #pragma unroll
-    for (int o = 0; o < 2; o++) {
-      const int cor = o ^ ordem;
-      const int dc = cor ? par ^ 1 : par;
-      float nb[4][5];
-#pragma unroll
-      for (int mm = 0; mm < 4; mm++) {
-        const int p = li[mm] + dc;
-        nb[mm][0] = tile[p - 1];
-        nb[mm][1] = tile[p + 1];
-        nb[mm][2] = tile[p - 18];
-        nb[mm][3] = tile[p + 18];
-        nb[mm][4] = tile[p];
-      }
-#pragma unroll
-      for (int mm = 0; mm < 4; mm++) {
-        const int v = cor ? vz[4 + mm] : vz[mm];
-        const int mk = v & 15;
-        if ((v & 16) && mk) {
-          float s = 0.0f;
-          s += (mk & 1) ? nb[mm][0] : 0.0f;
-          s += (mk & 2) ? nb[mm][1] : 0.0f;
-          s += (mk & 4) ? nb[mm][2] : 0.0f;
-          s += (mk & 8) ? nb[mm][3] : 0.0f;
-          const float q = nb[mm][4];
-          const float b = cor ? bv[4 + mm] : bv[mm];
-          const float iv = cor ? inv[4 + mm] : inv[mm];
-          tile[li[mm] + dc] = q + ((s + b) * iv - q);
-        }
-      }
-      __syncwarp();
+    for (int it = 0; it < VARREDURAS; it++) {
+      meiaVarredura<1>(tile, li, par ^ 1, vz, bv, inv);
+      meiaVarredura<0>(tile, li, par, vz, bv, inv);
     }
   }
 }
 
 // ---------------------------------------------------------------- grid-level smoother
-// suavizar (js/pressao-cpu.js:99-150) for one 16x16 block, by one warp.  Lane l owns the
-// cells t = l + 32m (m = 0..7) of the block: column t & 15, row t >> 4.  With PROL the
-// snapshot is x + P(x_coarse) (prolongar, js/pressao-cpu.js:191-214) built while loading.
-template <class T, bool PROL>
-__device__ __forceinline__ void suavizarBloco(const NivelF n, int blk, int nbx, int desl, int ordem, const T* src,
-                                              T* dst, float* area, const NivelF g, const float* xcSecao) {
+// Modes of a smoother pass over a grid level:
+//   M_NORMAL   snapshot = src, right side = b;
+//   M_PROL     snapshot = x + P(x_coarse) (prolongar, js/pressao-cpu.js:191-214), built while
+//              loading: the first pass on the way up;
+//   M_ZERO     snapshot = 0: the first pass on the way down, whose x the restriction (or the
+//              spread) leaves at 0 (js/pressao-cpu.js:186, :354);
+//   M_ESPALHAR level 0, first pass: also spreads the residual into b (precondicionar,
+//              js/pressao-cpu.js:353-355), b = escala * r, bubble cells their bubble's mean;
+//   M_JUNTAR   level 0, last pass: instead of storing x, gathers z = x / escala (:357-361),
+//              bubble cells' share into the bubble's fixed-point sum, and the partials of r.z
+//              and r.zOld.
+enum { M_NORMAL = 0, M_PROL = 1, M_ZERO = 2, M_ESPALHAR = 3, M_JUNTAR = 4 };
+
+// What the spread and the gather need (level 0).
+struct Reuniao {
+  float escala;          // b = escala * residual; z = x / escala
+  float* zNovo;
+  const float* zVelho;   // previous z (r.zOld), or null
+};
+
+// suavizar (js/pressao-cpu.js:99-150) for one 16x16 block, by one warp, cells as in
+// celulaBloco.  Every global load of the block goes out in one batch before the first
+// shared-memory store: a load-then-store sequence would wait for each L2 round trip in turn.
+template <class T, int MODO>
+__device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, int blk, int nbx, int desl, int ordem,
+                                              const T* src, T* dst, float* area, const NivelF& g,
+                                              const float* xcSecao, const Reuniao& ru, double& s0, double& s1) {
+  constexpr bool PROL = MODO == M_PROL;
+  constexpr bool ZERO = MODO == M_ZERO || MODO == M_ESPALHAR;
   const int lane = threadIdx.x & 31;
   const int bx = blk % nbx, by = blk / nbx;
   const int ox = bx * 16 - desl, oy = by * 16 - desl;
   const int nx = n.nx, ny = n.ny;
   float* tile = area;
-  // The tile's loads go out as one batch (registers first, shared memory after): a
-  // load-then-store loop would wait for each L2 round trip in turn.
   float tv[11];
-  int tz[11];
+  unsigned tAgua = 0;  // bit k: tile entry k is a water cell (PROL)
 #pragma unroll
   for (int k = 0; k < 11; k++) {
     const int s = lane + 32 * k;
     const int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
     const bool ok = s < TILE && sx >= 0 && sy >= 0 && sx < nx && sy < ny;
-    tv[k] = ok ? carregar(ldcg(src + sx + sy * nx)) : 0.0f;
-    if (PROL) tz[k] = ok ? ldcg8(n.viz + sx + sy * nx) : 0;
+    tv[k] = (!ZERO && ok) ? carregar(ldcg(src + sx + sy * nx)) : 0.0f;
+    if (PROL) tAgua |= (unsigned)((ok ? ldcg8(n.viz + sx + sy * nx) : 0) >> 4 & 1) << k;
+  }
+  int vz[8];
+  float bv[8];
+  int cel[8];
+  {
+    const T* b = (const T*)n.b;
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      const int t = celulaBloco(lane, m);
+      const int gx = ox + (t & 15), gy = oy + (t >> 4);
+      const bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
+      const int c = gx + gy * nx;
+      cel[m] = dentro ? c : -1;
+      vz[m] = dentro ? (ldcg8(n.viz + c) | 128) : 0;
+      if (MODO == M_ESPALHAR) bv[m] = dentro ? __ldcg(a.d.r + c) : 0.0f;
+      else bv[m] = dentro ? carregar(ldcg(b + c)) : 0.0f;
+    }
+  }
+  if (MODO == M_ESPALHAR) {
+    // cells of active bubbles take their bubble's mean residual; b is stored in the storage
+    // type and the sweep uses the stored value
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      if (cel[m] < 0) continue;
+      float v = bv[m];
+      if (a.bolhas && (__ldcg(a.op + cel[m]) & OP_BOLHA)) {
+        const uint32_t rb = __ldcg(a.d.rotulo + cel[m]);
+        v = (float)(__ldcg(a.d.rb + rb) / __ldcg(a.d.celsB + rb));
+      }
+      const T bt = guardar<T>(v * ru.escala);
+      ((T*)n.b)[cel[m]] = bt;
+      bv[m] = carregar(bt);
+    }
   }
   if (PROL) {
     // coarse tile: columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11, water x or 0
-    float* ct = area + TILE;
+    float* ct = area + TILE_AREA;
     const int cx0 = (ox - 2) >> 1, cy0 = (oy - 2) >> 1;
     float cv[4];
+    int cz[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       const int s = lane + 32 * k;
       const int I = cx0 + s % 11, J = cy0 + s / 11;
-      float v = 0.0f;
-      if (s < CT && I >= 0 && J >= 0 && I < g.nx && J < g.ny) {
-        const int C = I + J * g.nx;
-        const int gv = ldcg8(g.viz + C);
-        const float xv = xcSecao ? __ldcg(xcSecao + C) : lerN(g.meia, g.x, C);
-        v = (gv & 16) ? xv : 0.0f;
-      }
-      cv[k] = v;
+      const bool ok = s < CT && I >= 0 && J >= 0 && I < g.nx && J < g.ny;
+      const int C = ok ? I + J * g.nx : 0;
+      cz[k] = ok ? ldcg8(g.viz + C) : 0;
+      cv[k] = ok ? (xcSecao ? __ldcg(xcSecao + C) : lerN(g.meia, g.x, C)) : 0.0f;
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       const int s = lane + 32 * k;
-      if (s < CT) ct[s] = cv[k];
+      if (s < CT) ct[s] = (cz[k] & 16) ? cv[k] : 0.0f;
     }
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 11; k++) {
       const int s = lane + 32 * k;
-      if (s < TILE && (tz[k] & 16)) {
+      if (s < TILE && (tAgua >> k & 1)) {
         const int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
         const int I0 = grossoBaseF(sx) - cx0, J0 = grossoBaseF(sy) - cy0;
         const float wx0 = pesoBaseF(sx), wy0 = pesoBaseF(sy);
@@ -389,35 +473,54 @@ __device__ __forceinline__ void suavizarBloco(const NivelF n, int blk, int nbx, 
 #pragma unroll
   for (int k = 0; k < 11; k++) {
     const int s = lane + 32 * k;
-    if (s < TILE) tile[s] = tv[k];
-  }
-  int vz[8];
-  float bv[8];
-  const T* b = (const T*)n.b;
-#pragma unroll
-  for (int m = 0; m < 8; m++) {
-    int t = celulaBloco(lane, m);
-    int gx = ox + (t & 15), gy = oy + (t >> 4);
-    bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
-    int c = gx + gy * nx;
-    vz[m] = dentro ? (ldcg8(n.viz + c) | 128) : 0;
-    bv[m] = dentro ? carregar(ldcg(b + c)) : 0.0f;
+    if (s < TILE) tile[(s / 18) * PT + s % 18] = tv[k];
   }
   __syncwarp();
   varrerTile(tile, vz, bv, ordem);
+  if (MODO == M_JUNTAR) {
+    const float inv = 1.0f / ru.escala;
+    int om[8];
+    float rv[8], zv[8];
 #pragma unroll
-  for (int m = 0; m < 8; m++) {
-    if (!(vz[m] & 128)) continue;
-    int t = celulaBloco(lane, m);
-    int gx = ox + (t & 15), gy = oy + (t >> 4);
-    int li = ((t >> 4) + 1) * 18 + (t & 15) + 1;
-    dst[gx + gy * nx] = guardar<T>((vz[m] & 16) ? tile[li] : 0.0f);
+    for (int m = 0; m < 8; m++) {
+      const int c = cel[m] < 0 ? 0 : cel[m];
+      om[m] = cel[m] < 0 ? 0 : __ldcg(a.op + c);
+      rv[m] = __ldcg(a.d.r + c);
+      zv[m] = ru.zVelho ? __ldcg(ru.zVelho + c) : 0.0f;
+    }
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      if (cel[m] < 0) continue;
+      const int t = celulaBloco(lane, m);
+      const int li = ((t >> 4) + 1) * PT + (t & 15) + 1;
+      const float x = carregar(guardar<T>((vz[m] & 16) ? tile[li] : 0.0f)) * inv;
+      if (om[m] & OP_BOLHA) {
+        const uint32_t rb = __ldcg(a.d.rotulo + cel[m]);
+        somaFixa(&a.accZ[rb], (double)x / __ldcg(a.d.celsB + rb), ESC);
+        ru.zNovo[cel[m]] = 0.0f;
+        continue;
+      }
+      ru.zNovo[cel[m]] = x;
+      if (om[m] & OP_AGUA) {
+        s0 += (double)rv[m] * (double)x;
+        if (ru.zVelho) s1 += (double)rv[m] * (double)zv[m];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      if (cel[m] < 0) continue;
+      const int t = celulaBloco(lane, m);
+      const int li = ((t >> 4) + 1) * PT + (t & 15) + 1;
+      dst[cel[m]] = guardar<T>((vz[m] & 16) ? tile[li] : 0.0f);
+    }
   }
   __syncwarp();
 }
 
-template <class T, bool PROL>
-__device__ void faseSuavizarT(const Args& a, int l, int desl, int ordem, bool paraTmp, float* areas) {
+template <class T, int MODO>
+__device__ __noinline__ void faseSuavizarT(const Args& a, int l, int desl, int ordem, bool paraTmp, float* areas,
+                                           const Reuniao& ru, double* sh) {
   const NivelF n = a.niv[l];
   const int nbx = (n.nx + desl + 15) >> 4, nby = (n.ny + desl + 15) >> 4;
   const int nb = nbx * nby;
@@ -426,21 +529,40 @@ __device__ void faseSuavizarT(const Args& a, int l, int desl, int ordem, bool pa
   const T* src = (const T*)(paraTmp ? n.x : n.tmp);
   T* dst = (T*)(paraTmp ? n.tmp : n.x);
   NivelF g{};
-  if (PROL) g = a.niv[l + 1];
-  const float* xcSecao = (PROL && l + 1 == a.Lc) ? a.xc : nullptr;
+  if (MODO == M_PROL) g = a.niv[l + 1];
+  const float* xcSecao = (MODO == M_PROL && l + 1 == a.Lc) ? a.xc : nullptr;
+  double s0 = 0.0, s1 = 0.0;
   for (int blk = w * gridDim.x + blockIdx.x; blk < nb; blk += WARPS * gridDim.x)
-    suavizarBloco<T, PROL>(n, blk, nbx, desl, ordem, src, dst, area, g, xcSecao);
+    suavizarBloco<T, MODO>(a, n, blk, nbx, desl, ordem, src, dst, area, g, xcSecao, ru, s0, s1);
+  if (MODO == M_JUNTAR) {
+    const double t0 = somaBloco(s0, sh);
+    const double t1 = somaBloco(s1, sh);
+    if (threadIdx.x == 0) {
+      a.parc[blockIdx.x * NPARC + 0] = t0;
+      a.parc[blockIdx.x * NPARC + 1] = t1;
+    }
+  }
 }
 
 template <class T>
-__device__ void faseSuavizar(const Args& a, int l, int desl, int ordem, bool paraTmp, bool prol, float* areas,
-                             int meia) {
+__device__ void faseSuavizar(const Args& a, int l, int desl, int ordem, bool paraTmp, int modo, float* areas, int meia,
+                             const Reuniao& ru, double* sh) {
   if (meia) {
-    if (prol) faseSuavizarT<T, true>(a, l, desl, ordem, paraTmp, areas);
-    else faseSuavizarT<T, false>(a, l, desl, ordem, paraTmp, areas);
+    switch (modo) {
+      case M_PROL: faseSuavizarT<T, M_PROL>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
+      case M_ZERO: faseSuavizarT<T, M_ZERO>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
+      case M_ESPALHAR: faseSuavizarT<T, M_ESPALHAR>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
+      case M_JUNTAR: faseSuavizarT<T, M_JUNTAR>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
+      default: faseSuavizarT<T, M_NORMAL>(a, l, desl, ordem, paraTmp, areas, ru, sh);
+    }
   } else {
-    if (prol) faseSuavizarT<float, true>(a, l, desl, ordem, paraTmp, areas);
-    else faseSuavizarT<float, false>(a, l, desl, ordem, paraTmp, areas);
+    switch (modo) {
+      case M_PROL: faseSuavizarT<float, M_PROL>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
+      case M_ZERO: faseSuavizarT<float, M_ZERO>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
+      case M_ESPALHAR: faseSuavizarT<float, M_ESPALHAR>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
+      case M_JUNTAR: faseSuavizarT<float, M_JUNTAR>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
+      default: faseSuavizarT<float, M_NORMAL>(a, l, desl, ordem, paraTmp, areas, ru, sh);
+    }
   }
 }
 
@@ -448,6 +570,7 @@ __device__ void faseSuavizar(const Args& a, int l, int desl, int ordem, bool par
 // restringir (js/pressao-cpu.js:159-188) as a gather, one warp per 32-cell coarse row
 // segment: the fine footprint (x on 6 rows x 68 columns; b and flags on 4 x 66) is staged in
 // the warp's shared area, residuals computed once, then each lane sums its 4x4 window.
+template <class TFino>
 __device__ void faseRestringir(const Args& a, int l, float* areas) {
   const NivelF f = a.niv[l];
   const NivelF g = a.niv[l + 1];
@@ -472,7 +595,7 @@ __device__ void faseRestringir(const Args& a, int l, float* areas) {
       for (int k = 0; k < 13; k++) {
         const int s = lane + 32 * k;
         const int i = fi0 + s % 68, j = fj0 + s / 68;
-        xv[k] = (s < RX && i >= 0 && j >= 0 && i < f.nx && j < f.ny) ? lerN(f.meia, f.x, i + j * f.nx) : 0.0f;
+        xv[k] = (s < RX && i >= 0 && j >= 0 && i < f.nx && j < f.ny) ? carregar(ldcg((const TFino*)f.x + i + j * f.nx)) : 0.0f;
       }
       float bv[9];
       int vv[9];
@@ -483,7 +606,7 @@ __device__ void faseRestringir(const Args& a, int l, float* areas) {
         const bool d = s < RB && i >= 0 && j >= 0 && i < f.nx && j < f.ny;
         const int c = i + j * f.nx;
         vv[k] = d ? ldcg8(f.viz + c) : 0;
-        bv[k] = d ? lerN(f.meia, f.b, c) : 0.0f;
+        bv[k] = d ? carregar(ldcg((const TFino*)f.b + c)) : 0.0f;
       }
 #pragma unroll
       for (int k = 0; k < 13; k++) {
@@ -526,10 +649,7 @@ __device__ void faseRestringir(const Args& a, int l, float* areas) {
           for (int aa = 0; aa < 4; aa++) soma += rs[bb * 66 + 2 * lane + aa] * (pes[aa] * pes[bb]);
       }
       if (secao) a.bc[C] = soma;
-      else {
-        gravarN(g.meia, g.b, C, soma);
-        gravarN(g.meia, g.x, C, 0.0f);
-      }
+      else gravarN(g.meia, g.b, C, soma);  // x of the coarse level: its first pass reads 0
     }
     __syncwarp();
   }
@@ -558,7 +678,7 @@ __device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int
       const int s = lane + 32 * k;
       if (s < TILE) {
         const int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
-        tile[s] = (sx >= 0 && sy >= 0 && sx < nx && sy < ny) ? F[src + sx + sy * nx] : 0.0f;
+        tile[(s / 18) * PT + s % 18] = (sx >= 0 && sy >= 0 && sx < nx && sy < ny) ? F[src + sx + sy * nx] : 0.0f;
       }
     }
     int vz[8];
@@ -579,11 +699,110 @@ __device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int
       if (!(vz[m] & 128)) continue;
       const int t = celulaBloco(lane, m);
       const int gx = ox + (t & 15), gy = oy + (t >> 4);
-      F[dst + gx + gy * nx] = (vz[m] & 16) ? tile[((t >> 4) + 1) * 18 + (t & 15) + 1] : 0.0f;
+      F[dst + gx + gy * nx] = (vz[m] & 16) ? tile[((t >> 4) + 1) * PT + (t & 15) + 1] : 0.0f;
     }
     __syncwarp();
   }
   __syncthreads();
+}
+
+// The coarsest solve (resolverGrosso, js/pressao-cpu.js:217-238) is VARREDURAS_GROSSO
+// red-black sweeps from x = 0: a linear map of the right side, fixed for the whole PCG solve
+// because the cell types are.  CTA 0 builds that map once per solve: column j is the sweeps
+// applied to b = e_j, every thread of the first nL sweeping its own column (stored at
+// M[i * nL + j], so a warp touches consecutive words).  Each V-cycle then applies it as a
+// matrix-vector product.  Leaves the header count > DENSO_MAX when the level has more changing
+// cells, and the section keeps the sweeps.
+struct Denso {
+  float* M;
+  int* celula;  // cell | free-neighbour mask << 24, colour 0 first
+  int* viz4;    // list index of each free neighbour (left, right, down, up) or -1
+  float* inv;   // 1/k
+  int* cab;     // [0] count, [1] count of colour 0
+};
+__device__ __forceinline__ Denso denso(unsigned char* dyn, int off) {
+  Denso z;
+  z.M = (float*)(dyn + off);
+  z.celula = (int*)(z.M + DENSO_MAX * DENSO_MAX);
+  z.viz4 = z.celula + DENSO_MAX;
+  z.inv = (float*)(z.viz4 + 4 * DENSO_MAX);
+  z.cab = (int*)(z.inv + DENSO_MAX);
+  return z;
+}
+
+__device__ __noinline__ void montarDenso(const Args& a, unsigned char* dyn) {
+  const Denso z = denso(dyn, a.offDenso);
+  const NivelF n = a.niv[a.L - 1];
+  const int nx = n.nx, N = n.nx * n.ny;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int* mapa = (int*)z.M;  // cell -> list index, while the matrix is not written yet
+  if (w == 0) {
+    int base = 0, n0 = 0;
+    for (int cor = 0; cor < 2; cor++) {
+      for (int c0 = 0; c0 < N; c0 += 32) {
+        const int c = c0 + lane;
+        const bool minha = c < N && ((((c % nx) + (c / nx) + 1) & 1) == cor);
+        const int vz = minha ? ldcg8(n.viz + c) : 0;
+        const bool ok = minha && (vz & 16) && (vz & 15);
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        const int pos = base + __popc(m & ((1u << lane) - 1u));
+        if (minha) mapa[c] = ok ? pos : -1;
+        if (ok && pos < DENSO_MAX) z.celula[pos] = c | ((vz & 15) << 24);
+        base += __popc(m);
+      }
+      if (cor == 0) n0 = base;
+    }
+    if (lane == 0) {
+      z.cab[0] = base;
+      z.cab[1] = n0;
+    }
+  }
+  __syncthreads();
+  const int nL = z.cab[0];
+  if (nL > DENSO_MAX) return;
+  for (int i = threadIdx.x; i < nL; i += TF) {
+    const int e = z.celula[i], c = e & 0xffffff, mk = e >> 24;
+    z.viz4[4 * i + 0] = (mk & 1) ? mapa[c - 1] : -1;
+    z.viz4[4 * i + 1] = (mk & 2) ? mapa[c + 1] : -1;
+    z.viz4[4 * i + 2] = (mk & 4) ? mapa[c - nx] : -1;
+    z.viz4[4 * i + 3] = (mk & 8) ? mapa[c + nx] : -1;
+    z.inv[i] = inversoVizinhos(__popc(mk));
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nL * nL; k += TF) z.M[k] = 0.0f;
+  __syncthreads();
+  const int j = threadIdx.x;
+  if (j < nL) {
+    const int n0 = z.cab[1];
+    for (int k = 0; k < VARREDURAS_GROSSO; k++)
+      for (int o = 0; o < 2; o++) {
+        const int cor = (k & 1) ? 1 - o : o;
+        const int i0 = cor ? n0 : 0, i1 = cor ? nL : n0;
+        for (int i = i0; i < i1; i++) {
+          float t = 0.0f;
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const int v = z.viz4[4 * i + q];
+            t += v >= 0 ? z.M[v * nL + j] : 0.0f;
+          }
+          z.M[i * nL + j] = (t + (i == j ? 1.0f : 0.0f)) * z.inv[i];
+        }
+      }
+  }
+  __syncthreads();
+}
+
+// x = M b on the coarsest level (one warp per row, lanes over the row, fixed-order warp sum).
+__device__ void aplicarDenso(const Denso& z, float* F, int xa, int b) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nL = z.cab[0];
+  for (int i = w; i < nL; i += WARPS) {
+    float s = 0.0f;
+    for (int j = lane; j < nL; j += 32) s += z.M[i * nL + j] * F[b + (z.celula[j] & 0xffffff)];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) F[xa + (z.celula[i] & 0xffffff)] = s;
+  }
 }
 
 // Stamp of the coarse-section trace (CTA 0, thread 0, when tracing).
@@ -625,7 +844,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
     *tileOff = off;
   }
   __syncthreads();
-  float* tile = (float*)(smem + *tileOff) + w * TILE;
+  float* tile = (float*)(smem + *tileOff) + w * TILE_AREA;
   for (int l = a.Lc; l < a.L; l++) {
     const NivelS t = s[l];
     const uint8_t* viz = a.niv[l].viz;
@@ -706,7 +925,11 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
     __syncthreads();
     marcaSecao(a);
   }
-  if (w == 0) {  // resolverGrosso (js/pressao-cpu.js:217-238), one warp
+  const bool comDenso = a.offDenso >= 0 && denso(smem, a.offDenso).cab[0] <= DENSO_MAX;
+  if (comDenso) {
+    const NivelS n = s[a.L - 1];
+    aplicarDenso(denso(smem, a.offDenso), F, n.xa, n.b);
+  } else if (w == 0) {  // resolverGrosso (js/pressao-cpu.js:217-238), one warp
     const NivelS n = s[a.L - 1];
     const int nx = n.nx, N = n.nx * n.ny;
     float* x = F + n.xa;
@@ -819,24 +1042,28 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
 }
 
 // ---------------------------------------------------------------- the V-cycle
+// cicloV (js/pressao-cpu.js:241-255) between the spread of the residual (first pass) and the
+// gather of z (last pass): 5 Lc + 1 phases, each ending at a grid barrier.
 template <class T>
-__device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char* smem, NivelS* tabS, int* tileOff) {
+__device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char* smem, NivelS* tabS, int* tileOff,
+                       const Reuniao& ru, double* sh) {
   for (int l = 0; l < a.Lc; l++) {
     const int meia = a.niv[l].meia;
-    faseSuavizar<T>(a, l, 0, 0, true, false, areas, meia);
+    faseSuavizar<T>(a, l, 0, 0, true, l == 0 ? M_ESPALHAR : M_ZERO, areas, meia, ru, sh);
     if (!barreira(a, ep)) return false;
-    faseSuavizar<T>(a, l, 8, 0, false, false, areas, meia);
+    faseSuavizar<T>(a, l, 8, 0, false, M_NORMAL, areas, meia, ru, sh);
     if (!barreira(a, ep)) return false;
-    faseRestringir(a, l, areas);
+    if (meia) faseRestringir<T>(a, l, areas);
+    else faseRestringir<float>(a, l, areas);
     if (!barreira(a, ep)) return false;
   }
   if (blockIdx.x == 0) secaoGrossa(a, smem, tabS, tileOff);
   if (!barreira(a, ep)) return false;
   for (int l = a.Lc - 1; l >= 0; l--) {
     const int meia = a.niv[l].meia;
-    faseSuavizar<T>(a, l, 8, 1, true, true, areas, meia);  // prolongation folded in
+    faseSuavizar<T>(a, l, 8, 1, true, M_PROL, areas, meia, ru, sh);
     if (!barreira(a, ep)) return false;
-    faseSuavizar<T>(a, l, 0, 1, false, false, areas, meia);
+    faseSuavizar<T>(a, l, 0, 1, false, l == 0 ? M_JUNTAR : M_NORMAL, areas, meia, ru, sh);
     if (!barreira(a, ep)) return false;
   }
   return true;
@@ -864,58 +1091,83 @@ __device__ __forceinline__ float aplicarF(const Args& a, int c, FV val, FB valB)
   return (float)__popc(vz & 15) * val(c) - s;
 }
 
-// Spreads the residual into the V-cycle's level-0 right-hand side (precondicionar,
-// js/pressao-cpu.js:353-355) and zeroes level-0 x.  rb is read from d.rb.
-__device__ void faseEspalhar(const Args& a, const NivelF& n0, float escala) {
+// [DA] of a PCG iteration over this CTA's cells: p = z + beta p (z alone on the first
+// iteration), A p (js/pressao-cpu.js:84-93, bubble neighbours through their p), the partial of
+// p.Ap (channel 0) and, for air of active bubbles, the sums over their water faces.  Cells go in
+// batches of 4 per thread: descriptors first, then every z and p the batch needs.
+__device__ __noinline__ void faseDA(const Args& a, const float* zc, const float* pv, float* pn, bool prim, float betaf,
+                                    double beta, const double* pbVelho, double* sh) {
   const Dev& d = a.d;
-  for (int c = blockIdx.x * TF + threadIdx.x; c < d.N; c += gridDim.x * TF) {
-    float v = __ldcg(d.r + c);
-    if (a.bolhas && ldcg8(d.tipo + c) == AR) {
-      uint32_t b = __ldcg(d.rotulo + c);
-      if (b >= 2 && b < (uint32_t)MAX_BOLHAS) {
-        unsigned cels = __ldcg(d.celsB + b);
-        if (cels > 0) v = (float)(__ldcg(d.rb + b) / cels);
+  const int N = d.N, nx = d.nx, ny = d.ny;
+  const int gt0 = blockIdx.x * TF + threadIdx.x, GT = gridDim.x * TF;
+  auto pbNovoV = [&](int b) {
+    const double zb = (double)__ldcg(&a.accZ[b]) / ESC;
+    return prim ? zb : zb + beta * __ldcg(&pbVelho[b]);
+  };
+  double s = 0;
+  for (int c0 = gt0; c0 < N; c0 += 4 * GT) {
+    int m[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int c = c0 + k * GT;
+      m[k] = c < N ? __ldcg(a.op + c) : 0;
+    }
+    float zv[4][5], pw[4][5];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int c = c0 + k * GT < N ? c0 + k * GT : 0;
+      const int mk = m[k];
+      const int nb[5] = {c, (mk & 1) ? c - 1 : c, (mk & 2) ? c + 1 : c, (mk & 4) ? c - nx : c, (mk & 8) ? c + nx : c};
+#pragma unroll
+      for (int q = 0; q < 5; q++) {
+        zv[k][q] = __ldcg(zc + nb[q]);
+        pw[k][q] = prim ? 0.0f : __ldcg(pv + nb[q]);
       }
     }
-    gravarN(n0.meia, n0.b, c, v * escala);
-    gravarN(n0.meia, n0.x, c, 0.0f);
-  }
-}
-
-// Gathers z from the V-cycle (precondicionar, js/pressao-cpu.js:357-361): z = x/escala except
-// active bubble cells (zeroed; their mean correction accumulates into accZ); partials of r.z
-// (channel 0) and r.zOld (channel 1).
-__device__ void faseJuntar(const Args& a, const NivelF& n0, float invEscala, float* zNovo, const float* zVelho,
-                           double* sh) {
-  const Dev& d = a.d;
-  double s0 = 0, s1 = 0;
-  for (int c = blockIdx.x * TF + threadIdx.x; c < d.N; c += gridDim.x * TF) {
-    float x = lerN(n0.meia, n0.x, c) * invEscala;
-    const int t = ldcg8(d.tipo + c);
-    if (a.bolhas && t == AR) {
-      uint32_t b = __ldcg(d.rotulo + c);
-      if (b >= 2 && b < (uint32_t)MAX_BOLHAS) {
-        unsigned cels = __ldcg(d.celsB + b);
-        if (cels > 0) {
-          somaFixa(&a.accZ[b], (double)x / cels, ESC);
-          zNovo[c] = 0.0f;
-          continue;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int c = c0 + k * GT;
+      if (c >= N) continue;
+      const int mk = m[k];
+      float pq[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) pq[q] = prim ? zv[k][q] : zv[k][q] + betaf * pw[k][q];
+      if (mk & OP_AGUA) {
+        // water neighbours in the order left, right, down, up; air of an active bubble
+        // contributes its bubble's p
+        float sv = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          if (mk & (1 << q)) sv += pq[q + 1];
+          else if (mk & OP_VIZ_BOLHA) {
+            const int i = c % nx, j = c / nx;
+            const bool existe = q == 0 ? i > 0 : q == 1 ? i < nx - 1 : q == 2 ? j > 0 : j < ny - 1;
+            if (!existe) continue;
+            const int n = q == 0 ? c - 1 : q == 1 ? c + 1 : q == 2 ? c - nx : c + nx;
+            if (ldcg8(d.tipo + n) != AR) continue;
+            const uint32_t r = __ldcg(d.rotulo + n);
+            if (bolhaAtiva(a, r)) sv += (float)pbNovoV((int)r);
+          }
+        }
+        const float apc = (float)(mk >> 8) * pq[0] - sv;
+        pn[c] = pq[0];
+        d.ap[c] = apc;
+        s += (double)pq[0] * apc;
+      } else {
+        pn[c] = 0.0f;
+        d.ap[c] = 0.0f;
+        if (mk & OP_FACE) {  // the bubble's row: sum of p over its water faces
+          double t = 0;
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (mk & (1 << q)) t += (double)pq[q + 1];
+          if (t != 0) somaFixa(&d.accB[__ldcg(d.rotulo + c)], t, ESC);
         }
       }
     }
-    zNovo[c] = x;
-    if (t == AGUA) {
-      double r = __ldcg(d.r + c);
-      s0 += r * (double)x;
-      if (zVelho) s1 += r * (double)__ldcg(zVelho + c);
-    }
   }
-  double t0 = somaBloco(s0, sh);
-  double t1 = somaBloco(s1, sh);
-  if (threadIdx.x == 0) {
-    a.parc[blockIdx.x * NPARC + 0] = t0;
-    a.parc[blockIdx.x * NPARC + 1] = t1;
-  }
+  const double tb = somaBloco(s, sh);
+  if (threadIdx.x == 0) a.parc[blockIdx.x * NPARC + 0] = tb;
 }
 
 // ---------------------------------------------------------------- the kernel
@@ -991,6 +1243,27 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       n.viz[c] = (uint8_t)m;
     }
   }
+  for (int c = gt0; c < N; c += GT) {  // the operator descriptor (bubble faces are complete)
+    const int i = c % nx, j = c / nx;
+    const int t = d.tipo[c];
+    int m = 0, livres = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const bool existe = k == 0 ? i > 0 : k == 1 ? i < nx - 1 : k == 2 ? j > 0 : j < ny - 1;
+      if (!existe) continue;
+      const int nb = k == 0 ? c - 1 : k == 1 ? c + 1 : k == 2 ? c - nx : c + nx;
+      const int tn = d.tipo[nb];
+      if (tn != SOLIDO) livres++;
+      if (tn == AGUA) m |= 1 << k;
+      else if (a.bolhas && tn == AR && bolhaAtiva(a, d.rotulo[nb])) m |= OP_VIZ_BOLHA;
+    }
+    if (t == AGUA) m |= OP_AGUA;
+    if (a.bolhas && t == AR && bolhaAtiva(a, d.rotulo[c])) {
+      m |= OP_BOLHA;
+      if (i >= 1 && j >= 1 && i < nx - 1 && j < ny - 1) m |= OP_FACE;
+    }
+    a.op[c] = (uint16_t)(m | (livres << 8));
+  }
   if (a.bolhas) {
     for (int c = gt0; c < N; c += GT) {
       uint32_t b = d.rotulo[c];
@@ -1022,7 +1295,6 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
   }
   if (!barreira(a, ep)) return;
   const int nAt = a.bolhas ? __ldcg(a.nAtivos) : 0;
-  const NivelF n0 = a.niv[0];
 
   // ---- r = -div - A q (js/pressao-cpu.js:331-338), bubble aq sums
   {
@@ -1058,6 +1330,8 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       a.parc[blockIdx.x * NPARC + 1] = 0.0;
     }
   }
+  // the coarsest level's matrix (its neighbour masks are complete since the last barrier)
+  if (blockIdx.x == 0 && a.offDenso >= 0) montarDenso(a, dyn);
   if (!barreira(a, ep)) return;
   // rb = rhs - (faces*y - sum) (js/pressao-cpu.js:339-341); norm0
   auto rbInicial = [&](int b) {
@@ -1079,17 +1353,13 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
   }
   if (!barreira(a, ep)) return;  // rb visible before spreading
   float escala = (a.escalar && norma0 > 0) ? (float)(1.0 / norma0) : 1.0f;
-  faseEspalhar(a, n0, escala);
   if (blockIdx.x == 0)
     for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) {
       a.accZ[b] = 0;
       d.accB[b] = 0;
     }
-  if (!barreira(a, ep)) return;
-  if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff)) return;
+  if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, d.z, nullptr}, sh)) return;
   int cz = 0, cp = 0;  // which of the two z / p buffers holds the latest values
-  faseJuntar(a, n0, 1.0f / escala, d.z, nullptr, sh);
-  if (!barreira(a, ep)) return;
   auto zbAtual = [&](int b) { return (double)__ldcg(&a.accZ[b]) / ESC; };
   somasGlobais(a, nAt, [&](int b) { return __ldcg(&d.rb[b]) * zbAtual(b); }, [](int) { return 0.0; }, sh, somas);
   double rz = somas[0] + somas[2];
@@ -1115,7 +1385,6 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     }
     const float betaf = (float)beta;
     const bool prim = primeira;
-    auto pNovo = [&](int n) { return prim ? __ldcg(zc + n) : __ldcg(zc + n) + betaf * __ldcg(pv + n); };
     auto pbNovoV = [&](int b) { return prim ? zbAtual(b) : zbAtual(b) + beta * __ldcg(&pbVelho[b]); };
     if (blockIdx.x == 0)
       for (int k = threadIdx.x; k < nAt; k += TF) {
@@ -1123,36 +1392,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
         zbCur[b] = zbAtual(b);
         pbNovo[b] = pbNovoV(b);
       }
-    {
-      double s = 0;
-      for (int c = gt0; c < N; c += GT) {
-        if (d.tipo[c] != AGUA) {
-          pn[c] = 0.0f;
-          d.ap[c] = 0.0f;
-          continue;
-        }
-        const float pc = pNovo(c);
-        pn[c] = pc;
-        const float apc = aplicarF(a, c, pNovo, [&](uint32_t r) { return (float)pbNovoV((int)r); });
-        d.ap[c] = apc;
-        s += (double)pc * apc;
-      }
-      if (a.bolhas)
-        for (int c = gt0; c < N; c += GT) {
-          const int i = c % nx, j = c / nx;
-          if (i < 1 || j < 1 || i >= nx - 1 || j >= ny - 1) continue;
-          uint32_t b = d.rotulo[c];
-          if (d.tipo[c] != AR || !bolhaAtiva(a, b)) continue;
-          double t = 0;
-          if (d.tipo[c - 1] == AGUA) t += (double)pNovo(c - 1);
-          if (d.tipo[c + 1] == AGUA) t += (double)pNovo(c + 1);
-          if (d.tipo[c - nx] == AGUA) t += (double)pNovo(c - nx);
-          if (d.tipo[c + nx] == AGUA) t += (double)pNovo(c + nx);
-          if (t != 0) somaFixa(&d.accB[b], t, ESC);
-        }
-      double tb = somaBloco(s, sh);
-      if (threadIdx.x == 0) a.parc[blockIdx.x * NPARC + 0] = tb;
-    }
+    faseDA(a, zc, pv, pn, prim, betaf, beta, pbVelho, sh);
     if (!barreira(a, ep)) return;
     // ---- [B] alpha; q += alpha p, r -= alpha Ap; bubbles; r.r
     auto apbV = [&](int b) {
@@ -1164,12 +1404,27 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     {
       const float af = (float)alfa;
       double s = 0;
-      for (int c = gt0; c < N; c += GT) {
-        if (d.tipo[c] != AGUA) continue;
-        d.q[c] = d.q[c] + af * __ldcg(pn + c);
-        const float rv = d.r[c] - af * __ldcg(d.ap + c);
-        d.r[c] = rv;
-        s += (double)rv * rv;
+      for (int c0 = gt0; c0 < N; c0 += 4 * GT) {  // batches of 4 cells: all loads first
+        int m[4];
+        float qv[4], pnv[4], rv[4], apv[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const int c = c0 + k * GT < N ? c0 + k * GT : 0;
+          m[k] = c0 + k * GT < N ? __ldcg(a.op + c) : 0;
+          qv[k] = __ldcg(d.q + c);
+          pnv[k] = __ldcg(pn + c);
+          rv[k] = __ldcg(d.r + c);
+          apv[k] = __ldcg(d.ap + c);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          if (!(m[k] & OP_AGUA)) continue;
+          const int c = c0 + k * GT;
+          d.q[c] = qv[k] + af * pnv[k];
+          const float r = rv[k] - af * apv[k];
+          d.r[c] = r;
+          s += (double)r * r;
+        }
       }
       if (blockIdx.x == 0) {
         double sb = 0;
@@ -1199,13 +1454,9 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     }
     if (fim) break;
     escala = (a.escalar && norma > 0) ? (float)(1.0 / norma) : 1.0f;
-    faseEspalhar(a, n0, escala);
     if (blockIdx.x == 0)
       for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) d.accB[b] = 0;
-    if (!barreira(a, ep)) return;
-    if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff)) return;
-    faseJuntar(a, n0, 1.0f / escala, zo, zc, sh);
-    if (!barreira(a, ep)) return;
+    if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, zo, zc}, sh)) return;
     cz ^= 1;
     cp ^= 1;
     primeira = false;
@@ -1234,7 +1485,7 @@ Fundido* criarFundido(Pcg* p) {
   for (int l = p->L - 1; l >= 1; l--) {
     size_t n = (size_t)p->nxL[l] * p->nyL[l];
     size_t b = 3 * ((n * 4 + 15) & ~(size_t)15) + ((n + 15) & ~(size_t)15);
-    if (bytes + b + TILES_SECAO > SMEM_GROSSO_MAX) break;
+    if (bytes + b + TILES_SECAO > SMEM_GROSSO_MAX || (n > SECAO_MAX_CELULAS && l < p->L - 1)) break;
     bytes += b;
     Lc = l;
   }
@@ -1246,13 +1497,21 @@ Fundido* criarFundido(Pcg* p) {
   size_t porWarp = (size_t)(SUAV_W > REST_W ? SUAV_W : REST_W) * 4;
   size_t areas = (size_t)WARPS * porWarp;
   f->smem = bytes + TILES_SECAO > areas ? bytes + TILES_SECAO : areas;
+  {  // the coarsest level's matrix after everything else, when the level is small enough
+    const size_t nGrosso = (size_t)p->nxL[p->L - 1] * p->nyL[p->L - 1];
+    const size_t off = (f->smem + 15) & ~(size_t)15;
+    if (nGrosso <= (size_t)DENSO_MAPA_MAX && off + DENSO_BYTES <= SMEM_CTA_MAX) {
+      f->offDenso = (int)off;
+      f->smem = off + DENSO_BYTES;
+    }
+  }
   f->kern = p->precisao == TQ_PREC_FP16   ? kernelDe<__half>()
             : p->precisao == TQ_PREC_BF16 ? kernelDe<__nv_bfloat16>()
                                           : kernelDe<float>();
   int dev = 0, sms = 0, porSM = 0;
   // The attribute is per kernel and shared by every solver in the process: raise it to the
-  // largest size any grid uses (f->smem <= SMEM_GROSSO_MAX), never lower it to this grid's.
-  const size_t smemMax = SMEM_GROSSO_MAX > areas ? SMEM_GROSSO_MAX : areas;
+  // largest size any grid uses (f->smem <= SMEM_CTA_MAX), never lower it to this grid's.
+  const size_t smemMax = SMEM_CTA_MAX;
   bool ok = cudaGetDevice(&dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
             cudaFuncSetAttribute(f->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemMax) == cudaSuccess &&
@@ -1270,7 +1529,7 @@ Fundido* criarFundido(Pcg* p) {
          cudaMalloc(&f->ativos, MAX_BOLHAS * sizeof(int)) == cudaSuccess &&
          cudaMalloc(&f->nAtivos, sizeof(int)) == cudaSuccess && cudaMalloc(&f->p2, N * 4) == cudaSuccess &&
          cudaMalloc(&f->z2, N * 4) == cudaSuccess && cudaMalloc(&f->xc, nLc * 4) == cudaSuccess &&
-         cudaMalloc(&f->bc, nLc * 4) == cudaSuccess;
+         cudaMalloc(&f->bc, nLc * 4) == cudaSuccess && cudaMalloc(&f->op, N * sizeof(uint16_t)) == cudaSuccess;
   }
   if (ok) {
     NivelF tab[MAX_NIVEIS] = {};
@@ -1299,7 +1558,7 @@ Fundido* criarFundido(Pcg* p) {
 void destruirFundido(Fundido* f) {
   if (!f) return;
   void* ps[] = {f->niveis, f->parc, f->bar, f->erro, f->accZ, f->zb2, f->pb2, f->ativos,
-                f->nAtivos, f->p2, f->z2, f->xc, f->bc, f->perfil};
+                f->nAtivos, f->p2, f->z2, f->xc, f->bc, f->perfil, f->op};
   for (void* q : ps)
     if (q) cudaFree(q);
   delete f;
@@ -1329,6 +1588,8 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   a.z2 = f->z2;
   a.xc = f->xc;
   a.bc = f->bc;
+  a.offDenso = f->offDenso;
+  a.op = f->op;
   a.perfil = f->perfilar ? f->perfil : nullptr;
   if (a.perfil) {
     cudaMemsetAsync(f->perfil, 0, sizeof(unsigned long long), s);
