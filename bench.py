@@ -47,6 +47,9 @@ MAX_ITER = 200
 # first V-cycle).
 BYTES_ITER = {"fp32": 156.0, "fp16": 120.0, "bf16": 120.0}
 BYTES_SETUP = {"fp32": 110.0, "fp16": 85.0, "bf16": 85.0}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fused FP16 solve of this
+# scene, from one ncu capture of the kernel: the solve's working set stays in L2.
+TRAFEGO_SOLVE_BYTES = 167_721_472
 
 
 def picos():
@@ -59,41 +62,16 @@ def picos():
 
 
 # ------------------------------------------------------------------ scene
-def construir_cena(Cena, semente, labirinto, semear):
-    """Walls and water of the ultra scene; returns (cena, traces, particles, faucet)."""
-    cena = Cena(NX, NY, H)
-    W, Hh = cena.largura, cena.altura
-    tam = 12 * H
-    colunas, linhas = 56, 22
-    x0 = (W - colunas * tam) / 2
-    y0 = 0.40 * Hh
-    lab = labirinto(W, Hh, H, semente(3), linhas=linhas, corredor=tam, raio=2 * H, x0=x0, y0=y0, colunas=colunas)
-    for t in lab["tracos"]:
-        cena.tracar(t["x0"], t["y0"], t["x1"], t["y1"], t["raio"])
-    m = 2 * H
-    agua = semear(m, m, W - m, 0.85 * Hh, H, (0.0, 0.0, 0.0), s=3)
-    torneira = dict(x=lab["X"](0) + tam / 2, y=lab["Y"](linhas) + 10 * H, raio=6 * H, vx=0.0, vy=-1.2)
-    return cena, lab["tracos"], agua, torneira
+def construir_cena(Cena, *_):
+    """Walls and water of the ultra scene (tanque.cenarios.cena_ultra): (cena, traces, particles, faucet)."""
+    from tanque.cenarios import cena_ultra
+    return cena_ultra(Cena, NX, NY, H)
 
 
 def jato(torneira, quadro, dt=DT_QUADRO):
-    """emitirTorneira (js/principal.js:301-321) with a seeded LCG in place of Math.random:
-    particles in a disk of the jet's radius, at the jet velocity."""
-    from tanque.cenarios import semente
-    r0 = torneira["raio"]
-    vx, vy = torneira["vx"], torneira["vy"]
-    vazao = 2 * r0 * max(0.7, math.hypot(vx, vy))
-    n = min(40000, round((vazao * dt) / (H * H) * 4))
-    al = semente(1000 + quadro)
-    lista = np.zeros((n, 12), dtype=np.float32)
-    for k in range(n):
-        a = al() * math.pi * 2
-        r = math.sqrt(al()) * r0
-        lista[k, 0] = torneira["x"] + math.cos(a) * r
-        lista[k, 1] = torneira["y"] + math.sin(a) * r
-        lista[k, 2] = vx
-        lista[k, 3] = vy
-    return lista.ravel()
+    """The faucet's particles of frame `quadro` (tanque.cenarios.jato_torneira)."""
+    from tanque.cenarios import jato_torneira
+    return jato_torneira(torneira, quadro, dt)
 
 
 # ------------------------------------------------------------------ clocks
@@ -338,7 +316,8 @@ def executar_gpu(args, rank, mundo, dist):
                                   for k in SimulacaoGPU.ETAPAS},
         "roofline": {"kernel": "MGPCG pressure solve", "bound": "hbm", "achieved": round(r_m["gbs"], 1),
                      "peak": hbm, "peak_source": origem_pico, "unit": "GB/s",
-                     "frac": round(r_m["gbs"] / hbm, 4), "traffic": None,
+                     "frac": round(r_m["gbs"] / hbm, 4),
+                     "traffic": TRAFEGO_SOLVE_BYTES if motor_misto == _abi.TQ_ENGINE_FUSED else None,
                      "bytes_per_launch": round(r_m["bytes"])},
         "e2e": {"value": round(valor_e2e, 2), "unit": "steps/s", "h2d_bytes_per_step": int(e2e["h2d"]),
                 "d2h_bytes_per_step": int(e2e["d2h"])},

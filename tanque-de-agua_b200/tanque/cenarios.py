@@ -257,3 +257,44 @@ def montar_modelo(nome, nx, ny, h, aleatorio, Cena, fabrica):
     for a in m["agua"]:
         sim.adicionar(semear_agua(a, h, (0.0, 0.0, 0.0), aleatorio), False)
     return cena, sim, m
+
+
+# ------------------------------------------------------------------ the ultra scene
+def cena_ultra(Cena, nx: int = 840, ny: int = 536, h: float = 0.0016):
+    """The 450k-cell scene of the throughput benchmark: a seeded labyrinth (56 x 22 cells of 12h,
+    walls of radius 2h, from 40 % of the height) over water filling the tank to 85 %, and a
+    faucet 12 cells wide at 1.2 m/s at the labyrinth's entrance (js/principal.js:301-321).
+    Returns (cena, wall traces, particles, faucet)."""
+    cena = Cena(nx, ny, h)
+    W, Hh = cena.largura, cena.altura
+    tam = 12 * h
+    colunas, linhas = 56, 22
+    x0 = (W - colunas * tam) / 2
+    y0 = 0.40 * Hh
+    lab = labirinto(W, Hh, h, semente(3), linhas=linhas, corredor=tam, raio=2 * h, x0=x0, y0=y0, colunas=colunas)
+    for t in lab["tracos"]:
+        cena.tracar(t["x0"], t["y0"], t["x1"], t["y1"], t["raio"])
+    m = 2 * h
+    agua = semear_retangulo_rapido(m, m, W - m, 0.85 * Hh, h, (0.0, 0.0, 0.0), s=3)
+    torneira = dict(x=lab["X"](0) + tam / 2, y=lab["Y"](linhas) + 10 * h, raio=6 * h, vx=0.0, vy=-1.2, h=h)
+    return cena, lab["tracos"], agua, torneira
+
+
+def jato_torneira(torneira: dict, quadro: int, dt: float) -> np.ndarray:
+    """emitirTorneira (js/principal.js:301-321) with a seeded LCG in place of Math.random:
+    particles in a disk of the jet's radius, at the jet velocity, for frame `quadro`."""
+    h = torneira["h"]
+    r0 = torneira["raio"]
+    vx, vy = torneira["vx"], torneira["vy"]
+    vazao = 2 * r0 * max(0.7, math.hypot(vx, vy))
+    n = min(40000, round((vazao * dt) / (h * h) * 4))
+    al = semente(1000 + quadro)
+    lista = np.zeros((n, CAMPOS), dtype=np.float32)
+    for k in range(n):
+        a = al() * math.pi * 2
+        r = math.sqrt(al()) * r0
+        lista[k, 0] = torneira["x"] + math.cos(a) * r
+        lista[k, 1] = torneira["y"] + math.sin(a) * r
+        lista[k, 2] = vx
+        lista[k, 3] = vy
+    return lista.ravel()
