@@ -105,6 +105,10 @@ struct Args {
   unsigned long long* perfil;  // [0] count, [1..] %globaltimer at each barrier (null: off)
 };
 
+// The level table, copied into shared memory at kernel start: every phase reads its level's
+// sizes and pointers without an L2 round trip in front of its first data load.
+__shared__ NivelF s_niv[MAX_NIVEIS];
+
 // Phase trace of the fused solve (the %globaltimer at every grid barrier of the last solve).
 void perfilFundido(Fundido* f, bool ligar) {
   if (!f) return;
@@ -294,12 +298,11 @@ __device__ __forceinline__ float inversoVizinhos(int k) {
   return k == 1 ? 1.0f : k == 2 ? 0.5f : k == 3 ? (1.0f / 3.0f) : 0.25f;
 }
 
-// One half-sweep of colour COR over the lane's four cells of that colour (tile offsets li + dc).
+// One half-sweep of colour cor over the lane's four cells of that colour (tile offsets li + dc).
 // A cell reads only cells of the other colour and itself, so all loads go before the stores; a
 // cell that does not change (dry, outside the grid, or no free neighbour) stores its own value.
-template <int COR>
 __device__ __forceinline__ void meiaVarredura(float* tile, const int (&li)[4], int dc, const int (&vz)[8],
-                                              const float (&bv)[8], const float (&inv)[8]) {
+                                              const float (&bv)[8], const float (&inv)[8], int cor) {
   float nb[4][5];
 #pragma unroll
   for (int mm = 0; mm < 4; mm++) {
@@ -312,7 +315,7 @@ __device__ __forceinline__ void meiaVarredura(float* tile, const int (&li)[4], i
   }
 #pragma unroll
   for (int mm = 0; mm < 4; mm++) {
-    const int v = vz[4 * COR + mm];
+    const int v = cor ? vz[4 + mm] : vz[mm];
     const int mk = v & 15;
     float s = 0.0f;
     s += (mk & 1) ? nb[mm][0] : 0.0f;
@@ -320,7 +323,7 @@ __device__ __forceinline__ void meiaVarredura(float* tile, const int (&li)[4], i
     s += (mk & 4) ? nb[mm][2] : 0.0f;
     s += (mk & 8) ? nb[mm][3] : 0.0f;
     const float q = nb[mm][4];
-    const float novo = q + ((s + bv[4 * COR + mm]) * inv[4 * COR + mm] - q);
+    const float novo = q + ((s + (cor ? bv[4 + mm] : bv[mm])) * (cor ? inv[4 + mm] : inv[mm]) - q);
     tile[li[mm] + dc] = ((v & 16) && mk) ? novo : q;
   }
   __syncwarp();
@@ -338,18 +341,10 @@ __device__ __forceinline__ void varrerTile(float* tile, const int (&vz)[8], cons
   float inv[8];
 #pragma unroll
   for (int m = 0; m < 8; m++) inv[m] = inversoVizinhos(__popc(vz[m] & 15));
-  if (ordem == 0) {
-#pragma unroll
-    for (int it = 0; it < VARREDURAS; it++) {
-      meiaVarredura<0>(tile, li, par, vz, bv, inv);
-      meiaVarredura<1>(tile, li, par ^ 1, vz, bv, inv);
-    }
-  } else {
-#pragma unroll
-    for (int it = 0; it < VARREDURAS; it++) {
-      meiaVarredura<1>(tile, li, par ^ 1, vz, bv, inv);
-      meiaVarredura<0>(tile, li, par, vz, bv, inv);
-    }
+#pragma unroll 1
+  for (int h = 0; h < 2 * VARREDURAS; h++) {
+    const int cor = (h & 1) ^ ordem;
+    meiaVarredura(tile, li, cor ? par ^ 1 : par, vz, bv, inv, cor);
   }
 }
 
@@ -374,154 +369,252 @@ struct Reuniao {
   const float* zVelho;   // previous z (r.zOld), or null
 };
 
-// suavizar (js/pressao-cpu.js:99-150) for one 16x16 block, by one warp, cells as in
-// celulaBloco.  Every global load of the block goes out in one batch before the first
-// shared-memory store: a load-then-store sequence would wait for each L2 round trip in turn.
+// ---------------------------------------------------------------- register-resident block sweep
+// Lane l of the warp that owns a 16x16 block holds the cells (m, j) = row g + 4m, column 2k + j
+// (g = l >> 3, k = l & 7, m = 0..3, j = 0..1), and the block's frame cells next to them: left
+// and right of its rows (k = 0, k = 7), below and above its columns (g = 0, g = 3).  A cell's
+// colour is (row + column + 1) & 1 (js/pressao-cpu.js:120): in a half-sweep of colour COR the
+// lane updates its column j = (COR + 1 + g) & 1, and every neighbour is a cell of the other
+// colour: the lane's own other cell, the same rows in lane l -/+ 1, the rows below and above in
+// lanes l -/+ 8 (l +/- 24 with the next m across the group edge), or the frame.  Values move by
+// shuffles; the half-sweep reads only values that it does not write.
+struct Moldura {
+  float esq[4], dir[4];  // frame left / right of the lane's rows (k = 0 / k = 7)
+  float bai[2], cim[2];  // frame below / above the lane's columns (g = 0 / g = 3)
+};
+
+__device__ __forceinline__ void meiaReg(float (&x)[4][2], const int (&v)[4][2], const float (&bq)[4][2],
+                                        const float (&iq)[4][2], const Moldura& f, int cor) {
+  const int lane = threadIdx.x & 31, g = lane >> 3, k = lane & 7;
+  const int j = (cor + 1 + g) & 1;
+  float y[4], H[4], D[4], U[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) y[m] = j ? x[m][0] : x[m][1];
+  const int srcH = (j ? lane + 1 : lane - 1) & 31;
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    H[m] = __shfl_sync(0xffffffffu, y[m], srcH);
+    D[m] = __shfl_sync(0xffffffffu, y[m], (lane - 8) & 31);
+    U[m] = __shfl_sync(0xffffffffu, y[m], (lane + 8) & 31);
+  }
+  const float fb = j ? f.bai[1] : f.bai[0], fc = j ? f.cim[1] : f.cim[0];
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const float esq = j ? y[m] : (k == 0 ? f.esq[m] : H[m]);
+    const float dir = j ? (k == 7 ? f.dir[m] : H[m]) : y[m];
+    const float baixo = g >= 1 ? D[m] : (m >= 1 ? D[m > 0 ? m - 1 : 0] : fb);
+    const float cima = g <= 2 ? U[m] : (m <= 2 ? U[m < 3 ? m + 1 : 3] : fc);
+    const int vv = j ? v[m][1] : v[m][0];
+    const int mk = vv & 15;
+    float sm = 0.0f;
+    sm += (mk & 1) ? esq : 0.0f;
+    sm += (mk & 2) ? dir : 0.0f;
+    sm += (mk & 4) ? baixo : 0.0f;
+    sm += (mk & 8) ? cima : 0.0f;
+    const float q = j ? x[m][1] : x[m][0];
+    const float novo = q + ((sm + (j ? bq[m][1] : bq[m][0])) * (j ? iq[m][1] : iq[m][0]) - q);
+    const float r = ((vv & 16) && mk) ? novo : q;
+    x[m][0] = j ? x[m][0] : r;
+    x[m][1] = j ? r : x[m][1];
+  }
+}
+
+// The VARREDURAS red-black sweeps (js/pressao-cpu.js:114-137) of the warp's block in registers;
+// v = neighbour mask | 16 water | 128 in grid, bq = right side; ordem 0 sweeps colour 0 first.
+__device__ __forceinline__ void varrerReg(float (&x)[4][2], const int (&v)[4][2], const float (&bq)[4][2],
+                                         const Moldura& f, int ordem) {
+  float iq[4][2];
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+#pragma unroll
+    for (int j = 0; j < 2; j++) iq[m][j] = inversoVizinhos(__popc(v[m][j] & 15));
+  // one copy of the half-sweep in a rolled loop: the pass code stays small in the instruction
+  // cache, which each phase enters cold
+#pragma unroll 1
+  for (int h = 0; h < 2 * VARREDURAS; h++) meiaReg(x, v, bq, iq, f, (h & 1) ^ ordem);
+}
+
+// Bilinear coarse correction at fine cell (sx, sy) from the 11x11 coarse tile ct whose origin is
+// (cx0, cy0) (prolongar, js/pressao-cpu.js:191-214).
+__device__ __forceinline__ float correcaoGrossa(const float* ct, int cx0, int cy0, int sx, int sy) {
+  const int I0 = grossoBaseF(sx) - cx0, J0 = grossoBaseF(sy) - cy0;
+  const float wx0 = pesoBaseF(sx), wy0 = pesoBaseF(sy);
+  float e = 0.0f;
+#pragma unroll
+  for (int b = 0; b < 2; b++) {
+    const float wy = b ? 1.0f - wy0 : wy0;
+#pragma unroll
+    for (int aa = 0; aa < 2; aa++) e += ct[(J0 + b) * 11 + I0 + aa] * ((aa ? 1.0f - wx0 : wx0) * wy);
+  }
+  return e;
+}
+
+// suavizar (js/pressao-cpu.js:99-150) for one 16x16 block, by one warp, in registers (see
+// meiaReg).  Every global load of the block (cells, frame, flags, right side; with PROL the
+// coarse tile) goes out in one batch.
 template <class T, int MODO>
 __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, int blk, int nbx, int desl, int ordem,
                                               const T* src, T* dst, float* area, const NivelF& g,
                                               const float* xcSecao, const Reuniao& ru, double& s0, double& s1) {
   constexpr bool PROL = MODO == M_PROL;
   constexpr bool ZERO = MODO == M_ZERO || MODO == M_ESPALHAR;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, gl = lane >> 3, k = lane & 7;
   const int bx = blk % nbx, by = blk / nbx;
   const int ox = bx * 16 - desl, oy = by * 16 - desl;
   const int nx = n.nx, ny = n.ny;
-  float* tile = area;
-  float tv[11];
-  unsigned tAgua = 0;  // bit k: tile entry k is a water cell (PROL)
+  const T* b = (const T*)n.b;
+  float x[4][2], bq[4][2];
+  int v[4][2], cel[4][2];
+  int om[4][2];  // M_ESPALHAR: the cells' operator descriptors (bubble air)
+  Moldura f;
+  unsigned aguaF = 0;  // PROL: water flags of the frame cells (bits 0-3 left, 4-7 right, 8-9 below, 10-11 above)
 #pragma unroll
-  for (int k = 0; k < 11; k++) {
-    const int s = lane + 32 * k;
-    const int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
-    const bool ok = s < TILE && sx >= 0 && sy >= 0 && sx < nx && sy < ny;
-    tv[k] = (!ZERO && ok) ? carregar(ldcg(src + sx + sy * nx)) : 0.0f;
-    if (PROL) tAgua |= (unsigned)((ok ? ldcg8(n.viz + sx + sy * nx) : 0) >> 4 & 1) << k;
-  }
-  int vz[8];
-  float bv[8];
-  int cel[8];
-  {
-    const T* b = (const T*)n.b;
+  for (int m = 0; m < 4; m++)
 #pragma unroll
-    for (int m = 0; m < 8; m++) {
-      const int t = celulaBloco(lane, m);
-      const int gx = ox + (t & 15), gy = oy + (t >> 4);
+    for (int j = 0; j < 2; j++) {
+      const int gx = ox + 2 * k + j, gy = oy + gl + 4 * m;
       const bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
       const int c = gx + gy * nx;
-      cel[m] = dentro ? c : -1;
-      vz[m] = dentro ? (ldcg8(n.viz + c) | 128) : 0;
-      if (MODO == M_ESPALHAR) bv[m] = dentro ? __ldcg(a.d.r + c) : 0.0f;
-      else bv[m] = dentro ? carregar(ldcg(b + c)) : 0.0f;
+      cel[m][j] = dentro ? c : -1;
+      v[m][j] = dentro ? (ldcg8(n.viz + c) | 128) : 0;
+      x[m][j] = (!ZERO && dentro) ? carregar(ldcg(src + c)) : 0.0f;
+      if (MODO == M_ESPALHAR) {
+        bq[m][j] = dentro ? __ldcg(a.d.r + c) : 0.0f;
+        om[m][j] = (a.bolhas && dentro) ? __ldcg(a.op + c) : 0;
+      } else {
+        bq[m][j] = dentro ? carregar(ldcg(b + c)) : 0.0f;
+      }
+    }
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const int gy = oy + gl + 4 * m;
+    const int gxL = ox - 1, gxR = ox + 16;
+    const bool okL = k == 0 && gxL >= 0 && gy >= 0 && gy < ny;
+    const bool okR = k == 7 && gxR < nx && gy >= 0 && gy < ny;
+    f.esq[m] = (!ZERO && okL) ? carregar(ldcg(src + gxL + gy * nx)) : 0.0f;
+    f.dir[m] = (!ZERO && okR) ? carregar(ldcg(src + gxR + gy * nx)) : 0.0f;
+    if (PROL) {
+      aguaF |= (unsigned)((okL ? ldcg8(n.viz + gxL + gy * nx) : 0) >> 4 & 1) << m;
+      aguaF |= (unsigned)((okR ? ldcg8(n.viz + gxR + gy * nx) : 0) >> 4 & 1) << (4 + m);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int gx = ox + 2 * k + j;
+    const int gyB = oy - 1, gyT = oy + 16;
+    const bool okB = gl == 0 && gx >= 0 && gx < nx && gyB >= 0;
+    const bool okT = gl == 3 && gx >= 0 && gx < nx && gyT < ny;
+    f.bai[j] = (!ZERO && okB) ? carregar(ldcg(src + gx + gyB * nx)) : 0.0f;
+    f.cim[j] = (!ZERO && okT) ? carregar(ldcg(src + gx + gyT * nx)) : 0.0f;
+    if (PROL) {
+      aguaF |= (unsigned)((okB ? ldcg8(n.viz + gx + gyB * nx) : 0) >> 4 & 1) << (8 + j);
+      aguaF |= (unsigned)((okT ? ldcg8(n.viz + gx + gyT * nx) : 0) >> 4 & 1) << (10 + j);
     }
   }
   if (MODO == M_ESPALHAR) {
     // cells of active bubbles take their bubble's mean residual; b is stored in the storage
     // type and the sweep uses the stored value
 #pragma unroll
-    for (int m = 0; m < 8; m++) {
-      if (cel[m] < 0) continue;
-      float v = bv[m];
-      if (a.bolhas && (__ldcg(a.op + cel[m]) & OP_BOLHA)) {
-        const uint32_t rb = __ldcg(a.d.rotulo + cel[m]);
-        v = (float)(__ldcg(a.d.rb + rb) / __ldcg(a.d.celsB + rb));
+    for (int m = 0; m < 4; m++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        if (cel[m][j] < 0) continue;
+        float val = bq[m][j];
+        if (om[m][j] & OP_BOLHA) {
+          const uint32_t rb = __ldcg(a.d.rotulo + cel[m][j]);
+          val = (float)(__ldcg(a.d.rb + rb) / __ldcg(a.d.celsB + rb));
+        }
+        const T bt = guardar<T>(val * ru.escala);
+        ((T*)n.b)[cel[m][j]] = bt;
+        bq[m][j] = carregar(bt);
       }
-      const T bt = guardar<T>(v * ru.escala);
-      ((T*)n.b)[cel[m]] = bt;
-      bv[m] = carregar(bt);
-    }
   }
   if (PROL) {
-    // coarse tile: columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11, water x or 0
-    float* ct = area + TILE_AREA;
+    // coarse tile: columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11, water x or 0; the
+    // snapshot of every fine water cell, frame included, is x + P(x_coarse)
+    float* ct = area;
     const int cx0 = (ox - 2) >> 1, cy0 = (oy - 2) >> 1;
     float cv[4];
     int cz[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const int s = lane + 32 * k;
+    for (int kk = 0; kk < 4; kk++) {
+      const int s = lane + 32 * kk;
       const int I = cx0 + s % 11, J = cy0 + s / 11;
       const bool ok = s < CT && I >= 0 && J >= 0 && I < g.nx && J < g.ny;
       const int C = ok ? I + J * g.nx : 0;
-      cz[k] = ok ? ldcg8(g.viz + C) : 0;
-      cv[k] = ok ? (xcSecao ? __ldcg(xcSecao + C) : lerN(g.meia, g.x, C)) : 0.0f;
+      cz[kk] = ok ? ldcg8(g.viz + C) : 0;
+      cv[kk] = ok ? (xcSecao ? __ldcg(xcSecao + C) : lerN(g.meia, g.x, C)) : 0.0f;
     }
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const int s = lane + 32 * k;
-      if (s < CT) ct[s] = (cz[k] & 16) ? cv[k] : 0.0f;
+    for (int kk = 0; kk < 4; kk++) {
+      const int s = lane + 32 * kk;
+      if (s < CT) ct[s] = (cz[kk] & 16) ? cv[kk] : 0.0f;
     }
     __syncwarp();
 #pragma unroll
-    for (int k = 0; k < 11; k++) {
-      const int s = lane + 32 * k;
-      if (s < TILE && (tAgua >> k & 1)) {
-        const int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
-        const int I0 = grossoBaseF(sx) - cx0, J0 = grossoBaseF(sy) - cy0;
-        const float wx0 = pesoBaseF(sx), wy0 = pesoBaseF(sy);
-        float e = 0.0f;
+    for (int m = 0; m < 4; m++)
 #pragma unroll
-        for (int b = 0; b < 2; b++) {
-          const float wy = b ? 1.0f - wy0 : wy0;
+      for (int j = 0; j < 2; j++)
+        if (v[m][j] & 16) x[m][j] += correcaoGrossa(ct, cx0, cy0, ox + 2 * k + j, oy + gl + 4 * m);
 #pragma unroll
-          for (int aa = 0; aa < 2; aa++) e += ct[(J0 + b) * 11 + I0 + aa] * ((aa ? 1.0f - wx0 : wx0) * wy);
-        }
-        tv[k] = tv[k] + e;
-      }
+    for (int m = 0; m < 4; m++) {
+      const int gy = oy + gl + 4 * m;
+      if (aguaF >> m & 1) f.esq[m] += correcaoGrossa(ct, cx0, cy0, ox - 1, gy);
+      if (aguaF >> (4 + m) & 1) f.dir[m] += correcaoGrossa(ct, cx0, cy0, ox + 16, gy);
     }
-  }
 #pragma unroll
-  for (int k = 0; k < 11; k++) {
-    const int s = lane + 32 * k;
-    if (s < TILE) tile[(s / 18) * PT + s % 18] = tv[k];
+    for (int j = 0; j < 2; j++) {
+      const int gx = ox + 2 * k + j;
+      if (aguaF >> (8 + j) & 1) f.bai[j] += correcaoGrossa(ct, cx0, cy0, gx, oy - 1);
+      if (aguaF >> (10 + j) & 1) f.cim[j] += correcaoGrossa(ct, cx0, cy0, gx, oy + 16);
+    }
+    __syncwarp();
   }
-  __syncwarp();
-  varrerTile(tile, vz, bv, ordem);
+  varrerReg(x, v, bq, f, ordem);
   if (MODO == M_JUNTAR) {
     const float inv = 1.0f / ru.escala;
-    int om[8];
-    float rv[8], zv[8];
+    float rv[4][2], zv[4][2];
 #pragma unroll
-    for (int m = 0; m < 8; m++) {
-      const int c = cel[m] < 0 ? 0 : cel[m];
-      om[m] = cel[m] < 0 ? 0 : __ldcg(a.op + c);
-      rv[m] = __ldcg(a.d.r + c);
-      zv[m] = ru.zVelho ? __ldcg(ru.zVelho + c) : 0.0f;
-    }
+    for (int m = 0; m < 4; m++)
 #pragma unroll
-    for (int m = 0; m < 8; m++) {
-      if (cel[m] < 0) continue;
-      const int t = celulaBloco(lane, m);
-      const int li = ((t >> 4) + 1) * PT + (t & 15) + 1;
-      const float x = carregar(guardar<T>((vz[m] & 16) ? tile[li] : 0.0f)) * inv;
-      if (om[m] & OP_BOLHA) {
-        const uint32_t rb = __ldcg(a.d.rotulo + cel[m]);
-        somaFixa(&a.accZ[rb], (double)x / __ldcg(a.d.celsB + rb), ESC);
-        ru.zNovo[cel[m]] = 0.0f;
-        continue;
+      for (int j = 0; j < 2; j++) {
+        const int c = cel[m][j] < 0 ? 0 : cel[m][j];
+        om[m][j] = cel[m][j] < 0 ? 0 : __ldcg(a.op + c);
+        rv[m][j] = __ldcg(a.d.r + c);
+        zv[m][j] = ru.zVelho ? __ldcg(ru.zVelho + c) : 0.0f;
       }
-      ru.zNovo[cel[m]] = x;
-      if (om[m] & OP_AGUA) {
-        s0 += (double)rv[m] * (double)x;
-        if (ru.zVelho) s1 += (double)rv[m] * (double)zv[m];
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int c = cel[m][j];
+        if (c < 0) continue;
+        const float xz = carregar(guardar<T>((v[m][j] & 16) ? x[m][j] : 0.0f)) * inv;
+        if (om[m][j] & OP_BOLHA) {
+          const uint32_t rb = __ldcg(a.d.rotulo + c);
+          somaFixa(&a.accZ[rb], (double)xz / __ldcg(a.d.celsB + rb), ESC);
+          ru.zNovo[c] = 0.0f;
+          continue;
+        }
+        ru.zNovo[c] = xz;
+        if (om[m][j] & OP_AGUA) {
+          s0 += (double)rv[m][j] * (double)xz;
+          if (ru.zVelho) s1 += (double)rv[m][j] * (double)zv[m][j];
+        }
       }
-    }
   } else {
 #pragma unroll
-    for (int m = 0; m < 8; m++) {
-      if (cel[m] < 0) continue;
-      const int t = celulaBloco(lane, m);
-      const int li = ((t >> 4) + 1) * PT + (t & 15) + 1;
-      dst[cel[m]] = guardar<T>((vz[m] & 16) ? tile[li] : 0.0f);
-    }
+    for (int m = 0; m < 4; m++)
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+        if (cel[m][j] >= 0) dst[cel[m][j]] = guardar<T>((v[m][j] & 16) ? x[m][j] : 0.0f);
   }
-  __syncwarp();
 }
 
 template <class T, int MODO>
 __device__ __noinline__ void faseSuavizarT(const Args& a, int l, int desl, int ordem, bool paraTmp, float* areas,
                                            const Reuniao& ru, double* sh) {
-  const NivelF n = a.niv[l];
+  const NivelF n = s_niv[l];
   const int nbx = (n.nx + desl + 15) >> 4, nby = (n.ny + desl + 15) >> 4;
   const int nb = nbx * nby;
   const int w = threadIdx.x >> 5;
@@ -529,7 +622,7 @@ __device__ __noinline__ void faseSuavizarT(const Args& a, int l, int desl, int o
   const T* src = (const T*)(paraTmp ? n.x : n.tmp);
   T* dst = (T*)(paraTmp ? n.tmp : n.x);
   NivelF g{};
-  if (MODO == M_PROL) g = a.niv[l + 1];
+  if (MODO == M_PROL) g = s_niv[l + 1];
   const float* xcSecao = (MODO == M_PROL && l + 1 == a.Lc) ? a.xc : nullptr;
   double s0 = 0.0, s1 = 0.0;
   for (int blk = w * gridDim.x + blockIdx.x; blk < nb; blk += WARPS * gridDim.x)
@@ -572,8 +665,8 @@ __device__ void faseSuavizar(const Args& a, int l, int desl, int ordem, bool par
 // the warp's shared area, residuals computed once, then each lane sums its 4x4 window.
 template <class TFino>
 __device__ void faseRestringir(const Args& a, int l, float* areas) {
-  const NivelF f = a.niv[l];
-  const NivelF g = a.niv[l + 1];
+  const NivelF f = s_niv[l];
+  const NivelF g = s_niv[l + 1];
   const bool secao = l + 1 == a.Lc;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   float* xs = areas + w * REST_W;
@@ -732,7 +825,7 @@ __device__ __forceinline__ Denso denso(unsigned char* dyn, int off) {
 
 __device__ __noinline__ void montarDenso(const Args& a, unsigned char* dyn) {
   const Denso z = denso(dyn, a.offDenso);
-  const NivelF n = a.niv[a.L - 1];
+  const NivelF n = s_niv[a.L - 1];
   const int nx = n.nx, N = n.nx * n.ny;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int* mapa = (int*)z.M;  // cell -> list index, while the matrix is not written yet
@@ -827,7 +920,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
   if (threadIdx.x == 0) {
     int off = 0;  // bytes
     for (int l = a.Lc; l < a.L; l++) {
-      const NivelF n = a.niv[l];
+      const NivelF n = s_niv[l];
       const int N = n.nx * n.ny;
       NivelS& t = s[l];
       t.nx = n.nx;
@@ -847,7 +940,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
   float* tile = (float*)(smem + *tileOff) + w * TILE_AREA;
   for (int l = a.Lc; l < a.L; l++) {
     const NivelS t = s[l];
-    const uint8_t* viz = a.niv[l].viz;
+    const uint8_t* viz = s_niv[l].viz;
     const int N = t.nx * t.ny;
     for (int c0 = 0; c0 < N; c0 += 4 * TF) {  // loads in batches of 4 per thread
       int vv[4];
@@ -1048,7 +1141,7 @@ template <class T>
 __device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char* smem, NivelS* tabS, int* tileOff,
                        const Reuniao& ru, double* sh) {
   for (int l = 0; l < a.Lc; l++) {
-    const int meia = a.niv[l].meia;
+    const int meia = s_niv[l].meia;
     faseSuavizar<T>(a, l, 0, 0, true, l == 0 ? M_ESPALHAR : M_ZERO, areas, meia, ru, sh);
     if (!barreira(a, ep)) return false;
     faseSuavizar<T>(a, l, 8, 0, false, M_NORMAL, areas, meia, ru, sh);
@@ -1060,7 +1153,7 @@ __device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char*
   if (blockIdx.x == 0) secaoGrossa(a, smem, tabS, tileOff);
   if (!barreira(a, ep)) return false;
   for (int l = a.Lc - 1; l >= 0; l--) {
-    const int meia = a.niv[l].meia;
+    const int meia = s_niv[l].meia;
     faseSuavizar<T>(a, l, 8, 1, true, M_PROL, areas, meia, ru, sh);
     if (!barreira(a, ep)) return false;
     faseSuavizar<T>(a, l, 0, 1, false, l == 0 ? M_JUNTAR : M_NORMAL, areas, meia, ru, sh);
@@ -1091,10 +1184,12 @@ __device__ __forceinline__ float aplicarF(const Args& a, int c, FV val, FB valB)
   return (float)__popc(vz & 15) * val(c) - s;
 }
 
+constexpr int KDA = 4;  // cells per thread per batch in [DA]
+
 // [DA] of a PCG iteration over this CTA's cells: p = z + beta p (z alone on the first
 // iteration), A p (js/pressao-cpu.js:84-93, bubble neighbours through their p), the partial of
 // p.Ap (channel 0) and, for air of active bubbles, the sums over their water faces.  Cells go in
-// batches of 4 per thread: descriptors first, then every z and p the batch needs.
+// batches of KDA per thread: descriptors first, then every z and p the batch needs.
 __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float* pv, float* pn, bool prim, float betaf,
                                     double beta, const double* pbVelho, double* sh) {
   const Dev& d = a.d;
@@ -1105,16 +1200,16 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
     return prim ? zb : zb + beta * __ldcg(&pbVelho[b]);
   };
   double s = 0;
-  for (int c0 = gt0; c0 < N; c0 += 4 * GT) {
-    int m[4];
+  for (int c0 = gt0; c0 < N; c0 += KDA * GT) {
+    int m[KDA];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < KDA; k++) {
       const int c = c0 + k * GT;
       m[k] = c < N ? __ldcg(a.op + c) : 0;
     }
-    float zv[4][5], pw[4][5];
+    float zv[KDA][5], pw[KDA][5];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < KDA; k++) {
       const int c = c0 + k * GT < N ? c0 + k * GT : 0;
       const int mk = m[k];
       const int nb[5] = {c, (mk & 1) ? c - 1 : c, (mk & 2) ? c + 1 : c, (mk & 4) ? c - nx : c, (mk & 8) ? c + nx : c};
@@ -1125,7 +1220,7 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
       }
     }
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < KDA; k++) {
       const int c = c0 + k * GT;
       if (c >= N) continue;
       const int mk = m[k];
@@ -1184,10 +1279,12 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
   const int GT = gridDim.x * TF;
   unsigned ep = 0;
   double somas[4];
+  if (threadIdx.x < a.L) s_niv[threadIdx.x] = a.niv[threadIdx.x];
+  __syncthreads();
 
   // ---- setup: level-0 preconditioner types, operator masks, bubble faces
   {
-    uint8_t* t0 = a.niv[0].tipo;
+    uint8_t* t0 = s_niv[0].tipo;
     for (int c = gt0; c < N; c += GT) {
       const int t = d.tipo[c];
       const uint32_t rot = d.rotulo[c];
@@ -1211,8 +1308,8 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
   if (!barreira(a, ep)) return;
   // ---- coarse types (tiposGrossos, js/pressao-cpu.js:63-81), one level per phase
   for (int l = 1; l < a.L; l++) {
-    const NivelF f = a.niv[l - 1];
-    const NivelF g = a.niv[l];
+    const NivelF f = s_niv[l - 1];
+    const NivelF g = s_niv[l];
     for (int C = gt0; C < g.nx * g.ny; C += GT) {
       const int I = C % g.nx, J = C / g.nx;
       bool ar = false, agua = false;
@@ -1230,7 +1327,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
   }
   // ---- neighbour masks of every level, bubble cell counts, active list, initial y
   for (int l = 0; l < a.L; l++) {
-    const NivelF n = a.niv[l];
+    const NivelF n = s_niv[l];
     for (int c = gt0; c < n.nx * n.ny; c += GT) {
       const int i = c % n.nx, j = c / n.nx;
       const uint8_t* tp = n.tipo;
