@@ -47,14 +47,10 @@ constexpr int NPARC = 4;                           // partial slots per CTA
 constexpr int PERFIL_MAX = 1 << 16;                // phase-trace capacity
 constexpr int PERFIL_SECAO = 1 << 14;              // coarse-section stamps (after the phase trace)
 // per-warp shared-memory areas (floats)
-constexpr int TILE = 324;                          // 18x18 smoother tile (cells)
-constexpr int PT = 24;                             // its row pitch in shared memory: the sweeps'
-constexpr int TILE_AREA = 18 * PT;                 // strided loads then hit 32 distinct banks
 constexpr int CT = 121;                            // 11x11 coarse tile for the folded prolongation
-constexpr int SUAV_W = TILE_AREA + CT + 32;
+constexpr int SUAV_W = CT + 7;                     // the coarse tile of a PROL pass
 constexpr int RX = 6 * 68, RB = 4 * 66;            // restriction staging: x rows, b/viz/residual rows
 constexpr int REST_W = RX + 3 * RB;                // x, b, residual (floats) + viz (bytes in one RB)
-constexpr size_t TILES_SECAO = (size_t)WARPS * TILE_AREA * 4;  // per-warp tiles of the coarse section
 
 struct NivelF {
   int nx, ny, meia, pad;
@@ -235,15 +231,43 @@ template <class F0, class F1>
 __device__ void somasGlobais(const Args& a, int nAt, F0 f0, F1 f1, double* sh, double out[4]) {
   __syncthreads();
   if (threadIdx.x < 32) {
+    // Loads go out in batches before the sums (a rolled load-add loop waits one L2 round trip
+    // per step); each lane still adds its terms in ascending order.
     double v0 = 0, v1 = 0, b0 = 0, b1 = 0;
-    for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) {
-      v0 += __ldcg(&a.parc[k * NPARC + 0]);
-      v1 += __ldcg(&a.parc[k * NPARC + 1]);
+    constexpr int UC = 5;  // 5 x 32 slots cover one CTA per SM
+    for (int k0 = 0; k0 < (int)gridDim.x; k0 += 32 * UC) {
+      double p0[UC], p1[UC];
+#pragma unroll
+      for (int u = 0; u < UC; u++) {
+        const int k = k0 + threadIdx.x + 32 * u;
+        p0[u] = k < (int)gridDim.x ? __ldcg(&a.parc[k * NPARC + 0]) : 0.0;
+        p1[u] = k < (int)gridDim.x ? __ldcg(&a.parc[k * NPARC + 1]) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < UC; u++) {
+        v0 += p0[u];
+        v1 += p1[u];
+      }
     }
-    for (int k = threadIdx.x; k < nAt; k += 32) {
-      int b = __ldcg(&a.ativos[k]);
-      b0 += f0(b);
-      b1 += f1(b);
+    constexpr int UB = 4;
+    for (int k0 = 0; k0 < nAt; k0 += 32 * UB) {
+      int bs[UB];
+#pragma unroll
+      for (int u = 0; u < UB; u++) {
+        const int k = k0 + threadIdx.x + 32 * u;
+        bs[u] = k < nAt ? __ldcg(&a.ativos[k]) : -1;
+      }
+      double t0[UB], t1[UB];
+#pragma unroll
+      for (int u = 0; u < UB; u++) {
+        t0[u] = bs[u] >= 0 ? f0(bs[u]) : 0.0;
+        t1[u] = bs[u] >= 0 ? f1(bs[u]) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < UB; u++) {
+        b0 += t0[u];
+        b1 += t1[u];
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -282,70 +306,9 @@ __device__ __forceinline__ int grossoBaseF(int i) { return (i & 1) == 0 ? (i >> 
 __device__ __forceinline__ float pesoBaseF(int i) { return (i & 1) == 0 ? 0.25f : 0.75f; }
 
 // ---------------------------------------------------------------- block sweeps
-// Cell m (0..7) of lane l in a 16x16 block whose origin has even x + y (every block origin is
-// a multiple of 8): m < 4 are the lane's cells of colour 0, m >= 4 of colour 1, in rows
-// (l >> 3) + 4(m & 3) and the column pair 2(l & 7), 2(l & 7) + 1.  The colour of a cell is
-// (x + y + 1) & 1 (js/pressao-cpu.js:120), so every lane updates four cells in each half-sweep.
-// Returns row * 16 + column.
-__device__ __forceinline__ int celulaBloco(int lane, int m) {
-  const int row = (lane >> 3) + 4 * (m & 3);
-  const int col = 2 * (lane & 7) + (((m >> 2) + 1 + (lane >> 3)) & 1);
-  return row * 16 + col;
-}
-
 // 1/k for k free neighbours (k = 1..4), the correctly rounded float constants.
 __device__ __forceinline__ float inversoVizinhos(int k) {
   return k == 1 ? 1.0f : k == 2 ? 0.5f : k == 3 ? (1.0f / 3.0f) : 0.25f;
-}
-
-// One half-sweep of colour cor over the lane's four cells of that colour (tile offsets li + dc).
-// A cell reads only cells of the other colour and itself, so all loads go before the stores; a
-// cell that does not change (dry, outside the grid, or no free neighbour) stores its own value.
-__device__ __forceinline__ void meiaVarredura(float* tile, const int (&li)[4], int dc, const int (&vz)[8],
-                                              const float (&bv)[8], const float (&inv)[8], int cor) {
-  float nb[4][5];
-#pragma unroll
-  for (int mm = 0; mm < 4; mm++) {
-    const int p = li[mm] + dc;
-    nb[mm][0] = tile[p - 1];
-    nb[mm][1] = tile[p + 1];
-    nb[mm][2] = tile[p - PT];
-    nb[mm][3] = tile[p + PT];
-    nb[mm][4] = tile[p];
-  }
-#pragma unroll
-  for (int mm = 0; mm < 4; mm++) {
-    const int v = cor ? vz[4 + mm] : vz[mm];
-    const int mk = v & 15;
-    float s = 0.0f;
-    s += (mk & 1) ? nb[mm][0] : 0.0f;
-    s += (mk & 2) ? nb[mm][1] : 0.0f;
-    s += (mk & 4) ? nb[mm][2] : 0.0f;
-    s += (mk & 8) ? nb[mm][3] : 0.0f;
-    const float q = nb[mm][4];
-    const float novo = q + ((s + (cor ? bv[4 + mm] : bv[mm])) * (cor ? inv[4 + mm] : inv[mm]) - q);
-    tile[li[mm] + dc] = ((v & 16) && mk) ? novo : q;
-  }
-  __syncwarp();
-}
-
-// The VARREDURAS red-black sweeps of one 16x16 block on its 18x18 shared tile (row pitch PT)
-// (js/pressao-cpu.js:114-137), by one warp, cells as in celulaBloco; vz = neighbour mask |
-// 16 water | 128 in grid, bv = right side; ordem 0 sweeps colour 0 first.
-__device__ __forceinline__ void varrerTile(float* tile, const int (&vz)[8], const float (&bv)[8], int ordem) {
-  const int lane = threadIdx.x & 31;
-  int li[4];
-#pragma unroll
-  for (int mm = 0; mm < 4; mm++) li[mm] = ((lane >> 3) + 4 * mm + 1) * PT + 2 * (lane & 7) + 1;
-  const int par = (1 + (lane >> 3)) & 1;  // column offset of colour 0; colour 1 is the other one
-  float inv[8];
-#pragma unroll
-  for (int m = 0; m < 8; m++) inv[m] = inversoVizinhos(__popc(vz[m] & 15));
-#pragma unroll 1
-  for (int h = 0; h < 2 * VARREDURAS; h++) {
-    const int cor = (h & 1) ^ ordem;
-    meiaVarredura(tile, li, cor ? par ^ 1 : par, vz, bv, inv, cor);
-  }
 }
 
 // ---------------------------------------------------------------- grid-level smoother
@@ -370,68 +333,69 @@ struct Reuniao {
 };
 
 // ---------------------------------------------------------------- register-resident block sweep
-// Lane l of the warp that owns a 16x16 block holds the cells (m, j) = row g + 4m, column 2k + j
-// (g = l >> 3, k = l & 7, m = 0..3, j = 0..1), and the block's frame cells next to them: left
-// and right of its rows (k = 0, k = 7), below and above its columns (g = 0, g = 3).  A cell's
-// colour is (row + column + 1) & 1 (js/pressao-cpu.js:120): in a half-sweep of colour COR the
-// lane updates its column j = (COR + 1 + g) & 1, and every neighbour is a cell of the other
-// colour: the lane's own other cell, the same rows in lane l -/+ 1, the rows below and above in
-// lanes l -/+ 8 (l +/- 24 with the next m across the group edge), or the frame.  Values move by
-// shuffles; the half-sweep reads only values that it does not write.
+// Lane l of the warp that owns a 16x16 block holds, for each colour c and m = 0..3, the cell of
+// colour c in row g + 4m (g = l >> 3) among the columns 2k, 2k + 1 (k = l & 7): its column is
+// (c + 1 + g) & 1, since a cell's colour is (row + column + 1) & 1 (js/pressao-cpu.js:120).  It
+// also holds the block's frame next to its cells: left and right of its rows (k = 0, k = 7),
+// below and above its columns (g = 0, g = 3).  In a half-sweep of colour COR every neighbour of
+// an updated cell has the other colour: the lane's own other cell, the same rows in lane
+// l -/+ 1, the rows below and above in lanes l -/+ 8 (l +/- 24 with the next m across the group
+// edge), or the frame.  Values move by shuffles; a half-sweep reads no value that it writes.
+// Every snapshot holds x = 0 on cells that are not water (the passes store 0 there, the frame
+// outside the grid is 0), so a wall neighbour adds +0 and the sum needs no mask; only 1/k and
+// whether the cell changes come from the mask.
 struct Moldura {
   float esq[4], dir[4];  // frame left / right of the lane's rows (k = 0 / k = 7)
-  float bai[2], cim[2];  // frame below / above the lane's columns (g = 0 / g = 3)
+  float bai[2], cim[2];  // frame below / above the lane's columns (g = 0 / g = 3), by column
 };
 
-__device__ __forceinline__ void meiaReg(float (&x)[4][2], const int (&v)[4][2], const float (&bq)[4][2],
-                                        const float (&iq)[4][2], const Moldura& f, int cor) {
+template <int COR>
+__device__ __forceinline__ void meiaReg(float (&x)[2][4], const float (&bq)[2][4], const float (&iq)[2][4],
+                                        const float (&at)[2][4], const Moldura& f) {
   const int lane = threadIdx.x & 31, g = lane >> 3, k = lane & 7;
-  const int j = (cor + 1 + g) & 1;
-  float y[4], H[4], D[4], U[4];
-#pragma unroll
-  for (int m = 0; m < 4; m++) y[m] = j ? x[m][0] : x[m][1];
-  const int srcH = (j ? lane + 1 : lane - 1) & 31;
+  const int jc = (COR + 1 + g) & 1;  // the lane's column of colour COR
+  float H[4], D[4], U[4];
+  const int srcH = (jc ? lane + 1 : lane - 1) & 31;
 #pragma unroll
   for (int m = 0; m < 4; m++) {
-    H[m] = __shfl_sync(0xffffffffu, y[m], srcH);
-    D[m] = __shfl_sync(0xffffffffu, y[m], (lane - 8) & 31);
-    U[m] = __shfl_sync(0xffffffffu, y[m], (lane + 8) & 31);
+    H[m] = __shfl_sync(0xffffffffu, x[1 - COR][m], srcH);
+    D[m] = __shfl_sync(0xffffffffu, x[1 - COR][m], (lane - 8) & 31);
+    U[m] = __shfl_sync(0xffffffffu, x[1 - COR][m], (lane + 8) & 31);
   }
-  const float fb = j ? f.bai[1] : f.bai[0], fc = j ? f.cim[1] : f.cim[0];
+  const float fb = jc ? f.bai[1] : f.bai[0], fc = jc ? f.cim[1] : f.cim[0];
 #pragma unroll
   for (int m = 0; m < 4; m++) {
-    const float esq = j ? y[m] : (k == 0 ? f.esq[m] : H[m]);
-    const float dir = j ? (k == 7 ? f.dir[m] : H[m]) : y[m];
+    const float y = x[1 - COR][m];
+    const float esq = jc ? y : (k == 0 ? f.esq[m] : H[m]);
+    const float dir = jc ? (k == 7 ? f.dir[m] : H[m]) : y;
     const float baixo = g >= 1 ? D[m] : (m >= 1 ? D[m > 0 ? m - 1 : 0] : fb);
     const float cima = g <= 2 ? U[m] : (m <= 2 ? U[m < 3 ? m + 1 : 3] : fc);
-    const int vv = j ? v[m][1] : v[m][0];
-    const int mk = vv & 15;
-    float sm = 0.0f;
-    sm += (mk & 1) ? esq : 0.0f;
-    sm += (mk & 2) ? dir : 0.0f;
-    sm += (mk & 4) ? baixo : 0.0f;
-    sm += (mk & 8) ? cima : 0.0f;
-    const float q = j ? x[m][1] : x[m][0];
-    const float novo = q + ((sm + (j ? bq[m][1] : bq[m][0])) * (j ? iq[m][1] : iq[m][0]) - q);
-    const float r = ((vv & 16) && mk) ? novo : q;
-    x[m][0] = j ? x[m][0] : r;
-    x[m][1] = j ? r : x[m][1];
+    const float sm = ((esq + dir) + baixo) + cima;
+    const float q = x[COR][m];
+    const float dlt = (sm + bq[COR][m]) * iq[COR][m] - q;
+    x[COR][m] = fmaf(at[COR][m], dlt, q);  // at = 1 (the cell changes) or 0: exact either way
   }
 }
 
 // The VARREDURAS red-black sweeps (js/pressao-cpu.js:114-137) of the warp's block in registers;
 // v = neighbour mask | 16 water | 128 in grid, bq = right side; ordem 0 sweeps colour 0 first.
-__device__ __forceinline__ void varrerReg(float (&x)[4][2], const int (&v)[4][2], const float (&bq)[4][2],
+__device__ __forceinline__ void varrerReg(float (&x)[2][4], const int (&v)[2][4], const float (&bq)[2][4],
                                          const Moldura& f, int ordem) {
-  float iq[4][2];
+  float iq[2][4], at[2][4];
 #pragma unroll
-  for (int m = 0; m < 4; m++)
+  for (int c = 0; c < 2; c++)
 #pragma unroll
-    for (int j = 0; j < 2; j++) iq[m][j] = inversoVizinhos(__popc(v[m][j] & 15));
-  // one copy of the half-sweep in a rolled loop: the pass code stays small in the instruction
-  // cache, which each phase enters cold
+    for (int m = 0; m < 4; m++) {
+      const int mk = v[c][m] & 15;
+      iq[c][m] = inversoVizinhos(__popc(mk));
+      at[c][m] = ((v[c][m] & 16) && mk) ? 1.0f : 0.0f;
+    }
+  // rolled loop: the pass code stays small in the instruction cache, which each phase enters cold
 #pragma unroll 1
-  for (int h = 0; h < 2 * VARREDURAS; h++) meiaReg(x, v, bq, iq, f, (h & 1) ^ ordem);
+  for (int h = 0; h < 2 * VARREDURAS; h++) {
+    if (((h & 1) ^ ordem) == 0) meiaReg<0>(x, bq, iq, at, f);
+    else meiaReg<1>(x, bq, iq, at, f);
+  }
 }
 
 // Bilinear coarse correction at fine cell (sx, sy) from the 11x11 coarse tile ct whose origin is
@@ -463,26 +427,26 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   const int ox = bx * 16 - desl, oy = by * 16 - desl;
   const int nx = n.nx, ny = n.ny;
   const T* b = (const T*)n.b;
-  float x[4][2], bq[4][2];
-  int v[4][2], cel[4][2];
-  int om[4][2];  // M_ESPALHAR: the cells' operator descriptors (bubble air)
+  float x[2][4], bq[2][4];  // [colour][m], see meiaReg
+  int v[2][4], cel[2][4];
+  int om[2][4];  // M_ESPALHAR: the cells' operator descriptors (bubble air)
   Moldura f;
   unsigned aguaF = 0;  // PROL: water flags of the frame cells (bits 0-3 left, 4-7 right, 8-9 below, 10-11 above)
 #pragma unroll
-  for (int m = 0; m < 4; m++)
+  for (int cr = 0; cr < 2; cr++)
 #pragma unroll
-    for (int j = 0; j < 2; j++) {
-      const int gx = ox + 2 * k + j, gy = oy + gl + 4 * m;
+    for (int m = 0; m < 4; m++) {
+      const int gx = ox + 2 * k + ((cr + 1 + gl) & 1), gy = oy + gl + 4 * m;
       const bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
       const int c = gx + gy * nx;
-      cel[m][j] = dentro ? c : -1;
-      v[m][j] = dentro ? (ldcg8(n.viz + c) | 128) : 0;
-      x[m][j] = (!ZERO && dentro) ? carregar(ldcg(src + c)) : 0.0f;
+      cel[cr][m] = dentro ? c : -1;
+      v[cr][m] = dentro ? (ldcg8(n.viz + c) | 128) : 0;
+      x[cr][m] = (!ZERO && dentro) ? carregar(ldcg(src + c)) : 0.0f;
       if (MODO == M_ESPALHAR) {
-        bq[m][j] = dentro ? __ldcg(a.d.r + c) : 0.0f;
-        om[m][j] = (a.bolhas && dentro) ? __ldcg(a.op + c) : 0;
+        bq[cr][m] = dentro ? __ldcg(a.d.r + c) : 0.0f;
+        om[cr][m] = (a.bolhas && dentro) ? __ldcg(a.op + c) : 0;
       } else {
-        bq[m][j] = dentro ? carregar(ldcg(b + c)) : 0.0f;
+        bq[cr][m] = dentro ? carregar(ldcg(b + c)) : 0.0f;
       }
     }
 #pragma unroll
@@ -515,18 +479,18 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     // cells of active bubbles take their bubble's mean residual; b is stored in the storage
     // type and the sweep uses the stored value
 #pragma unroll
-    for (int m = 0; m < 4; m++)
+    for (int cr = 0; cr < 2; cr++)
 #pragma unroll
-      for (int j = 0; j < 2; j++) {
-        if (cel[m][j] < 0) continue;
-        float val = bq[m][j];
-        if (om[m][j] & OP_BOLHA) {
-          const uint32_t rb = __ldcg(a.d.rotulo + cel[m][j]);
+      for (int m = 0; m < 4; m++) {
+        if (cel[cr][m] < 0) continue;
+        float val = bq[cr][m];
+        if (om[cr][m] & OP_BOLHA) {
+          const uint32_t rb = __ldcg(a.d.rotulo + cel[cr][m]);
           val = (float)(__ldcg(a.d.rb + rb) / __ldcg(a.d.celsB + rb));
         }
         const T bt = guardar<T>(val * ru.escala);
-        ((T*)n.b)[cel[m][j]] = bt;
-        bq[m][j] = carregar(bt);
+        ((T*)n.b)[cel[cr][m]] = bt;
+        bq[cr][m] = carregar(bt);
       }
   }
   if (PROL) {
@@ -552,10 +516,10 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     }
     __syncwarp();
 #pragma unroll
-    for (int m = 0; m < 4; m++)
+    for (int cr = 0; cr < 2; cr++)
 #pragma unroll
-      for (int j = 0; j < 2; j++)
-        if (v[m][j] & 16) x[m][j] += correcaoGrossa(ct, cx0, cy0, ox + 2 * k + j, oy + gl + 4 * m);
+      for (int m = 0; m < 4; m++)
+        if (v[cr][m] & 16) x[cr][m] += correcaoGrossa(ct, cx0, cy0, ox + 2 * k + ((cr + 1 + gl) & 1), oy + gl + 4 * m);
 #pragma unroll
     for (int m = 0; m < 4; m++) {
       const int gy = oy + gl + 4 * m;
@@ -573,41 +537,41 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   varrerReg(x, v, bq, f, ordem);
   if (MODO == M_JUNTAR) {
     const float inv = 1.0f / ru.escala;
-    float rv[4][2], zv[4][2];
+    float rv[2][4], zv[2][4];
 #pragma unroll
-    for (int m = 0; m < 4; m++)
+    for (int cr = 0; cr < 2; cr++)
 #pragma unroll
-      for (int j = 0; j < 2; j++) {
-        const int c = cel[m][j] < 0 ? 0 : cel[m][j];
-        om[m][j] = cel[m][j] < 0 ? 0 : __ldcg(a.op + c);
-        rv[m][j] = __ldcg(a.d.r + c);
-        zv[m][j] = ru.zVelho ? __ldcg(ru.zVelho + c) : 0.0f;
+      for (int m = 0; m < 4; m++) {
+        const int c = cel[cr][m] < 0 ? 0 : cel[cr][m];
+        om[cr][m] = cel[cr][m] < 0 ? 0 : __ldcg(a.op + c);
+        rv[cr][m] = __ldcg(a.d.r + c);
+        zv[cr][m] = ru.zVelho ? __ldcg(ru.zVelho + c) : 0.0f;
       }
 #pragma unroll
-    for (int m = 0; m < 4; m++)
+    for (int cr = 0; cr < 2; cr++)
 #pragma unroll
-      for (int j = 0; j < 2; j++) {
-        const int c = cel[m][j];
+      for (int m = 0; m < 4; m++) {
+        const int c = cel[cr][m];
         if (c < 0) continue;
-        const float xz = carregar(guardar<T>((v[m][j] & 16) ? x[m][j] : 0.0f)) * inv;
-        if (om[m][j] & OP_BOLHA) {
+        const float xz = carregar(guardar<T>((v[cr][m] & 16) ? x[cr][m] : 0.0f)) * inv;
+        if (om[cr][m] & OP_BOLHA) {
           const uint32_t rb = __ldcg(a.d.rotulo + c);
           somaFixa(&a.accZ[rb], (double)xz / __ldcg(a.d.celsB + rb), ESC);
           ru.zNovo[c] = 0.0f;
           continue;
         }
         ru.zNovo[c] = xz;
-        if (om[m][j] & OP_AGUA) {
-          s0 += (double)rv[m][j] * (double)xz;
-          if (ru.zVelho) s1 += (double)rv[m][j] * (double)zv[m][j];
+        if (om[cr][m] & OP_AGUA) {
+          s0 += (double)rv[cr][m] * (double)xz;
+          if (ru.zVelho) s1 += (double)rv[cr][m] * (double)zv[cr][m];
         }
       }
   } else {
 #pragma unroll
-    for (int m = 0; m < 4; m++)
+    for (int cr = 0; cr < 2; cr++)
 #pragma unroll
-      for (int j = 0; j < 2; j++)
-        if (cel[m][j] >= 0) dst[cel[m][j]] = guardar<T>((v[m][j] & 16) ? x[m][j] : 0.0f);
+      for (int m = 0; m < 4; m++)
+        if (cel[cr][m] >= 0) dst[cel[cr][m]] = guardar<T>((v[cr][m] & 16) ? x[cr][m] : 0.0f);
   }
 }
 
@@ -758,43 +722,51 @@ struct NivelS {
 };
 
 // One smoother pass over a level held in shared memory: the level's 16x16 blocks are taken in
-// turn by the CTA's warps, each sweeping a tile read from `src` (varrerTile) and writing `dst`.
-__device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int ordem, int src, int dst,
-                       float* tile) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+// turn by the CTA's warps, each sweeping its block in registers (varrerReg) from the snapshot
+// `src` and writing `dst`.
+__device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int ordem, int src, int dst) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, gl = lane >> 3, k = lane & 7;
   const int nx = n.nx, ny = n.ny;
   const int nbx = (nx + desl + 15) >> 4, nby = (ny + desl + 15) >> 4;
   for (int blk = w; blk < nbx * nby; blk += WARPS) {
     const int ox = (blk % nbx) * 16 - desl, oy = (blk / nbx) * 16 - desl;
+    float x[2][4], bq[2][4];  // [colour][m], see meiaReg
+    int v[2][4], cel[2][4];
+    Moldura f;
 #pragma unroll
-    for (int k = 0; k < 11; k++) {
-      const int s = lane + 32 * k;
-      if (s < TILE) {
-        const int sx = s % 18 - 1 + ox, sy = s / 18 - 1 + oy;
-        tile[(s / 18) * PT + s % 18] = (sx >= 0 && sy >= 0 && sx < nx && sy < ny) ? F[src + sx + sy * nx] : 0.0f;
+    for (int cr = 0; cr < 2; cr++)
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const int gx = ox + 2 * k + ((cr + 1 + gl) & 1), gy = oy + gl + 4 * m;
+        const bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
+        const int c = gx + gy * nx;
+        cel[cr][m] = dentro ? c : -1;
+        v[cr][m] = dentro ? (U[n.v + c] | 128) : 0;
+        x[cr][m] = dentro ? F[src + c] : 0.0f;
+        bq[cr][m] = dentro ? F[n.b + c] : 0.0f;
       }
-    }
-    int vz[8];
-    float bv[8];
 #pragma unroll
-    for (int m = 0; m < 8; m++) {
-      const int t = celulaBloco(lane, m);
-      const int gx = ox + (t & 15), gy = oy + (t >> 4);
-      const bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
-      const int c = gx + gy * nx;
-      vz[m] = dentro ? (U[n.v + c] | 128) : 0;
-      bv[m] = dentro ? F[n.b + c] : 0.0f;
+    for (int m = 0; m < 4; m++) {
+      const int gy = oy + gl + 4 * m;
+      const bool okL = k == 0 && ox - 1 >= 0 && gy >= 0 && gy < ny;
+      const bool okR = k == 7 && ox + 16 < nx && gy >= 0 && gy < ny;
+      f.esq[m] = okL ? F[src + ox - 1 + gy * nx] : 0.0f;
+      f.dir[m] = okR ? F[src + ox + 16 + gy * nx] : 0.0f;
     }
-    __syncwarp();
-    varrerTile(tile, vz, bv, ordem);
 #pragma unroll
-    for (int m = 0; m < 8; m++) {
-      if (!(vz[m] & 128)) continue;
-      const int t = celulaBloco(lane, m);
-      const int gx = ox + (t & 15), gy = oy + (t >> 4);
-      F[dst + gx + gy * nx] = (vz[m] & 16) ? tile[((t >> 4) + 1) * PT + (t & 15) + 1] : 0.0f;
+    for (int j = 0; j < 2; j++) {
+      const int gx = ox + 2 * k + j;
+      const bool okB = gl == 0 && gx >= 0 && gx < nx && oy - 1 >= 0;
+      const bool okT = gl == 3 && gx >= 0 && gx < nx && oy + 16 < ny;
+      f.bai[j] = okB ? F[src + gx + (oy - 1) * nx] : 0.0f;
+      f.cim[j] = okT ? F[src + gx + (oy + 16) * nx] : 0.0f;
     }
-    __syncwarp();
+    varrerReg(x, v, bq, f, ordem);
+#pragma unroll
+    for (int cr = 0; cr < 2; cr++)
+#pragma unroll
+      for (int m = 0; m < 4; m++)
+        if (cel[cr][m] >= 0) F[dst + cel[cr][m]] = (v[cr][m] & 16) ? x[cr][m] : 0.0f;
   }
   __syncthreads();
 }
@@ -937,7 +909,6 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
     *tileOff = off;
   }
   __syncthreads();
-  float* tile = (float*)(smem + *tileOff) + w * TILE_AREA;
   for (int l = a.Lc; l < a.L; l++) {
     const NivelS t = s[l];
     const uint8_t* viz = s_niv[l].viz;
@@ -968,9 +939,9 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
   for (int l = a.Lc; l < a.L - 1; l++) {
     const NivelS f = s[l];
     const NivelS g = s[l + 1];
-    passoS(F, U, f, 0, 0, f.xa, f.xb, tile);
+    passoS(F, U, f, 0, 0, f.xa, f.xb);
     marcaSecao(a);
-    passoS(F, U, f, 8, 0, f.xb, f.xa, tile);
+    passoS(F, U, f, 8, 0, f.xb, f.xa);
     marcaSecao(a);
     // restringir: residuals of the fine level into its free x buffer, then the 4x4 gathers.
     // Out-of-range and dry neighbours enter with weight or value 0, which adds +0 to a sum.
@@ -1124,9 +1095,9 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
     }
     __syncthreads();
     marcaSecao(a);
-    passoS(F, U, f, 8, 1, f.xa, f.xb, tile);
+    passoS(F, U, f, 8, 1, f.xa, f.xb);
     marcaSecao(a);
-    passoS(F, U, f, 0, 1, f.xb, f.xa, tile);
+    passoS(F, U, f, 0, 1, f.xb, f.xa);
     marcaSecao(a);
   }
   const NivelS t = s[a.Lc];
@@ -1582,7 +1553,7 @@ Fundido* criarFundido(Pcg* p) {
   for (int l = p->L - 1; l >= 1; l--) {
     size_t n = (size_t)p->nxL[l] * p->nyL[l];
     size_t b = 3 * ((n * 4 + 15) & ~(size_t)15) + ((n + 15) & ~(size_t)15);
-    if (bytes + b + TILES_SECAO > SMEM_GROSSO_MAX || (n > SECAO_MAX_CELULAS && l < p->L - 1)) break;
+    if (bytes + b > SMEM_GROSSO_MAX || (n > SECAO_MAX_CELULAS && l < p->L - 1)) break;
     bytes += b;
     Lc = l;
   }
@@ -1593,7 +1564,7 @@ Fundido* criarFundido(Pcg* p) {
   f->Lc = Lc;
   size_t porWarp = (size_t)(SUAV_W > REST_W ? SUAV_W : REST_W) * 4;
   size_t areas = (size_t)WARPS * porWarp;
-  f->smem = bytes + TILES_SECAO > areas ? bytes + TILES_SECAO : areas;
+  f->smem = bytes > areas ? bytes : areas;
   {  // the coarsest level's matrix after everything else, when the level is small enough
     const size_t nGrosso = (size_t)p->nxL[p->L - 1] * p->nyL[p->L - 1];
     const size_t off = (f->smem + 15) & ~(size_t)15;
