@@ -43,6 +43,13 @@ constexpr int DENSO_MAX = 128;
 constexpr int DENSO_MAPA_MAX = DENSO_MAX * DENSO_MAX;
 constexpr size_t DENSO_BYTES = (size_t)DENSO_MAX * DENSO_MAX * 4 + (size_t)DENSO_MAX * 4 * 6 + 16;
 constexpr size_t SMEM_CTA_MAX = 227 * 1024 - 2048;  // dynamic shared memory cap (static share aside)
+// The whole coarse section (levels Lc..L-1 of the V-cycle, from x = 0) is a linear map of level
+// Lc's right side, fixed during a solve.  For a top section level of at most SECAO_DENSA_MAX
+// cells, a solve that may run at least SECAO_DENSA_MIN_ITERS iterations builds that map once (a
+// column per water cell, every CTA running the section on unit vectors) and applies it as one
+// grid-wide matrix-vector product per V-cycle, instead of CTA 0 running the section alone.
+constexpr int SECAO_DENSA_MAX = 2048;
+constexpr int SECAO_DENSA_MIN_ITERS = 30;
 constexpr int NPARC = 4;                           // partial slots per CTA
 constexpr int PERFIL_MAX = 1 << 16;                // phase-trace capacity
 constexpr int PERFIL_SECAO = 1 << 14;              // coarse-section stamps (after the phase trace)
@@ -73,6 +80,10 @@ struct Fundido {
   float *p2 = nullptr, *z2 = nullptr;
   float *xc = nullptr, *bc = nullptr;
   int offDenso = -1;  // byte offset of the coarsest level's matrix in CTA 0's shared memory
+  bool secaoDensa = false;  // the section's matrix can be built (buffers below allocated)
+  float* mSecao = nullptr;   // nW x nW, row i = water cell i of level Lc
+  int *wSecao = nullptr, *wInv = nullptr, *nW = nullptr;  // water cells of level Lc, cell -> row, count
+  unsigned* densoG = nullptr;  // the coarsest level's matrix block, copied from CTA 0 to every CTA
   uint16_t* op = nullptr;
   void* kern = nullptr;
   unsigned long long* perfil = nullptr;
@@ -97,6 +108,10 @@ struct Args {
   float *p2, *z2;
   float *xc, *bc;
   int offDenso;  // coarsest-level matrix in CTA 0's dynamic shared memory (-1: sweeps)
+  int secaoDensa;  // 1: the section may be replaced by its matrix
+  float* mSecao;
+  int *wSecao, *wInv, *nWp;
+  unsigned* densoG;
   uint16_t* op;  // per-cell operator descriptor of level 0 (OP_*)
   unsigned long long* perfil;  // [0] count, [1..] %globaltimer at each barrier (null: off)
 };
@@ -427,6 +442,22 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   const int ox = bx * 16 - desl, oy = by * 16 - desl;
   const int nx = n.nx, ny = n.ny;
   const T* b = (const T*)n.b;
+  // PROL: the coarse tile (columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11) is loaded first,
+  // so that every load of the block is in flight before any result is used
+  const int cx0 = (ox - 2) >> 1, cy0 = (oy - 2) >> 1;
+  float cv[4];
+  int cz[4];
+  if (PROL) {
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+      const int s = lane + 32 * kk;
+      const int I = cx0 + s % 11, J = cy0 + s / 11;
+      const bool ok = s < CT && I >= 0 && J >= 0 && I < g.nx && J < g.ny;
+      const int C = ok ? I + J * g.nx : 0;
+      cz[kk] = ok ? ldcg8(g.viz + C) : 0;
+      cv[kk] = ok ? (xcSecao ? __ldcg(xcSecao + C) : lerN(g.meia, g.x, C)) : 0.0f;
+    }
+  }
   float x[2][4], bq[2][4];  // [colour][m], see meiaReg
   int v[2][4], cel[2][4];
   int om[2][4];  // M_ESPALHAR: the cells' operator descriptors (bubble air)
@@ -497,18 +528,6 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     // coarse tile: columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11, water x or 0; the
     // snapshot of every fine water cell, frame included, is x + P(x_coarse)
     float* ct = area;
-    const int cx0 = (ox - 2) >> 1, cy0 = (oy - 2) >> 1;
-    float cv[4];
-    int cz[4];
-#pragma unroll
-    for (int kk = 0; kk < 4; kk++) {
-      const int s = lane + 32 * kk;
-      const int I = cx0 + s % 11, J = cy0 + s / 11;
-      const bool ok = s < CT && I >= 0 && J >= 0 && I < g.nx && J < g.ny;
-      const int C = ok ? I + J * g.nx : 0;
-      cz[kk] = ok ? ldcg8(g.viz + C) : 0;
-      cv[kk] = ok ? (xcSecao ? __ldcg(xcSecao + C) : lerN(g.meia, g.x, C)) : 0.0f;
-    }
 #pragma unroll
     for (int kk = 0; kk < 4; kk++) {
       const int s = lane + 32 * kk;
@@ -871,8 +890,8 @@ __device__ void aplicarDenso(const Denso& z, float* F, int xa, int b) {
 }
 
 // Stamp of the coarse-section trace (CTA 0, thread 0, when tracing).
-__device__ __forceinline__ void marcaSecao(const Args& a) {
-  if (a.perfil && threadIdx.x == 0) {
+__device__ __forceinline__ void marcaSecao(const Args& a, bool marcar = true) {
+  if (marcar && a.perfil && threadIdx.x == 0) {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     unsigned long long* base = a.perfil + PERFIL_MAX + 1;
@@ -884,11 +903,12 @@ __device__ __forceinline__ void marcaSecao(const Args& a) {
 // Levels Lc..L-1 of the V-cycle inside CTA 0: loads b of level Lc (a.bc), runs the down
 // passes and restrictions, the coarsest red-black solve (one warp), the prolongations and up
 // passes, and stores x of level Lc (a.xc).
-__device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, NivelS* s, int* tileOff) {
+__device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, NivelS* s, int* tileOff, int coluna) {
+  const bool marcar = coluna < 0 && blockIdx.x == 0;
   float* F = (float*)smem;
   uint8_t* U = smem;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  marcaSecao(a);
+  marcaSecao(a, marcar);
   if (threadIdx.x == 0) {
     int off = 0;  // bytes
     for (int l = a.Lc; l < a.L; l++) {
@@ -909,6 +929,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
     *tileOff = off;
   }
   __syncthreads();
+  const int celJ = coluna >= 0 ? __ldcg(a.wSecao + coluna) : -1;  // column build: b = unit vector
   for (int l = a.Lc; l < a.L; l++) {
     const NivelS t = s[l];
     const uint8_t* viz = s_niv[l].viz;
@@ -920,7 +941,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
       for (int k = 0; k < 4; k++) {
         const int c = c0 + threadIdx.x + k * TF;
         vv[k] = c < N ? ldcg8(viz + c) : 0;
-        bb[k] = (c < N && l == a.Lc) ? __ldcg(a.bc + c) : 0.0f;
+        bb[k] = (c < N && l == a.Lc) ? (coluna < 0 ? __ldcg(a.bc + c) : (c == celJ ? 1.0f : 0.0f)) : 0.0f;
       }
 #pragma unroll
       for (int k = 0; k < 4; k++) {
@@ -934,15 +955,15 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
     }
   }
   __syncthreads();
-  marcaSecao(a);
+  marcaSecao(a, marcar);
   const float pes[4] = {0.25f, 0.75f, 0.75f, 0.25f};
   for (int l = a.Lc; l < a.L - 1; l++) {
     const NivelS f = s[l];
     const NivelS g = s[l + 1];
     passoS(F, U, f, 0, 0, f.xa, f.xb);
-    marcaSecao(a);
+    marcaSecao(a, marcar);
     passoS(F, U, f, 8, 0, f.xb, f.xa);
-    marcaSecao(a);
+    marcaSecao(a, marcar);
     // restringir: residuals of the fine level into its free x buffer, then the 4x4 gathers.
     // Out-of-range and dry neighbours enter with weight or value 0, which adds +0 to a sum.
     {
@@ -987,7 +1008,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
       }
     }
     __syncthreads();
-    marcaSecao(a);
+    marcaSecao(a, marcar);
   }
   const bool comDenso = a.offDenso >= 0 && denso(smem, a.offDenso).cab[0] <= DENSO_MAX;
   if (comDenso) {
@@ -1062,7 +1083,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
       }
   }
   __syncthreads();
-  marcaSecao(a);
+  marcaSecao(a, marcar);
   for (int l = a.L - 2; l >= a.Lc; l--) {
     const NivelS g = s[l + 1];
     const NivelS f = s[l];
@@ -1094,15 +1115,42 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
       if (U[f.v + c] & 16) F[f.xa + c] = xf + e;
     }
     __syncthreads();
-    marcaSecao(a);
+    marcaSecao(a, marcar);
     passoS(F, U, f, 8, 1, f.xa, f.xb);
-    marcaSecao(a);
+    marcaSecao(a, marcar);
     passoS(F, U, f, 0, 1, f.xb, f.xa);
-    marcaSecao(a);
+    marcaSecao(a, marcar);
   }
   const NivelS t = s[a.Lc];
   const int Nc = t.nx * t.ny;
-  for (int c = threadIdx.x; c < Nc; c += TF) a.xc[c] = F[t.xa + c];
+  if (coluna < 0) {
+    for (int c = threadIdx.x; c < Nc; c += TF) a.xc[c] = F[t.xa + c];
+  } else {  // column `coluna` of the section's matrix, rows = water cells of level Lc
+    const int nW = __ldcg(a.nWp);
+    for (int c = threadIdx.x; c < Nc; c += TF) {
+      const int r = __ldcg(a.wInv + c);
+      if (r >= 0) a.mSecao[(size_t)r * nW + coluna] = F[t.xa + c];
+    }
+  }
+}
+
+// x of level Lc = M b over its water cells, every CTA staging b in shared memory and each warp
+// producing rows (lanes over the row, fixed-order warp sum).  Entries off water stay 0.
+__device__ void aplicarSecaoDensa(const Args& a, unsigned char* dyn) {
+  const int nW = __ldcg(a.nWp);
+  float* bs = (float*)dyn;
+  for (int j = threadIdx.x; j < nW; j += TF) bs[j] = __ldcg(a.bc + __ldcg(a.wSecao + j));
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int i = (threadIdx.x >> 5) * gridDim.x + blockIdx.x; i < nW; i += WARPS * gridDim.x) {
+    const float* Mi = a.mSecao + (size_t)i * nW;
+    float sm = 0.0f;
+#pragma unroll 8
+    for (int j = lane; j < nW; j += 32) sm += __ldcg(Mi + j) * bs[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sm += __shfl_xor_sync(0xffffffffu, sm, o);
+    if (lane == 0) a.xc[__ldcg(a.wSecao + i)] = sm;
+  }
 }
 
 // ---------------------------------------------------------------- the V-cycle
@@ -1110,7 +1158,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
 // gather of z (last pass): 5 Lc + 1 phases, each ending at a grid barrier.
 template <class T>
 __device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char* smem, NivelS* tabS, int* tileOff,
-                       const Reuniao& ru, double* sh) {
+                       const Reuniao& ru, double* sh, bool secaoDensa) {
   for (int l = 0; l < a.Lc; l++) {
     const int meia = s_niv[l].meia;
     faseSuavizar<T>(a, l, 0, 0, true, l == 0 ? M_ESPALHAR : M_ZERO, areas, meia, ru, sh);
@@ -1121,7 +1169,8 @@ __device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char*
     else faseRestringir<float>(a, l, areas);
     if (!barreira(a, ep)) return false;
   }
-  if (blockIdx.x == 0) secaoGrossa(a, smem, tabS, tileOff);
+  if (secaoDensa) aplicarSecaoDensa(a, smem);
+  else if (blockIdx.x == 0) secaoGrossa(a, smem, tabS, tileOff, -1);
   if (!barreira(a, ep)) return false;
   for (int l = a.Lc - 1; l >= 0; l--) {
     const int meia = s_niv[l].meia;
@@ -1181,9 +1230,11 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
     float zv[KDA][5], pw[KDA][5];
 #pragma unroll
     for (int k = 0; k < KDA; k++) {
+      // neighbour indices from the grid position alone, so these loads go out with the
+      // descriptors' (the descriptor then picks the water neighbours)
       const int c = c0 + k * GT < N ? c0 + k * GT : 0;
-      const int mk = m[k];
-      const int nb[5] = {c, (mk & 1) ? c - 1 : c, (mk & 2) ? c + 1 : c, (mk & 4) ? c - nx : c, (mk & 8) ? c + nx : c};
+      const int i = c % nx, j = c / nx;
+      const int nb[5] = {c, i > 0 ? c - 1 : c, i < nx - 1 ? c + 1 : c, j > 0 ? c - nx : c, j < ny - 1 ? c + nx : c};
 #pragma unroll
       for (int q = 0; q < 5; q++) {
         zv[k][q] = __ldcg(zc + nb[q]);
@@ -1399,7 +1450,29 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     }
   }
   // the coarsest level's matrix (its neighbour masks are complete since the last barrier)
-  if (blockIdx.x == 0 && a.offDenso >= 0) montarDenso(a, dyn);
+  if (blockIdx.x == 0 && a.offDenso >= 0) {
+    montarDenso(a, dyn);
+    if (a.secaoDensa) {  // every CTA will need it to build the section's columns
+      const unsigned* src = (const unsigned*)(dyn + a.offDenso);
+      for (int k = threadIdx.x; k < (int)(DENSO_BYTES / 4); k += TF) a.densoG[k] = src[k];
+    }
+  }
+  if (a.secaoDensa && blockIdx.x == (gridDim.x > 1 ? 1 : 0) && threadIdx.x < 32) {
+    // the water cells of level Lc, in cell order (one warp, ballot-compacted)
+    const NivelF n = s_niv[a.Lc];
+    const int Nc = n.nx * n.ny;
+    int base = 0;
+    for (int c0 = 0; c0 < Nc; c0 += 32) {
+      const int c = c0 + threadIdx.x;
+      const bool agua = c < Nc && (ldcg8(n.viz + c) & 16);
+      const unsigned m = __ballot_sync(0xffffffffu, agua);
+      const int pos = base + __popc(m & ((1u << threadIdx.x) - 1u));
+      if (c < Nc) a.wInv[c] = agua ? pos : -1;
+      if (agua) a.wSecao[pos] = c;
+      base += __popc(m);
+    }
+    if (threadIdx.x == 0) *a.nWp = base;
+  }
   if (!barreira(a, ep)) return;
   // rb = rhs - (faces*y - sum) (js/pressao-cpu.js:339-341); norm0
   auto rbInicial = [&](int b) {
@@ -1420,13 +1493,26 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     }
   }
   if (!barreira(a, ep)) return;  // rb visible before spreading
+  // ---- the section's matrix: every CTA builds its share of the columns with its own copy of
+  // the coarsest level's matrix
+  const bool secaoDensa = a.secaoDensa && a.iteracoes >= SECAO_DENSA_MIN_ITERS;
+  if (secaoDensa) {
+    unsigned* blocoDenso = (unsigned*)(dyn + a.offDenso);
+    for (int k = threadIdx.x; k < (int)(DENSO_BYTES / 4); k += TF) blocoDenso[k] = __ldcg(a.densoG + k);
+    __syncthreads();
+    const int nW = __ldcg(a.nWp);
+    for (int col = blockIdx.x; col < nW; col += gridDim.x) secaoGrossa(a, dyn, tabS, &tileOff, col);
+    const NivelF nc = s_niv[a.Lc];
+    for (int c = gt0; c < nc.nx * nc.ny; c += GT) a.xc[c] = 0.0f;  // off water, x of level Lc stays 0
+    if (!barreira(a, ep)) return;
+  }
   float escala = (a.escalar && norma0 > 0) ? (float)(1.0 / norma0) : 1.0f;
   if (blockIdx.x == 0)
     for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) {
       a.accZ[b] = 0;
       d.accB[b] = 0;
     }
-  if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, d.z, nullptr}, sh)) return;
+  if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, d.z, nullptr}, sh, secaoDensa)) return;
   int cz = 0, cp = 0;  // which of the two z / p buffers holds the latest values
   auto zbAtual = [&](int b) { return (double)__ldcg(&a.accZ[b]) / ESC; };
   somasGlobais(a, nAt, [&](int b) { return __ldcg(&d.rb[b]) * zbAtual(b); }, [](int) { return 0.0; }, sh, somas);
@@ -1524,7 +1610,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     escala = (a.escalar && norma > 0) ? (float)(1.0 / norma) : 1.0f;
     if (blockIdx.x == 0)
       for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) d.accB[b] = 0;
-    if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, zo, zc}, sh)) return;
+    if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, zo, zc}, sh, secaoDensa)) return;
     cz ^= 1;
     cp ^= 1;
     primeira = false;
@@ -1573,6 +1659,8 @@ Fundido* criarFundido(Pcg* p) {
       f->smem = off + DENSO_BYTES;
     }
   }
+  const size_t nSecao = (size_t)p->nxL[Lc] * p->nyL[Lc];
+  f->secaoDensa = f->offDenso >= 0 && nSecao <= (size_t)SECAO_DENSA_MAX && Lc < p->L - 1;
   f->kern = p->precisao == TQ_PREC_FP16   ? kernelDe<__half>()
             : p->precisao == TQ_PREC_BF16 ? kernelDe<__nv_bfloat16>()
                                           : kernelDe<float>();
@@ -1598,6 +1686,10 @@ Fundido* criarFundido(Pcg* p) {
          cudaMalloc(&f->nAtivos, sizeof(int)) == cudaSuccess && cudaMalloc(&f->p2, N * 4) == cudaSuccess &&
          cudaMalloc(&f->z2, N * 4) == cudaSuccess && cudaMalloc(&f->xc, nLc * 4) == cudaSuccess &&
          cudaMalloc(&f->bc, nLc * 4) == cudaSuccess && cudaMalloc(&f->op, N * sizeof(uint16_t)) == cudaSuccess;
+    if (ok && f->secaoDensa)
+      ok = cudaMalloc(&f->mSecao, nLc * nLc * 4) == cudaSuccess && cudaMalloc(&f->wSecao, nLc * 4) == cudaSuccess &&
+           cudaMalloc(&f->wInv, nLc * 4) == cudaSuccess && cudaMalloc(&f->nW, 4) == cudaSuccess &&
+           cudaMalloc(&f->densoG, DENSO_BYTES) == cudaSuccess;
   }
   if (ok) {
     NivelF tab[MAX_NIVEIS] = {};
@@ -1626,7 +1718,8 @@ Fundido* criarFundido(Pcg* p) {
 void destruirFundido(Fundido* f) {
   if (!f) return;
   void* ps[] = {f->niveis, f->parc, f->bar, f->erro, f->accZ, f->zb2, f->pb2, f->ativos,
-                f->nAtivos, f->p2, f->z2, f->xc, f->bc, f->perfil, f->op};
+                f->nAtivos, f->p2, f->z2, f->xc, f->bc, f->perfil, f->op, f->mSecao, f->wSecao, f->wInv, f->nW,
+                f->densoG};
   for (void* q : ps)
     if (q) cudaFree(q);
   delete f;
@@ -1657,6 +1750,12 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   a.xc = f->xc;
   a.bc = f->bc;
   a.offDenso = f->offDenso;
+  a.secaoDensa = f->secaoDensa ? 1 : 0;
+  a.mSecao = f->mSecao;
+  a.wSecao = f->wSecao;
+  a.wInv = f->wInv;
+  a.nWp = f->nW;
+  a.densoG = f->densoG;
   a.op = f->op;
   a.perfil = f->perfilar ? f->perfil : nullptr;
   if (a.perfil) {
