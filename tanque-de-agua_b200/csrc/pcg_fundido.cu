@@ -85,6 +85,7 @@ struct Fundido {
   int *wSecao = nullptr, *wInv = nullptr, *nW = nullptr;  // water cells of level Lc, cell -> row, count
   unsigned* densoG = nullptr;  // the coarsest level's matrix block, copied from CTA 0 to every CTA
   uint16_t* op = nullptr;
+  unsigned long long* rotB = nullptr;
   void* kern = nullptr;
   unsigned long long* perfil = nullptr;
   bool perfilar = false;
@@ -113,6 +114,9 @@ struct Args {
   int *wSecao, *wInv, *nWp;
   unsigned* densoG;
   uint16_t* op;  // per-cell operator descriptor of level 0 (OP_*)
+  // per-cell bubble labels of level 0, 12 bits each: bits 0-11 the cell's own (air of an active
+  // bubble), 12-23 / 24-35 / 36-47 / 48-59 its left / right / down / up neighbour's (0: none)
+  unsigned long long* rotB;
   unsigned long long* perfil;  // [0] count, [1..] %globaltimer at each barrier (null: off)
 };
 
@@ -460,7 +464,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   }
   float x[2][4], bq[2][4];  // [colour][m], see meiaReg
   int v[2][4], cel[2][4];
-  int om[2][4];  // M_ESPALHAR: the cells' operator descriptors (bubble air)
+  int om[2][4];  // M_ESPALHAR: the cells' own bubble labels (0: not bubble air)
   Moldura f;
   unsigned aguaF = 0;  // PROL: water flags of the frame cells (bits 0-3 left, 4-7 right, 8-9 below, 10-11 above)
 #pragma unroll
@@ -475,7 +479,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
       x[cr][m] = (!ZERO && dentro) ? carregar(ldcg(src + c)) : 0.0f;
       if (MODO == M_ESPALHAR) {
         bq[cr][m] = dentro ? __ldcg(a.d.r + c) : 0.0f;
-        om[cr][m] = (a.bolhas && dentro) ? __ldcg(a.op + c) : 0;
+        om[cr][m] = (a.bolhas && dentro) ? (int)(__ldcg(a.rotB + c) & 0xfff) : 0;  // own bubble label
       } else {
         bq[cr][m] = dentro ? carregar(ldcg(b + c)) : 0.0f;
       }
@@ -515,10 +519,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
       for (int m = 0; m < 4; m++) {
         if (cel[cr][m] < 0) continue;
         float val = bq[cr][m];
-        if (om[cr][m] & OP_BOLHA) {
-          const uint32_t rb = __ldcg(a.d.rotulo + cel[cr][m]);
-          val = (float)(__ldcg(a.d.rb + rb) / __ldcg(a.d.celsB + rb));
-        }
+        if (om[cr][m]) val = (float)(__ldcg(a.d.rb + om[cr][m]) / __ldcg(a.d.celsB + om[cr][m]));
         const T bt = guardar<T>(val * ru.escala);
         ((T*)n.b)[cel[cr][m]] = bt;
         bq[cr][m] = carregar(bt);
@@ -557,15 +558,26 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   if (MODO == M_JUNTAR) {
     const float inv = 1.0f / ru.escala;
     float rv[2][4], zv[2][4];
+    int lb[2][4];
 #pragma unroll
     for (int cr = 0; cr < 2; cr++)
 #pragma unroll
       for (int m = 0; m < 4; m++) {
         const int c = cel[cr][m] < 0 ? 0 : cel[cr][m];
         om[cr][m] = cel[cr][m] < 0 ? 0 : __ldcg(a.op + c);
+        lb[cr][m] = (a.bolhas && cel[cr][m] >= 0) ? (int)(__ldcg(a.rotB + c) & 0xfff) : 0;
         rv[cr][m] = __ldcg(a.d.r + c);
         zv[cr][m] = ru.zVelho ? __ldcg(ru.zVelho + c) : 0.0f;
       }
+    unsigned cels[2][4];
+#pragma unroll
+    for (int cr = 0; cr < 2; cr++)
+#pragma unroll
+      for (int m = 0; m < 4; m++) cels[cr][m] = lb[cr][m] ? __ldcg(a.d.celsB + lb[cr][m]) : 1u;
+    // a bubble cell's share of z goes to its bubble's fixed-point sum; the lane adds its
+    // consecutive cells of one bubble before the atomic (integer sums: same result)
+    int labA = 0;
+    long long acc = 0;
 #pragma unroll
     for (int cr = 0; cr < 2; cr++)
 #pragma unroll
@@ -573,9 +585,14 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
         const int c = cel[cr][m];
         if (c < 0) continue;
         const float xz = carregar(guardar<T>((v[cr][m] & 16) ? x[cr][m] : 0.0f)) * inv;
-        if (om[cr][m] & OP_BOLHA) {
-          const uint32_t rb = __ldcg(a.d.rotulo + c);
-          somaFixa(&a.accZ[rb], (double)xz / __ldcg(a.d.celsB + rb), ESC);
+        if (lb[cr][m]) {
+          const long long q = __double2ll_rn((double)xz / cels[cr][m] * ESC);
+          if (lb[cr][m] != labA) {
+            if (labA && acc) atomicAdd((unsigned long long*)&a.accZ[labA], (unsigned long long)acc);
+            labA = lb[cr][m];
+            acc = 0;
+          }
+          acc += q;
           ru.zNovo[c] = 0.0f;
           continue;
         }
@@ -585,6 +602,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
           if (ru.zVelho) s1 += (double)rv[cr][m] * (double)zv[cr][m];
         }
       }
+    if (labA && acc) atomicAdd((unsigned long long*)&a.accZ[labA], (unsigned long long)acc);
   } else {
 #pragma unroll
     for (int cr = 0; cr < 2; cr++)
@@ -1228,6 +1246,7 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
       m[k] = c < N ? __ldcg(a.op + c) : 0;
     }
     float zv[KDA][5], pw[KDA][5];
+    unsigned long long rl[KDA];
 #pragma unroll
     for (int k = 0; k < KDA; k++) {
       // neighbour indices from the grid position alone, so these loads go out with the
@@ -1240,6 +1259,7 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
         zv[k][q] = __ldcg(zc + nb[q]);
         pw[k][q] = prim ? 0.0f : __ldcg(pv + nb[q]);
       }
+      rl[k] = a.bolhas ? __ldcg(a.rotB + c) : 0ull;
     }
 #pragma unroll
     for (int k = 0; k < KDA; k++) {
@@ -1256,14 +1276,9 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
 #pragma unroll
         for (int q = 0; q < 4; q++) {
           if (mk & (1 << q)) sv += pq[q + 1];
-          else if (mk & OP_VIZ_BOLHA) {
-            const int i = c % nx, j = c / nx;
-            const bool existe = q == 0 ? i > 0 : q == 1 ? i < nx - 1 : q == 2 ? j > 0 : j < ny - 1;
-            if (!existe) continue;
-            const int n = q == 0 ? c - 1 : q == 1 ? c + 1 : q == 2 ? c - nx : c + nx;
-            if (ldcg8(d.tipo + n) != AR) continue;
-            const uint32_t r = __ldcg(d.rotulo + n);
-            if (bolhaAtiva(a, r)) sv += (float)pbNovoV((int)r);
+          else if (mk & OP_VIZ_BOLHA) {  // neighbour q is air of an active bubble: that bubble's p
+            const int r = (int)(rl[k] >> (12 + 12 * q)) & 0xfff;
+            if (r) sv += (float)pbNovoV(r);
           }
         }
         const float apc = (float)(mk >> 8) * pq[0] - sv;
@@ -1278,7 +1293,7 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
 #pragma unroll
           for (int q = 0; q < 4; q++)
             if (mk & (1 << q)) t += (double)pq[q + 1];
-          if (t != 0) somaFixa(&d.accB[__ldcg(d.rotulo + c)], t, ESC);
+          if (t != 0) somaFixa(&d.accB[(int)(rl[k] & 0xfff)], t, ESC);
         }
       }
     }
@@ -1382,6 +1397,19 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       if (i >= 1 && j >= 1 && i < nx - 1 && j < ny - 1) m |= OP_FACE;
     }
     a.op[c] = (uint16_t)(m | (livres << 8));
+    unsigned long long rl = 0;
+    if (a.bolhas && (m & (OP_BOLHA | OP_VIZ_BOLHA))) {
+      if (m & OP_BOLHA) rl = d.rotulo[c] & 0xfffu;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const bool existe = k == 0 ? i > 0 : k == 1 ? i < nx - 1 : k == 2 ? j > 0 : j < ny - 1;
+        if (!existe) continue;
+        const int nb = k == 0 ? c - 1 : k == 1 ? c + 1 : k == 2 ? c - nx : c + nx;
+        if (d.tipo[nb] == AR && bolhaAtiva(a, d.rotulo[nb]))
+          rl |= (unsigned long long)(d.rotulo[nb] & 0xfffu) << (12 + 12 * k);
+      }
+    }
+    a.rotB[c] = rl;
   }
   if (a.bolhas) {
     for (int c = gt0; c < N; c += GT) {
@@ -1685,7 +1713,8 @@ Fundido* criarFundido(Pcg* p) {
          cudaMalloc(&f->ativos, MAX_BOLHAS * sizeof(int)) == cudaSuccess &&
          cudaMalloc(&f->nAtivos, sizeof(int)) == cudaSuccess && cudaMalloc(&f->p2, N * 4) == cudaSuccess &&
          cudaMalloc(&f->z2, N * 4) == cudaSuccess && cudaMalloc(&f->xc, nLc * 4) == cudaSuccess &&
-         cudaMalloc(&f->bc, nLc * 4) == cudaSuccess && cudaMalloc(&f->op, N * sizeof(uint16_t)) == cudaSuccess;
+         cudaMalloc(&f->bc, nLc * 4) == cudaSuccess && cudaMalloc(&f->op, N * sizeof(uint16_t)) == cudaSuccess &&
+         cudaMalloc(&f->rotB, N * sizeof(unsigned long long)) == cudaSuccess;
     if (ok && f->secaoDensa)
       ok = cudaMalloc(&f->mSecao, nLc * nLc * 4) == cudaSuccess && cudaMalloc(&f->wSecao, nLc * 4) == cudaSuccess &&
            cudaMalloc(&f->wInv, nLc * 4) == cudaSuccess && cudaMalloc(&f->nW, 4) == cudaSuccess &&
@@ -1718,7 +1747,7 @@ Fundido* criarFundido(Pcg* p) {
 void destruirFundido(Fundido* f) {
   if (!f) return;
   void* ps[] = {f->niveis, f->parc, f->bar, f->erro, f->accZ, f->zb2, f->pb2, f->ativos,
-                f->nAtivos, f->p2, f->z2, f->xc, f->bc, f->perfil, f->op, f->mSecao, f->wSecao, f->wInv, f->nW,
+                f->nAtivos, f->p2, f->z2, f->xc, f->bc, f->perfil, f->op, f->rotB, f->mSecao, f->wSecao, f->wInv, f->nW,
                 f->densoG};
   for (void* q : ps)
     if (q) cudaFree(q);
@@ -1757,6 +1786,7 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   a.nWp = f->nW;
   a.densoG = f->densoG;
   a.op = f->op;
+  a.rotB = f->rotB;
   a.perfil = f->perfilar ? f->perfil : nullptr;
   if (a.perfil) {
     cudaMemsetAsync(f->perfil, 0, sizeof(unsigned long long), s);
