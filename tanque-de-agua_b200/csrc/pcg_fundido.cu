@@ -717,20 +717,22 @@ __device__ void faseRestringir(const Args& a, int l, float* areas) {
       }
     }
     __syncwarp();
-    for (int s = lane; s < RB; s += 32) {
-      int rr = s / 66, cc = s % 66;
-      int vz = vs[s];
-      float r = 0.0f;
-      if (vz & 16) {
-        const float* xc = xs + (rr + 1) * 68 + cc + 1;
-        float t = 0.0f;
-        if (vz & 1) t += xc[-1];
-        if (vz & 2) t += xc[1];
-        if (vz & 4) t += xc[-68];
-        if (vz & 8) t += xc[68];
-        r = bs[s] - ((float)__popc(vz & 15) * xc[0] - t);
+    {
+      // residuals of the 4 x 66 fine cells: every shared load of the lane's nine cells goes out
+      // before the first store.  x is 0 off water and outside the grid, so the neighbour sum
+      // needs no mask; the residual is 0 off water.
+      float rv[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        const int s = lane + 32 * k < RB ? lane + 32 * k : 0;
+        const float* xc = xs + (s / 66 + 1) * 68 + s % 66 + 1;
+        const int vz = vs[s];
+        const float t = ((xc[-1] + xc[1]) + xc[-68]) + xc[68];
+        rv[k] = (vz & 16) ? bs[s] - ((float)__popc(vz & 15) * xc[0] - t) : 0.0f;
       }
-      rs[s] = r;
+#pragma unroll
+      for (int k = 0; k < 9; k++)
+        if (lane + 32 * k < RB) rs[lane + 32 * k] = rv[k];
     }
     __syncwarp();
     if (I < g.nx) {
