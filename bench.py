@@ -155,6 +155,25 @@ def medir_oraculo(passos, aquecimento, orcamento_s=None):
     return feitos / t, feitos, n_part
 
 
+# ------------------------------------------------------------------ replicas
+def tempos_max_ranks(tempos, dist, dispositivo):
+    """This rank's device times (ms) -> their maximum over the ranks, on every rank: the job's time
+    is its slowest replica's."""
+    t = np.asarray(tempos, dtype=np.float64)
+    if dist is None:
+        return t
+    import torch
+    tt = torch.tensor(t, device=dispositivo)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return tt.cpu().numpy()
+
+
+def vazao_replicas(mundo, passos, subpassos, ms):
+    """Whole-job substeps per second: each of the `mundo` ranks advanced its own tank (a replica;
+    a tank does not shard) through `passos` frames of `subpassos` substeps in `ms`."""
+    return mundo * passos * subpassos / (ms / 1000.0)
+
+
 # ------------------------------------------------------------------ GPU arm
 def executar_gpu(args, rank, mundo, dist):
     import torch
@@ -264,16 +283,8 @@ def executar_gpu(args, rank, mundo, dist):
     plano = medir(_abi.TQ_PREC_FP32, _abi.TQ_ENGINE_PLAIN)
     e2e = medir_e2e(precisao_mista, motor_misto)
 
-    # max over ranks
-    tempos = np.array([misto["ms"], plano["ms"], e2e["ms"]], dtype=np.float64)
-    if dist is not None:
-        t = torch.tensor(tempos, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tempos = t.cpu().numpy()
-    subpassos_total = mundo * args.steps * SUB
-    valor = subpassos_total / (tempos[0] / 1000)
-    valor_plano = subpassos_total / (tempos[1] / 1000)
-    valor_e2e = subpassos_total / (tempos[2] / 1000)
+    tempos = tempos_max_ranks([misto["ms"], plano["ms"], e2e["ms"]], dist, "cuda")
+    valor, valor_plano, valor_e2e = (vazao_replicas(mundo, args.steps, SUB, t) for t in tempos)
 
     def roofline(res, rotulo):
         et = res["etapas"]

@@ -298,3 +298,39 @@ def jato_torneira(torneira: dict, quadro: int, dt: float) -> np.ndarray:
         lista[k, 2] = vx
         lista[k, 3] = vy
     return lista.ravel()
+
+
+# ------------------------------------------------------------------ benchmark configurations
+def cena_barragem_160(Cena):
+    """Dam break of the benchmark set: 160 x 100 cells, h = 6.25 mm (1.0 x 0.625 m), the tank's
+    wall frame, a water block x in [0, 0.4 m], y in [0, 0.375 m] seeded 2 x 2 per cell with the
+    LCG of semente(1), at rest.  Returns (cena, particles)."""
+    h = 0.00625
+    cena = Cena(160, 100, h)
+    m = MOLDURA * h
+    return cena, semear_retangulo_rapido(m, m, 0.4, 0.375, h, s=1)
+
+
+def cena_ar_preso(Cena, nx: int = 480, ny: int = 270, h: float = 0.0022):
+    """Trapped air of the benchmark set: a tank 60 % full with an inverted cup of 4-cell walls
+    half submerged (an air pocket under its top, the water inside lower than outside) and 8
+    circular air voids of radius 6-15 cells near the bottom (positions and radii from the LCG
+    of semente(2)); 2 x 2 particles per cell.  Returns (cena, particles)."""
+    cena = Cena(nx, ny, h)
+    W, H = cena.largura, cena.altura
+    raio = 2 * h
+    cx0, cx1, cy0, cy1 = 0.35 * W, 0.65 * W, 0.35 * H, 0.75 * H
+    cena.tracar(cx0, cy0, cx0, cy1, raio)
+    cena.tracar(cx1, cy0, cx1, cy1, raio)
+    cena.tracar(cx0, cy1, cx1, cy1, raio)
+    m = MOLDURA * h
+    agua = semear_retangulo_rapido(m, m, W - m, 0.6 * H, h, s=2).reshape(-1, CAMPOS)
+    x, y = agua[:, 0].astype(np.float64), agua[:, 1].astype(np.float64)
+    fora = ~((x > cx0) & (x < cx1) & (y > 0.45 * H))  # the pocket under the cup
+    al = semente(2)
+    for _ in range(8):
+        r = (6 + 9 * al()) * h
+        bx = m + r + al() * (W - 2 * (m + r))
+        by = m + r + al() * (0.25 * H - r)
+        fora &= (x - bx) ** 2 + (y - by) ** 2 >= r * r
+    return cena, agua[fora].ravel()

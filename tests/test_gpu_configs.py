@@ -1,0 +1,117 @@
+"""Parity on the benchmark set's own scenes, at their full sizes, and the volume bound.
+
+- Dam break, 160 x 100 (h = 6.25 mm) and trapped air, 480 x 270 (h = 2.2 mm, an inverted cup
+  and 8 voids): from the same state, one substep on the GPU and in the oracle, every pressure
+  solve run to ||r|| <= 1e-6 ||r0|| (the benchmark's stopping rule), for the FP32 plain engine
+  and the FP16 fused one.  Integer work is compared bit for bit (particle-to-grid sums, flags,
+  counts, air labels, bubble ids and volumes).  Pressure and velocities: both solves stop at the
+  same relative residual from the same warm start, so q agrees to the solve's own accuracy,
+  1e-3 relative (L-infinity); positions to 1e-5 m.
+- Volume: 1000 substeps of the dam break on the GPU keep the particle count (the water volume
+  the particles carry) within 0.1 % (north_star's bound).
+"""
+import numpy as np
+import pytest
+
+from estado import copiar_estado, erro_relativo
+from oraculo import CenaOraculo, SimulacaoOraculo
+from tanque import Cena, SimulacaoGPU, _abi
+from tanque.cenarios import cena_ar_preso, cena_barragem_160
+from tanque.constantes import CAMPOS
+
+pytestmark = pytest.mark.gpu
+
+SOLVE = {"tolerance": 1e-6, "iterations": 200}
+MOTORES = [pytest.param({"precision": _abi.TQ_PREC_FP32, "engine": _abi.TQ_ENGINE_PLAIN}, id="fp32-plain"),
+           pytest.param({"precision": _abi.TQ_PREC_FP16, "engine": _abi.TQ_ENGINE_FUSED}, id="fp16-fused")]
+INTEIROS = ["accU", "accV", "accCel", "accCor", "tipo", "contagemCelula", "rotulo", "vivo", "volumeBolha"]
+
+
+def _par(cena_fn, opcoes):
+    cena_o, agua = cena_fn(CenaOraculo)
+    cena_g = Cena(cena_o.nx, cena_o.ny, cena_o.h)
+    cena_g.sdf[:] = cena_o.sdf
+    o = SimulacaoOraculo(cena_o, dict(SOLVE, p2g_mode=_abi.TQ_P2G_FIXED))
+    g = SimulacaoGPU(cena_g, dict(SOLVE, **opcoes))
+    o.adicionar(agua, False)
+    g.adicionar(agua, False)
+    return o, g
+
+
+def _comparar(o, g, quadro):
+    for campo in INTEIROS:
+        a, b = g.campo(campo), o.campo(campo)
+        assert np.array_equal(a, b), f"{quadro}: {campo} differs in {np.count_nonzero(a != b)} entries"
+    for campo in ["q", "u", "v"]:
+        e = erro_relativo(g.campo(campo), o.campo(campo))
+        assert e <= 1e-3, f"{quadro}: {campo} relative error {e:.3g}"
+    pg, po = g.p.reshape(-1, CAMPOS), o.p.reshape(-1, CAMPOS)
+    assert pg.shape == po.shape, quadro
+    assert float(np.max(np.abs(pg[:, :2].astype(np.float64) - po[:, :2]))) < 1e-5, quadro
+
+
+@pytest.mark.parametrize("opcoes", MOTORES)
+def test_barragem_160x100(lib_gpu, opcoes):
+    o, g = _par(cena_barragem_160, opcoes)
+    for s in (o, g):  # the water is moving before the compared substeps
+        s.avancar(1 / 240, 1)
+    for quadro in range(3):
+        copiar_estado(o, g)
+        o.avancar(1 / 240, 1)
+        g.avancar(1 / 240, 1)
+        _comparar(o, g, f"substep {quadro}")
+
+
+@pytest.mark.parametrize("opcoes", MOTORES)
+def test_ar_preso_480x270(lib_gpu, opcoes):
+    o, g = _par(cena_ar_preso, opcoes)
+    dt = 1 / 840
+    for s in (o, g):
+        s.atualizarAr()
+    for campo in ["rotulo", "vivo"]:
+        assert np.array_equal(g.campo(campo), o.campo(campo)), campo
+    assert np.array_equal(g.campo("volumeAlvo").view(np.uint32), o.campo("volumeAlvo").view(np.uint32))
+    assert int(np.count_nonzero(g.campo("vivo"))) >= 5  # the cup's pocket and the voids are bubbles
+    for quadro in range(2):
+        copiar_estado(o, g)
+        o.avancar(dt, 1)
+        g.avancar(dt, 1)
+        _comparar(o, g, f"substep {quadro}")
+
+
+def test_volume_barragem_1000_subpassos(lib_gpu):
+    cena, agua = cena_barragem_160(Cena)
+    g = SimulacaoGPU(cena, dict(SOLVE, precision=_abi.TQ_PREC_FP16, engine=_abi.TQ_ENGINE_FUSED))
+    g.adicionar(agua, False)
+    n0 = g.n
+    for _ in range(250):
+        g.avancar(1 / 60, 4)  # 1000 substeps of 1/240 s
+    p = g.p.reshape(-1, CAMPOS)
+    assert abs(g.n - n0) <= 1e-3 * n0, (n0, g.n)
+    assert np.all(np.isfinite(p[:, :4]))
+    # settled: the water surface is below its initial height and the particles are at rest-ish
+    assert float(np.max(p[:, 1])) < 0.375 and float(np.mean(np.abs(p[:, 3]))) < 0.2
+
+
+@pytest.mark.parametrize("opcoes", MOTORES)
+def test_erro_contra_fp64(lib_gpu, opcoes, capsys):
+    """Error of one substep against the FP64 build of the oracle (double storage everywhere),
+    from the same state, on the trapped-air scene: the price of FP32 arithmetic and of FP16
+    V-cycle storage once the solve has converged to 1e-6.  Bound: 1e-4 relative on q, u, v
+    (measured on a B200: 9e-6 FP32 plain, 1.5e-5 FP16 fused)."""
+    cena_o, agua = cena_ar_preso(CenaOraculo)
+    cena_g = Cena(cena_o.nx, cena_o.ny, cena_o.h)
+    cena_g.sdf[:] = cena_o.sdf
+    o = SimulacaoOraculo(cena_o, dict(SOLVE, p2g_mode=_abi.TQ_P2G_FIXED), fp64=True)
+    g = SimulacaoGPU(cena_g, dict(SOLVE, **opcoes))
+    o.adicionar(agua, False)
+    g.adicionar(agua, False)
+    for s in (o, g):
+        s.atualizarAr()
+    copiar_estado(o, g)
+    o.avancar(1 / 840, 1)
+    g.avancar(1 / 840, 1)
+    erros = {c: erro_relativo(g.campo(c), o.campo(c)) for c in ["q", "u", "v"]}
+    with capsys.disabled():
+        print(f"\nerror vs FP64 oracle ({opcoes}): " + ", ".join(f"{k} {v:.2e}" for k, v in erros.items()))
+    assert max(erros.values()) <= 1e-4, erros
