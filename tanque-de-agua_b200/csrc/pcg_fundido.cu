@@ -554,7 +554,14 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     }
     __syncwarp();
   }
-  varrerReg(x, v, bq, f, ordem);
+  // a block with no cell to update (air, solid, walled-in water) keeps its values: the warp skips
+  // the sweeps (fmaf(0, d, q) = q for every cell of the block)
+  bool mexe = false;
+#pragma unroll
+  for (int cr = 0; cr < 2; cr++)
+#pragma unroll
+    for (int m = 0; m < 4; m++) mexe |= (v[cr][m] & 16) && (v[cr][m] & 15);
+  if (__any_sync(0xffffffffu, mexe)) varrerReg(x, v, bq, f, ordem);
   if (MODO == M_JUNTAR) {
     const float inv = 1.0f / ru.escala;
     float rv[2][4], zv[2][4];
@@ -626,8 +633,14 @@ __device__ __noinline__ void faseSuavizarT(const Args& a, int l, int desl, int o
   if (MODO == M_PROL) g = s_niv[l + 1];
   const float* xcSecao = (MODO == M_PROL && l + 1 == a.Lc) ? a.xc : nullptr;
   double s0 = 0.0, s1 = 0.0;
-  for (int blk = w * gridDim.x + blockIdx.x; blk < nb; blk += WARPS * gridDim.x)
+  // with more blocks than warps (exc > 0), the warps that take two blocks take the last 2 exc
+  // blocks of the row-major order, the top rows: air above the water in a tank, whose blocks
+  // skip their sweeps, so the pass lasts about one water block
+  const int tot = WARPS * gridDim.x, exc = nb - tot;
+  for (int t = w * gridDim.x + blockIdx.x; t < nb; t += tot) {
+    const int blk = exc > 0 ? nb - 1 - (t + exc) % nb : t;
     suavizarBloco<T, MODO>(a, n, blk, nbx, desl, ordem, src, dst, area, g, xcSecao, ru, s0, s1);
+  }
   if (MODO == M_JUNTAR) {
     const double t0 = somaBloco(s0, sh);
     const double t1 = somaBloco(s1, sh);
