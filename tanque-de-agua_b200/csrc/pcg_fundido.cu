@@ -50,6 +50,8 @@ constexpr size_t SMEM_CTA_MAX = 227 * 1024 - 2048;  // dynamic shared memory cap
 // grid-wide matrix-vector product per V-cycle, instead of CTA 0 running the section alone.
 constexpr int SECAO_DENSA_MAX = 2048;
 constexpr int SECAO_DENSA_MIN_ITERS = 30;
+// The coarsest level's sweeps run on one warp up to this many cells, on every warp of CTA 0 above.
+constexpr int GROSSO_UM_WARP = 1024;
 constexpr int NPARC = 4;                           // partial slots per CTA
 constexpr int PERFIL_MAX = 1 << 16;                // phase-trace capacity
 constexpr int PERFIL_SECAO = 1 << 14;              // coarse-section stamps (after the phase trace)
@@ -1047,45 +1049,74 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
   if (comDenso) {
     const NivelS n = s[a.L - 1];
     aplicarDenso(denso(smem, a.offDenso), F, n.xa, n.b);
-  } else if (w == 0) {  // resolverGrosso (js/pressao-cpu.js:217-238), one warp
+  } else if (s[a.L - 1].nx * s[a.L - 1].ny > GROSSO_UM_WARP || w == 0) {
+    // resolverGrosso (js/pressao-cpu.js:217-238): one warp on a small level, every warp of the
+    // CTA on a large one (a wide, flat coarsest level of a tank atlas)
+    const bool todos = s[a.L - 1].nx * s[a.L - 1].ny > GROSSO_UM_WARP;
+    const int P = todos ? WARPS : 1;
+    auto sincronizar = [&]() {
+      if (todos) __syncthreads();
+      else __syncwarp();
+    };
     const NivelS n = s[a.L - 1];
     const int nx = n.nx, N = n.nx * n.ny;
     float* x = F + n.xa;
     // The cells that change (water with a free neighbour), listed per colour in the free x
-    // buffer as cell | mask << 24, colour 0 first.
+    // buffer as cell | mask << 24, colour 0 first, in cell order: each warp lists a slice of
+    // the cells (a multiple of 32) at the offset of the slices before it.
     int* lista = (int*)(F + n.xb);
-    int cont[2];
+    __shared__ int contW[2][WARPS];
+    const int fatia = ((N + P * 32 - 1) / (P * 32)) * 32;
+    const int lo = min(w * fatia, N), hi = min(lo + fatia, N);
+    auto muda = [&](int c, int cor) {
+      const int vz = c < hi ? U[n.v + c] : 0;
+      const bool ok = c < hi && (vz & 16) && (vz & 15) && ((((c % nx) + (c / nx) + 1) & 1) == cor);
+      return ok ? (c | ((vz & 15) << 24)) : -1;
+    };
 #pragma unroll
     for (int cor = 0; cor < 2; cor++) {
-      int base = cor ? cont[0] : 0;
-      for (int c0 = 0; c0 < N; c0 += 32) {
-        const int c = c0 + lane;
-        const int vz = c < N ? U[n.v + c] : 0;
-        const bool ok = c < N && (vz & 16) && (vz & 15) && ((((c % nx) + (c / nx) + 1) & 1) == cor);
-        const unsigned m = __ballot_sync(0xffffffffu, ok);
-        if (ok) lista[base + __popc(m & ((1u << lane) - 1u))] = c | ((vz & 15) << 24);
-        base += __popc(m);
-      }
-      cont[cor] = base - (cor ? cont[0] : 0);
+      int k = 0;
+      for (int c0 = lo; c0 < hi; c0 += 32) k += __popc(__ballot_sync(0xffffffffu, muda(c0 + lane, cor) >= 0));
+      if (lane == 0) contW[cor][w] = k;
     }
-    __syncwarp();
+    sincronizar();
+    int cont[2] = {0, 0}, base[2] = {0, 0};
+    for (int q = 0; q < P; q++)
+#pragma unroll
+      for (int cor = 0; cor < 2; cor++) {
+        if (q == w) base[cor] = cont[cor];
+        cont[cor] += contW[cor][q];
+      }
+    base[1] += cont[0];
+#pragma unroll
+    for (int cor = 0; cor < 2; cor++) {
+      int b = base[cor];
+      for (int c0 = lo; c0 < hi; c0 += 32) {
+        const int e = muda(c0 + lane, cor);
+        const unsigned m = __ballot_sync(0xffffffffu, e >= 0);
+        if (e >= 0) lista[b + __popc(m & ((1u << lane) - 1u))] = e;
+        b += __popc(m);
+      }
+    }
+    sincronizar();
+    const int t0 = todos ? threadIdx.x : lane, nt = P * 32;
     for (int k = 0; k < VARREDURAS_GROSSO; k++)
       for (int o = 0; o < 2; o++) {
         const int cor = (k & 1) ? 1 - o : o;
-        const int ini = cor ? cont[0] : 0, n_ = cor ? cont[1] : cont[0];
-        for (int e0 = 0; e0 < n_; e0 += 64) {
-          const int eA = e0 + lane, eB = e0 + 32 + lane;
-          const int EA = eA < n_ ? lista[ini + eA] : -1, EB = eB < n_ ? lista[ini + eB] : -1;
+        const int ini = cor ? cont[0] : 0, n_ = cont[cor];
+        for (int e0 = t0; e0 < n_; e0 += 2 * nt) {
+          const int eA = e0, eB = e0 + nt;
+          const int EA = lista[ini + eA], EB = eB < n_ ? lista[ini + eB] : -1;
           float va[5], vb[5];
-          {  // an idle lane (entry -1) reads cell 0
-            const int c = EA < 0 ? 0 : EA & 0xffffff, mk = EA < 0 ? 0 : EA >> 24;
+          {
+            const int c = EA & 0xffffff, mk = EA >> 24;
             va[0] = x[(mk & 1) ? c - 1 : c];
             va[1] = x[(mk & 2) ? c + 1 : c];
             va[2] = x[(mk & 4) ? c - nx : c];
             va[3] = x[(mk & 8) ? c + nx : c];
             va[4] = F[n.b + c];
           }
-          {
+          {  // an idle entry (-1) reads cell 0
             const int c = EB < 0 ? 0 : EB & 0xffffff, mk = EB < 0 ? 0 : EB >> 24;
             vb[0] = x[(mk & 1) ? c - 1 : c];
             vb[1] = x[(mk & 2) ? c + 1 : c];
@@ -1093,7 +1124,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
             vb[3] = x[(mk & 8) ? c + nx : c];
             vb[4] = F[n.b + c];
           }
-          if (EA >= 0) {
+          {
             const int mk = EA >> 24;
             float t = 0.0f;
             t += (mk & 1) ? va[0] : 0.0f;
@@ -1112,7 +1143,7 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
             x[EB & 0xffffff] = (t + vb[4]) * inversoVizinhos(__popc(mk));
           }
         }
-        __syncwarp();
+        sincronizar();
       }
   }
   __syncthreads();

@@ -60,3 +60,22 @@ def erro_relativo(a, b) -> float:
     b = np.asarray(b, dtype=np.float64)
     escala = max(float(np.max(np.abs(b))) if b.size else 0.0, 1e-30)
     return float(np.max(np.abs(a - b))) / escala if a.size else 0.0
+
+
+# Fields compared bit for bit after a substep from the same state: particle-to-grid sums, flags,
+# counts, air labels, bubble liveness and volumes.
+INTEIROS = ["accU", "accV", "accCel", "accCor", "tipo", "contagemCelula", "rotulo", "vivo", "volumeBolha"]
+
+
+def comparar_passo(o, g, quadro, tol_campos=1e-3, tol_pos=1e-5):
+    """GPU `g` against the oracle `o` after the same substep: integers bit for bit; pressure
+    and velocities to the solve's accuracy (relative L-infinity); positions in metres."""
+    for campo in INTEIROS:
+        a, b = g.campo(campo), o.campo(campo)
+        assert np.array_equal(a, b), f"{quadro}: {campo} differs in {np.count_nonzero(a != b)} entries"
+    for campo in ["q", "u", "v"]:
+        e = erro_relativo(g.campo(campo), o.campo(campo))
+        assert e <= tol_campos, f"{quadro}: {campo} relative error {e:.3g}"
+    pg, po = g.p.reshape(-1, CAMPOS), o.p.reshape(-1, CAMPOS)
+    assert pg.shape == po.shape, quadro
+    assert float(np.max(np.abs(pg[:, :2].astype(np.float64) - po[:, :2]))) < tol_pos, quadro

@@ -13,6 +13,7 @@
 import numpy as np
 import pytest
 
+from estado import comparar_passo as _comparar
 from estado import copiar_estado, erro_relativo
 from oraculo import CenaOraculo, SimulacaoOraculo
 from tanque import Cena, SimulacaoGPU, _abi
@@ -24,7 +25,6 @@ pytestmark = pytest.mark.gpu
 SOLVE = {"tolerance": 1e-6, "iterations": 200}
 MOTORES = [pytest.param({"precision": _abi.TQ_PREC_FP32, "engine": _abi.TQ_ENGINE_PLAIN}, id="fp32-plain"),
            pytest.param({"precision": _abi.TQ_PREC_FP16, "engine": _abi.TQ_ENGINE_FUSED}, id="fp16-fused")]
-INTEIROS = ["accU", "accV", "accCel", "accCor", "tipo", "contagemCelula", "rotulo", "vivo", "volumeBolha"]
 
 
 def _par(cena_fn, opcoes):
@@ -36,18 +36,6 @@ def _par(cena_fn, opcoes):
     o.adicionar(agua, False)
     g.adicionar(agua, False)
     return o, g
-
-
-def _comparar(o, g, quadro):
-    for campo in INTEIROS:
-        a, b = g.campo(campo), o.campo(campo)
-        assert np.array_equal(a, b), f"{quadro}: {campo} differs in {np.count_nonzero(a != b)} entries"
-    for campo in ["q", "u", "v"]:
-        e = erro_relativo(g.campo(campo), o.campo(campo))
-        assert e <= 1e-3, f"{quadro}: {campo} relative error {e:.3g}"
-    pg, po = g.p.reshape(-1, CAMPOS), o.p.reshape(-1, CAMPOS)
-    assert pg.shape == po.shape, quadro
-    assert float(np.max(np.abs(pg[:, :2].astype(np.float64) - po[:, :2]))) < 1e-5, quadro
 
 
 @pytest.mark.parametrize("opcoes", MOTORES)

@@ -1,0 +1,72 @@
+"""Batched tanks on the GPU: atlases (tanque.lote) against the oracle on the same atlas, for the
+FP32 plain engine and the FP16 fused one: 8 tanks, and 12 wide flat ones whose coarsest
+multigrid level is large enough for the coarsest sweeps to run on a whole CTA.
+
+From the same state, one air relabel and two substeps, every pressure solve to
+||r|| <= 1e-6 ||r0||: integers bit for bit (particle-to-grid sums, flags, counts, air labels,
+bubble ids and volumes), q, u, v to 1e-3 relative, positions to 1e-5 m.  Then the whole batch
+helper advances two atlases of the same tanks on the GPU and keeps every particle in its tank.
+"""
+import numpy as np
+import pytest
+
+from estado import comparar_passo, copiar_estado
+from oraculo import SimulacaoOraculo
+from tanque import Cena, SimulacaoGPU, _abi
+from tanque.lote import Lote, gerar_tanques, montar_atlas
+
+pytestmark = pytest.mark.gpu
+
+H = 1 / 128
+SOLVE = {"tolerance": 1e-6, "iterations": 200}
+MOTORES = [pytest.param({"precision": _abi.TQ_PREC_FP32, "engine": _abi.TQ_ENGINE_PLAIN}, id="fp32-plain"),
+           pytest.param({"precision": _abi.TQ_PREC_FP16, "engine": _abi.TQ_ENGINE_FUSED}, id="fp16-fused")]
+
+
+def _tanques():
+    return gerar_tanques(n=8, s=21, h=H, largura=(40, 120), altura=(30, 90))
+
+
+def _largos():
+    """A wide, flat atlas: its coarsest level (238 x 7) has more than 1024 cells, so CTA 0's
+    coarsest sweeps run on every warp."""
+    return gerar_tanques(n=12, s=22, h=H, largura=(120, 200), altura=(36, 50))
+
+
+@pytest.mark.parametrize("tanques", [_tanques, _largos], ids=["8-tanques", "largo"])
+@pytest.mark.parametrize("opcoes", MOTORES)
+def test_atlas_contra_o_oraculo(lib_gpu, opcoes, tanques):
+    at = montar_atlas(Cena, tanques(), H)
+    o = SimulacaoOraculo(at["cena"], dict(SOLVE, p2g_mode=_abi.TQ_P2G_FIXED))
+    g = SimulacaoGPU(at["cena"], dict(SOLVE, **opcoes))
+    for s in (o, g):
+        s.adicionar(at["particulas"], False)
+        s.avancar(1 / 240, 1)  # the water is moving before the compared substeps
+    copiar_estado(o, g)
+    for s in (o, g):
+        s.atualizarAr()
+    for campo in ["rotulo", "vivo"]:
+        assert np.array_equal(g.campo(campo), o.campo(campo)), campo
+    for quadro in range(2):
+        copiar_estado(o, g)
+        o.avancar(1 / 240, 1)
+        g.avancar(1 / 240, 1)
+        comparar_passo(o, g, f"substep {quadro}")
+    g.fechar()
+
+
+def test_lote_no_gpu(lib_gpu):
+    t = _tanques()
+    lote = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, t, H,
+                dict(SOLVE, precision=_abi.TQ_PREC_FP16, engine=_abi.TQ_ENGINE_FUSED), limite_grosso=300)
+    assert len(lote.atlas) >= 2
+    n0 = [len(lote.particulas(k)) for k in range(len(t))]
+    for _ in range(3):
+        lote.avancar(1 / 60, 4)
+    lote.sincronizar()
+    for k in range(len(t)):
+        q = lote.particulas(k)
+        assert len(q) == n0[k]
+        assert np.all(np.isfinite(q[:, :4]))
+        assert np.all(q[:, 0] > 0) and np.all(q[:, 0] < t[k]["nx"] * H)
+    lote.fechar()
