@@ -155,6 +155,35 @@ def medir_oraculo(passos, aquecimento, orcamento_s=None):
     return feitos / t, feitos, n_part
 
 
+def medir_oraculo_lote(orcamento_s=20.0):
+    """Tank-substeps/s of the CPU oracle on the 256-tank batch: the tanks in seed order, each a
+    scene of its own, one substep each in turn until the time budget is spent."""
+    sys.path.insert(0, os.path.join(RAIZ, "tests"))
+    from oraculo import SimulacaoOraculo
+    from tanque import Cena, _abi, passo_maximo
+    from tanque.cenarios import semear_retangulo_rapido
+    from tanque.lote import gerar_tanques
+    todos = gerar_tanques(h=LOTE_H)
+    dt = DT_QUADRO / math.ceil(DT_QUADRO / passo_maximo(LOTE_H, max(t["ny"] for t in todos) * LOTE_H) - 1e-9)
+    sims, feitos, t0 = [], 0, time.perf_counter()
+    tempo = 0.0
+    for t in todos:
+        cena = Cena(t["nx"], t["ny"], LOTE_H)
+        for tr in t["tracos"]:
+            cena.tracar(tr["x0"], tr["y0"], tr["x1"], tr["y1"], tr["raio"])
+        sim = SimulacaoOraculo(cena, {"p2g_mode": _abi.TQ_P2G_FLOAT, "tolerance": TOL, "iterations": MAX_ITER})
+        sim.adicionar(semear_retangulo_rapido(*t["agua"], LOTE_H, s=t["semente"]), False)
+        sim.atualizarAr()
+        sim.subpasso(dt)  # warm-up
+        a = time.perf_counter()
+        sim.subpasso(dt)
+        tempo += time.perf_counter() - a
+        feitos += 1
+        if time.perf_counter() - t0 > orcamento_s:
+            break
+    return feitos / tempo, feitos
+
+
 # ------------------------------------------------------------------ replicas
 def tempos_max_ranks(tempos, dist, dispositivo):
     """This rank's device times (ms) -> their maximum over the ranks, on every rank: the job's time
@@ -338,6 +367,142 @@ def executar_gpu(args, rank, mundo, dist):
     return linha
 
 
+# ------------------------------------------------------------------ the 256-tank batch
+LOTE_H = 0.003
+METRIC_LOTE = "tank-substeps/s @256-tank batch (8.8M cells): mixed vs FP32 plain at 1e-6 residual"
+
+
+def executar_lote(args, rank, mundo, dist):
+    """--workload lote: the 256-tank batch (tanque.lote), its tanks split over the GPUs by cells
+    and laid out in atlases; a step is one 1/60 s frame of every tank."""
+    import ctypes as C
+
+    import torch
+    from tanque import Cena, SimulacaoGPU, _abi, passo_maximo
+    from tanque.lote import BYTES_POR_CELULA_ITER, Lote, gerar_tanques, repartir
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    todos = gerar_tanques(h=LOTE_H)
+    meus = [todos[k] for k in repartir(todos, mundo)[rank]]
+    dt = passo_maximo(LOTE_H, max(t["ny"] for t in todos) * LOTE_H)
+    sub = math.ceil(DT_QUADRO / dt - 1e-9)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    hbm, origem_pico = picos()
+
+    def barreira():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def medir(precisao, motor, com_relogio=False, e2e=False):
+        lote = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H,
+                    {"tolerance": TOL, "iterations": MAX_ITER, "precision": precisao, "engine": motor, "device": dev})
+        fluxos = [torch.cuda.ExternalStream(s.stream()) for s in lote.sims]
+        lig = _abi.carregar()
+        saidas = []
+        if e2e:
+            for s in lote.sims:
+                cap = s.n + 16
+                saidas.append((torch.empty(cap * 12, dtype=torch.float32, pin_memory=True).numpy(), cap))
+        for q in range(args.warmup):
+            lote.avancar(DT_QUADRO, sub)
+        lote.sincronizar()
+        barreira()
+        for s in lote.sims:
+            s.tempos(True)
+        l0 = SimulacaoGPU.lancamentos()
+        rel = Relogios(dev) if com_relogio else None
+        if rel:
+            rel.__enter__()
+        eventos, d2h = [], 0
+        for q in range(args.steps):
+            p0 = fluxos[0]
+            with torch.cuda.stream(p0):
+                flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e0.record(p0)
+            for f in fluxos[1:]:
+                f.wait_event(e0)
+            lote.avancar(DT_QUADRO, sub)
+            if e2e:
+                for s, (buf, cap) in zip(lote.sims, saidas):
+                    n = C.c_int32(0)
+                    lig("get_particles", s._h, buf.ctypes.data, cap, C.byref(n))
+                    d2h += n.value * 48
+            for f in fluxos[1:]:
+                e = torch.cuda.Event()
+                e.record(f)
+                p0.wait_event(e)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record(p0)
+            eventos.append((e0, e1))
+        lote.sincronizar()
+        torch.cuda.synchronize()
+        if rel:
+            rel.__exit__()
+        lanc = SimulacaoGPU.lancamentos() - l0
+        ms = sum(a.elapsed_time(b) for a, b in eventos)
+        etapas = [s.tempos() for s in lote.sims]
+        celulas = [at["cena"].nx * at["cena"].ny for at in lote.atlas]
+        res = dict(ms=ms, lancamentos=lanc, particulas=lote.n, etapas=etapas, celulas=celulas,
+                   atlas=[[at["cena"].nx, at["cena"].ny] for at in lote.atlas], relogios=rel.resumo() if rel else None,
+                   d2h=d2h / max(args.steps, 1))
+        lote.fechar()
+        return res
+
+    def solve(res, rotulo):
+        """Pressure-solve figures of one rank: algorithmic MGPCG bytes over the solves' time."""
+        t = sum(e["pressao"] for e in res["etapas"]) / 1000
+        b = sum(c * (e["iteracoes"] * BYTES_POR_CELULA_ITER[rotulo][0] + e["subpassos"] * BYTES_POR_CELULA_ITER[rotulo][1])
+                for c, e in zip(res["celulas"], res["etapas"]))
+        iters = sum(e["iteracoes"] for e in res["etapas"]) / max(sum(e["subpassos"] for e in res["etapas"]), 1)
+        return dict(gbs=b / t / 1e9 if t > 0 else 0.0, iters=iters, bytes=b, s=t)
+
+    misto = medir(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED, com_relogio=True)
+    plano = medir(_abi.TQ_PREC_FP32, _abi.TQ_ENGINE_PLAIN)
+    e2e = medir(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED, e2e=True)
+    tempos = tempos_max_ranks([misto["ms"], plano["ms"], e2e["ms"]], dist, "cuda")
+    valor, valor_plano, valor_e2e = (len(todos) * args.steps * sub / (t / 1000) for t in tempos)
+    r_m, r_p = solve(misto, "fp16"), solve(plano, "fp32")
+    if rank != 0:
+        return None
+    return {
+        "metric": METRIC_LOTE,
+        "value": round(valor, 1),
+        "unit": "tank-substeps/s",
+        "n_gpus": mundo,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(tempos[0] / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"256 tanks (seed 4): widths logU[64,512], heights logU[64,320] cells, h=3mm, random walls, "
+                        f"water 20-70 %, 4 ppc; one step = 1 relabel + {sub} substeps of {DT_QUADRO / sub * 1000:.3f} ms "
+                        "for every tank",
+            "tank_cells": sum(t["nx"] * t["ny"] for t in todos), "atlases_rank0": misto["atlas"],
+            "atlas_cells_rank0": sum(misto["celulas"]), "particles_rank0": misto["particulas"], "tolerance": TOL,
+            "mixed_precision": "fp16 V-cycle storage", "mixed_engine": "fused",
+            "l2": "flushed (256 MB write) between timed steps", "parallelism": f"tanks split over {mundo} GPU(s) by cells",
+        },
+        "fp32_plain": {"value": round(valor_plano, 1), "unit": "tank-substeps/s", "mgpcg_gbs": round(r_p["gbs"], 1),
+                       "pcg_iters_per_atlas_substep": round(r_p["iters"], 2)},
+        "mixed": {"mgpcg_gbs": round(r_m["gbs"], 1), "pcg_iters_per_atlas_substep": round(r_m["iters"], 2),
+                  "speedup_vs_fp32_plain": round(valor / valor_plano, 3)},
+        "roofline": {"kernel": "MGPCG pressure solve", "bound": "hbm", "achieved": round(r_m["gbs"], 1),
+                     "peak": hbm, "peak_source": origem_pico, "unit": "GB/s", "frac": round(r_m["gbs"] / hbm, 4),
+                     "traffic": None},
+        "e2e": {"value": round(valor_e2e, 1), "unit": "tank-substeps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(e2e["d2h"])},
+        "gpu_launches": int(misto["lancamentos"]),
+        "clocks": misto["relogios"],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -347,11 +512,29 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-oracle timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", dest="fused", action="store_false", help="mixed config on the plain engine")
+    ap.add_argument("--workload", default="ultra", choices=["ultra", "lote"],
+                    help="ultra: the 450k-cell scene (default); lote: the 256-tank batch")
     args = ap.parse_args()
 
     mundo = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
 
+    if args.impl == "reference" and args.workload == "lote":
+        if rank != 0:
+            return
+        v, feitos = medir_oraculo_lote(args.cpu_budget)
+        linha = {
+            "metric": METRIC_LOTE, "impl": "reference", "value": round(v, 3), "unit": "tank-substeps/s",
+            "n_gpus": args.gpus, "steps": feitos, "warmup": 1, "ms_per_step": round(1000 / v, 2),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "256-tank batch (as ours); one step = one substep of one tank", "tolerance": TOL},
+            "cpu_baseline": {"value": round(v, 3), "unit": "tank-substeps/s", "cores": 1, "kind": "port",
+                             "sample": f"one substep of each of the first {feitos} tanks after one warm-up substep, "
+                                       "CPU oracle (reference CPU engine restated in C++, single thread)"},
+            "e2e": {"value": round(v, 3), "unit": "tank-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(linha))
+        return
     if args.impl == "reference":
         if rank != 0:
             return
@@ -377,12 +560,17 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    linha = executar_gpu(args, rank, mundo, dist)
+    linha = (executar_lote if args.workload == "lote" else executar_gpu)(args, rank, mundo, dist)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0 and linha is not None:
-        if mundo == 1 and not args.no_cpu_baseline:
+        if mundo == 1 and not args.no_cpu_baseline and args.workload == "lote":
+            v, feitos = medir_oraculo_lote(args.cpu_budget)
+            linha["cpu_baseline"] = {"value": round(v, 3), "unit": "tank-substeps/s", "cores": 1, "kind": "port",
+                                     "sample": f"one substep of each of the first {feitos} tanks of the batch after "
+                                               "one warm-up substep (CPU oracle, single thread)"}
+        if mundo == 1 and not args.no_cpu_baseline and args.workload == "ultra":
             v, feitos, n_part = medir_oraculo(10 ** 6, 1, orcamento_s=args.cpu_budget)
             linha["cpu_baseline"] = {"value": round(v, 4), "unit": "steps/s", "cores": 1, "kind": "port",
                                      "sample": f"{feitos} substeps of the same scene after 1 warm-up substep "

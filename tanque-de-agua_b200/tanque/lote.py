@@ -217,3 +217,20 @@ class Lote:
         for s in self.sims:
             if hasattr(s, "fechar"):
                 s.fechar()
+
+
+def repartir(tanques: list[dict], partes: int) -> list[list[int]]:
+    """Tank indices per GPU: largest tank first onto the least-loaded GPU (by cells).  The tanks
+    are independent, so the GPUs share no data while they step."""
+    carga = [0] * partes
+    out: list[list[int]] = [[] for _ in range(partes)]
+    for k in sorted(range(len(tanques)), key=lambda k: (-tanques[k]["nx"] * tanques[k]["ny"], k)):
+        p = min(range(partes), key=lambda i: (carga[i], i))
+        out[p].append(k)
+        carga[p] += tanques[k]["nx"] * tanques[k]["ny"]
+    return [sorted(o) for o in out]
+
+
+# Algorithmic HBM bytes of the pressure solve per atlas cell: (per PCG iteration, per solve's
+# setup), for FP32 and 16-bit V-cycle storage (the same model as the single-tank benchmark).
+BYTES_POR_CELULA_ITER = {"fp32": (156.0, 110.0), "fp16": (120.0, 85.0), "bf16": (120.0, 85.0)}

@@ -135,3 +135,14 @@ def test_lote_avanca_e_separa_os_tanques():
         assert len(q) == n0[k]  # no particle leaves its tank
         assert np.all(q[:, 0] > 0) and np.all(q[:, 0] < t[k]["nx"] * H)
         assert lote.campo(k, "tipo").shape == (t[k]["ny"], t[k]["nx"])
+
+
+@pytest.mark.parametrize("partes", [1, 2, 3, 8])
+def test_repartir_entre_gpus(partes):
+    from tanque.lote import repartir
+    t = gerar_tanques()
+    grupos = repartir(t, partes)
+    assert sorted(k for g in grupos for k in g) == list(range(256))
+    cargas = [sum(t[k]["nx"] * t[k]["ny"] for k in g) for g in grupos]
+    maior = max(x["nx"] * x["ny"] for x in t)
+    assert max(cargas) - min(cargas) <= maior  # LPT: within one tank of balance
