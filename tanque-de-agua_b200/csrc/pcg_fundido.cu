@@ -58,8 +58,8 @@ constexpr int PERFIL_SECAO = 1 << 14;              // coarse-section stamps (aft
 // per-warp shared-memory areas (floats)
 constexpr int CT = 121;                            // 11x11 coarse tile for the folded prolongation
 constexpr int SUAV_W = CT + 7;                     // the coarse tile of a PROL pass
-constexpr int RX = 6 * 68, RB = 4 * 66;            // restriction staging: x rows, b/viz/residual rows
-constexpr int REST_W = RX + 3 * RB;                // x, b, residual (floats) + viz (bytes in one RB)
+// restriction staging of up to two coarse rows: x (8 x 68), b / residual (floats) + viz (bytes) (6 x 66)
+constexpr int REST_W = 8 * 68 + 3 * 6 * 66;
 
 struct NivelF {
   int nx, ny, meia, pad;
@@ -355,13 +355,15 @@ struct Reuniao {
 
 // ---------------------------------------------------------------- register-resident block sweep
 // Lane l of the warp that owns a 16x16 block holds, for each colour c and m = 0..3, the cell of
-// colour c in row g + 4m (g = l >> 3) among the columns 2k, 2k + 1 (k = l & 7): its column is
-// (c + 1 + g) & 1, since a cell's colour is (row + column + 1) & 1 (js/pressao-cpu.js:120).  It
+// colour c in row 4g + m (g = l >> 3) among the columns 2k, 2k + 1 (k = l & 7): its column is
+// (c + 1 + m) & 1, since a cell's colour is (row + column + 1) & 1 (js/pressao-cpu.js:120).  It
 // also holds the block's frame next to its cells: left and right of its rows (k = 0, k = 7),
 // below and above its columns (g = 0, g = 3).  In a half-sweep of colour COR every neighbour of
-// an updated cell has the other colour: the lane's own other cell, the same rows in lane
-// l -/+ 1, the rows below and above in lanes l -/+ 8 (l +/- 24 with the next m across the group
-// edge), or the frame.  Values move by shuffles; a half-sweep reads no value that it writes.
+// an updated cell has the other colour: the lane's own other cell in the row, the rows m -/+ 1
+// of the lane (same column), the row in lane l -/+ 1, the row below row 0 in lane l - 8 (its
+// m = 3), the row above row 3 in lane l + 8 (its m = 0), or the frame: 6 shuffles a half-sweep,
+// which keeps the shuffle pipe, shared by the SM's warps, half as busy as rows g + 4m would.
+// A half-sweep reads no value that it writes.
 // Every snapshot holds x = 0 on cells that are not water (the passes store 0 there, the frame
 // outside the grid is 0), so a wall neighbour adds +0 and the sum needs no mask; only 1/k and
 // whether the cell changes come from the mask.
@@ -374,23 +376,20 @@ template <int COR>
 __device__ __forceinline__ void meiaReg(float (&x)[2][4], const float (&bq)[2][4], const float (&iq)[2][4],
                                         const float (&at)[2][4], const Moldura& f) {
   const int lane = threadIdx.x & 31, g = lane >> 3, k = lane & 7;
-  const int jc = (COR + 1 + g) & 1;  // the lane's column of colour COR
-  float H[4], D[4], U[4];
-  const int srcH = (jc ? lane + 1 : lane - 1) & 31;
+  float H[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++)  // row m's neighbour in lane l + 1 (colour COR in the odd column) or l - 1
+    H[m] = __shfl_sync(0xffffffffu, x[1 - COR][m], (((COR + 1 + m) & 1) ? lane + 1 : lane - 1) & 31);
+  const float D = __shfl_sync(0xffffffffu, x[1 - COR][3], (lane - 8) & 31);
+  const float U = __shfl_sync(0xffffffffu, x[1 - COR][0], (lane + 8) & 31);
 #pragma unroll
   for (int m = 0; m < 4; m++) {
-    H[m] = __shfl_sync(0xffffffffu, x[1 - COR][m], srcH);
-    D[m] = __shfl_sync(0xffffffffu, x[1 - COR][m], (lane - 8) & 31);
-    U[m] = __shfl_sync(0xffffffffu, x[1 - COR][m], (lane + 8) & 31);
-  }
-  const float fb = jc ? f.bai[1] : f.bai[0], fc = jc ? f.cim[1] : f.cim[0];
-#pragma unroll
-  for (int m = 0; m < 4; m++) {
+    const int jc = (COR + 1 + m) & 1;  // the column of colour COR in row m
     const float y = x[1 - COR][m];
     const float esq = jc ? y : (k == 0 ? f.esq[m] : H[m]);
     const float dir = jc ? (k == 7 ? f.dir[m] : H[m]) : y;
-    const float baixo = g >= 1 ? D[m] : (m >= 1 ? D[m > 0 ? m - 1 : 0] : fb);
-    const float cima = g <= 2 ? U[m] : (m <= 2 ? U[m < 3 ? m + 1 : 3] : fc);
+    const float baixo = m >= 1 ? x[1 - COR][m >= 1 ? m - 1 : 0] : (g >= 1 ? D : f.bai[jc]);
+    const float cima = m <= 2 ? x[1 - COR][m <= 2 ? m + 1 : 3] : (g <= 2 ? U : f.cim[jc]);
     const float sm = ((esq + dir) + baixo) + cima;
     const float q = x[COR][m];
     const float dlt = (sm + bq[COR][m]) * iq[COR][m] - q;
@@ -473,7 +472,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   for (int cr = 0; cr < 2; cr++)
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-      const int gx = ox + 2 * k + ((cr + 1 + gl) & 1), gy = oy + gl + 4 * m;
+      const int gx = ox + 2 * k + ((cr + 1 + m) & 1), gy = oy + 4 * gl + m;
       const bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
       const int c = gx + gy * nx;
       cel[cr][m] = dentro ? c : -1;
@@ -488,7 +487,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     }
 #pragma unroll
   for (int m = 0; m < 4; m++) {
-    const int gy = oy + gl + 4 * m;
+    const int gy = oy + 4 * gl + m;
     const int gxL = ox - 1, gxR = ox + 16;
     const bool okL = k == 0 && gxL >= 0 && gy >= 0 && gy < ny;
     const bool okR = k == 7 && gxR < nx && gy >= 0 && gy < ny;
@@ -541,10 +540,10 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     for (int cr = 0; cr < 2; cr++)
 #pragma unroll
       for (int m = 0; m < 4; m++)
-        if (v[cr][m] & 16) x[cr][m] += correcaoGrossa(ct, cx0, cy0, ox + 2 * k + ((cr + 1 + gl) & 1), oy + gl + 4 * m);
+        if (v[cr][m] & 16) x[cr][m] += correcaoGrossa(ct, cx0, cy0, ox + 2 * k + ((cr + 1 + m) & 1), oy + 4 * gl + m);
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-      const int gy = oy + gl + 4 * m;
+      const int gy = oy + 4 * gl + m;
       if (aguaF >> m & 1) f.esq[m] += correcaoGrossa(ct, cx0, cy0, ox - 1, gy);
       if (aguaF >> (4 + m) & 1) f.dir[m] += correcaoGrossa(ct, cx0, cy0, ox + 16, gy);
     }
@@ -676,56 +675,61 @@ __device__ void faseSuavizar(const Args& a, int l, int desl, int ordem, bool par
 }
 
 // ---------------------------------------------------------------- restriction
-// restringir (js/pressao-cpu.js:159-188) as a gather, one warp per 32-cell coarse row
-// segment: the fine footprint (x on 6 rows x 68 columns; b and flags on 4 x 66) is staged in
-// the warp's shared area, residuals computed once, then each lane sums its 4x4 window.
-template <class TFino>
-__device__ void faseRestringir(const Args& a, int l, float* areas) {
+// restringir (js/pressao-cpu.js:159-188) as a gather, one warp per region of R coarse rows x 32
+// columns: the fine footprint (x on 2R+4 rows x 68 columns; b and flags on 2R+2 x 66) is staged
+// in the warp's shared area, residuals computed once, then each lane sums its 4x4 windows.
+template <class TFino, int R>
+__device__ __forceinline__ void faseRestringirR(const Args& a, int l, float* areas) {
+  constexpr int RXn = (2 * R + 4) * 68, RBn = (2 * R + 2) * 66;
+  constexpr int KX = (RXn + 31) / 32, KB = (RBn + 31) / 32;
+  static_assert(RXn + 3 * RBn <= REST_W, "restriction staging area");
   const NivelF f = s_niv[l];
   const NivelF g = s_niv[l + 1];
   const bool secao = l + 1 == a.Lc;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   float* xs = areas + w * REST_W;
-  float* bs = xs + RX;
-  float* rs = bs + RB;
-  uint8_t* vs = (uint8_t*)(rs + RB);
+  float* bs = xs + RXn;
+  float* rs = bs + RBn;
+  uint8_t* vs = (uint8_t*)(rs + RBn);
   const float pes[4] = {0.25f, 0.75f, 0.75f, 0.25f};
   const int nseg = (g.nx + 31) >> 5;
-  const int total = nseg * g.ny;
+  const int total = nseg * ((g.ny + R - 1) / R);
   for (int seg = w * gridDim.x + blockIdx.x; seg < total; seg += WARPS * gridDim.x) {
-    const int J = seg / nseg, I0 = (seg % nseg) * 32;
-    const int fi0 = 2 * I0 - 2, fj0 = 2 * J - 2;  // x window origin (fine)
+    const int J0 = (seg / nseg) * R, I0 = (seg % nseg) * 32;
+    const int fi0 = 2 * I0 - 2, fj0 = 2 * J0 - 2;  // x window origin (fine)
     const int I = I0 + lane;
-    const int gvz = I < g.nx ? ldcg8(g.viz + I + J * g.nx) : 0;
+    int gvz[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) gvz[r] = (I < g.nx && J0 + r < g.ny) ? ldcg8(g.viz + I + (J0 + r) * g.nx) : 0;
     // staging loads issued as one batch per array (registers, then shared memory)
     {
-      float xv[13];
+      float xv[KX];
 #pragma unroll
-      for (int k = 0; k < 13; k++) {
+      for (int k = 0; k < KX; k++) {
         const int s = lane + 32 * k;
         const int i = fi0 + s % 68, j = fj0 + s / 68;
-        xv[k] = (s < RX && i >= 0 && j >= 0 && i < f.nx && j < f.ny) ? carregar(ldcg((const TFino*)f.x + i + j * f.nx)) : 0.0f;
+        xv[k] = (s < RXn && i >= 0 && j >= 0 && i < f.nx && j < f.ny) ? carregar(ldcg((const TFino*)f.x + i + j * f.nx)) : 0.0f;
       }
-      float bv[9];
-      int vv[9];
+      float bv[KB];
+      int vv[KB];
 #pragma unroll
-      for (int k = 0; k < 9; k++) {
+      for (int k = 0; k < KB; k++) {
         const int s = lane + 32 * k;
         const int i = fi0 + 1 + s % 66, j = fj0 + 1 + s / 66;
-        const bool d = s < RB && i >= 0 && j >= 0 && i < f.nx && j < f.ny;
+        const bool d = s < RBn && i >= 0 && j >= 0 && i < f.nx && j < f.ny;
         const int c = i + j * f.nx;
         vv[k] = d ? ldcg8(f.viz + c) : 0;
         bv[k] = d ? carregar(ldcg((const TFino*)f.b + c)) : 0.0f;
       }
 #pragma unroll
-      for (int k = 0; k < 13; k++) {
+      for (int k = 0; k < KX; k++) {
         const int s = lane + 32 * k;
-        if (s < RX) xs[s] = xv[k];
+        if (s < RXn) xs[s] = xv[k];
       }
 #pragma unroll
-      for (int k = 0; k < 9; k++) {
+      for (int k = 0; k < KB; k++) {
         const int s = lane + 32 * k;
-        if (s < RB) {
+        if (s < RBn) {
           vs[s] = (uint8_t)vv[k];
           bs[s] = bv[k];
         }
@@ -733,37 +737,49 @@ __device__ void faseRestringir(const Args& a, int l, float* areas) {
     }
     __syncwarp();
     {
-      // residuals of the 4 x 66 fine cells: every shared load of the lane's nine cells goes out
-      // before the first store.  x is 0 off water and outside the grid, so the neighbour sum
-      // needs no mask; the residual is 0 off water.
-      float rv[9];
+      // residuals of the fine cells: every shared load of the lane's cells goes out before the
+      // first store.  x is 0 off water and outside the grid, so the neighbour sum needs no
+      // mask; the residual is 0 off water.
+      float rv[KB];
 #pragma unroll
-      for (int k = 0; k < 9; k++) {
-        const int s = lane + 32 * k < RB ? lane + 32 * k : 0;
+      for (int k = 0; k < KB; k++) {
+        const int s = lane + 32 * k < RBn ? lane + 32 * k : 0;
         const float* xc = xs + (s / 66 + 1) * 68 + s % 66 + 1;
         const int vz = vs[s];
         const float t = ((xc[-1] + xc[1]) + xc[-68]) + xc[68];
         rv[k] = (vz & 16) ? bs[s] - ((float)__popc(vz & 15) * xc[0] - t) : 0.0f;
       }
 #pragma unroll
-      for (int k = 0; k < 9; k++)
-        if (lane + 32 * k < RB) rs[lane + 32 * k] = rv[k];
+      for (int k = 0; k < KB; k++)
+        if (lane + 32 * k < RBn) rs[lane + 32 * k] = rv[k];
     }
     __syncwarp();
-    if (I < g.nx) {
-      const int C = I + J * g.nx;
-      float soma = 0.0f;
-      if (gvz & 16) {
 #pragma unroll
-        for (int bb = 0; bb < 4; bb++)
+    for (int r = 0; r < R; r++)
+      if (I < g.nx && J0 + r < g.ny) {
+        const int C = I + (J0 + r) * g.nx;
+        float soma = 0.0f;
+        if (gvz[r] & 16) {
 #pragma unroll
-          for (int aa = 0; aa < 4; aa++) soma += rs[bb * 66 + 2 * lane + aa] * (pes[aa] * pes[bb]);
+          for (int bb = 0; bb < 4; bb++)
+#pragma unroll
+            for (int aa = 0; aa < 4; aa++) soma += rs[(2 * r + bb) * 66 + 2 * lane + aa] * (pes[aa] * pes[bb]);
+        }
+        if (secao) a.bc[C] = soma;
+        else gravarN(g.meia, g.b, C, soma);  // x of the coarse level: its first pass reads 0
       }
-      if (secao) a.bc[C] = soma;
-      else gravarN(g.meia, g.b, C, soma);  // x of the coarse level: its first pass reads 0
-    }
     __syncwarp();
   }
+}
+
+// Two coarse rows per warp where one-row segments would take four or more rounds of the
+// grid's warps (the finest restriction of a large atlas): half the rounds, each with the 6
+// residual rows of 2 coarse rows instead of 2 x 4.
+template <class TFino>
+__device__ void faseRestringir(const Args& a, int l, float* areas) {
+  const NivelF g = s_niv[l + 1];
+  if (((g.nx + 31) >> 5) * g.ny > 4 * WARPS * (int)gridDim.x) faseRestringirR<TFino, 2>(a, l, areas);
+  else faseRestringirR<TFino, 1>(a, l, areas);
 }
 
 // ---------------------------------------------------------------- coarse section (CTA 0)
@@ -791,7 +807,7 @@ __device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int
     for (int cr = 0; cr < 2; cr++)
 #pragma unroll
       for (int m = 0; m < 4; m++) {
-        const int gx = ox + 2 * k + ((cr + 1 + gl) & 1), gy = oy + gl + 4 * m;
+        const int gx = ox + 2 * k + ((cr + 1 + m) & 1), gy = oy + 4 * gl + m;
         const bool dentro = gx >= 0 && gy >= 0 && gx < nx && gy < ny;
         const int c = gx + gy * nx;
         cel[cr][m] = dentro ? c : -1;
@@ -801,7 +817,7 @@ __device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int
       }
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-      const int gy = oy + gl + 4 * m;
+      const int gy = oy + 4 * gl + m;
       const bool okL = k == 0 && ox - 1 >= 0 && gy >= 0 && gy < ny;
       const bool okR = k == 7 && ox + 16 < nx && gy >= 0 && gy < ny;
       f.esq[m] = okL ? F[src + ox - 1 + gy * nx] : 0.0f;
