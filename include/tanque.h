@@ -104,6 +104,27 @@ int tq_destroy(tq_sim* s);
  * (Cena.celulaSolida, js/cena.js:119-127). */
 int tq_set_walls(tq_sim* s, const float* sdf, int32_t mw, int32_t mh);
 
+/* Cena.tracar(x0, y0, x1, y1, raio, apagar) (js/cena.js:43-72) + atualizarParedes, on the
+ * device: draws (erase = 0) or erases (erase != 0) a capsule wall segment (metres) in the
+ * handle's SDF mask, in the reference's double arithmetic, and recomputes the solid cells.
+ * The mask equals, bit for bit, the one Cena.tracar makes.  Non-finite arguments: TQ_E_ARG
+ * (the JavaScript draws nothing or NaNs). */
+int tq_trace_wall(tq_sim* s, double x0, double y0, double x1, double y1, double radius, int32_t erase);
+
+/* Cena.limpar() (js/cena.js:74-77, #zerar :139-144) + atualizarParedes on the device: the mask
+ * of an empty tank (the frame alone) and its solid cells. */
+int tq_clear_walls(tq_sim* s);
+
+/* The particle splat of the renderer (WGSL_MANCHA, js/gpu/render.js:11-43, drawn in
+ * js/gpu/render.js:236-265) without a graphics API: into `out`, a DEVICE buffer of 5 * w * h
+ * floats (planes of w x h pixels covering the tank, row 0 at the top), every live particle
+ * adds at each pixel centre within RAIO_MANCHA = 2.1 cells the weight (1 - r^2)^2 (plane 0),
+ * times its foam (plane 1) and times its three absorptions (planes 2-4); r is the distance
+ * over the radius.  Sums are 64-bit fixed point (2^-32), so the image does not depend on the
+ * order of the particles; the renderer keeps them in half floats.  Runs on the handle's
+ * stream and returns when `out` is written.  w * h above 2^26: TQ_E_ARG. */
+int tq_splat(tq_sim* s, int32_t w, int32_t h, float* out);
+
 /* SimulacaoCPU.adicionar(lista, checarCheia) (js/fisica-cpu.js:92-111).  Particles inside
  * walls or (check_full) in a cell already holding >= 3 particles are skipped.  *accepted
  * receives the count kept.  Particles beyond capacity: TQ_E_CAPACITY, nothing added. */

@@ -1564,6 +1564,43 @@ double tqo_scene_distance(tqo_scene* c, double x, double y) { return c->c.distan
 void tqo_scene_normal(tqo_scene* c, double x, double y, double* nx, double* ny) { c->c.normal(x, y, nx, ny); }
 int32_t tqo_scene_solid_cell(tqo_scene* c, int32_t i, int32_t j) { return c->c.celulaSolida(i, j) ? 1 : 0; }
 
+// WGSL_MANCHA (js/gpu/render.js:11-43) restated on the CPU: the w x h target covers the tank
+// (W = nx h, H = ny h as f32, row 0 at the top); a live particle (x >= 0) adds at each pixel
+// centre within raio = RAIO_MANCHA h (f32) the weight (1 - r^2)^2, r = |centre - position| /
+// raio, and that weight times its extra vector (foam, three absorptions), in f32 arithmetic;
+// the sums are 64-bit fixed point (2^32) and `out` gets them as floats, 5 planes of w x h.
+void tqo_splat(const float* p12, int32_t n, int32_t nx, int32_t ny, double h, int32_t w, int32_t hp, float* out) {
+  const size_t plano = (size_t)w * hp;
+  std::vector<long long> acc(5 * plano, 0);
+  const float W = (float)(nx * h), H = (float)(ny * h), raio = (float)(2.1 * h);
+  const float px = W / (float)w, py = H / (float)hp;
+  auto fixo = [](float v) { return (long long)std::nearbyint((double)v * 4294967296.0); };
+  for (int32_t k = 0; k < n; k++) {
+    const float* p = p12 + (size_t)k * CAMPOS;
+    const float x = p[0], y = p[1];
+    if (!(x == x) || !(y == y) || x < 0.0f) continue;
+    const float e[4] = {p[8], p[9], p[10], p[11]};
+    const int i0 = std::max(0, (int)std::floor((x - raio) / px - 0.5f) - 1);
+    const int i1 = std::min(w - 1, (int)std::ceil((x + raio) / px - 0.5f) + 1);
+    const int j0 = std::max(0, (int)std::floor((H - (y + raio)) / py - 0.5f) - 1);
+    const int j1 = std::min(hp - 1, (int)std::ceil((H - (y - raio)) / py - 0.5f) + 1);
+    for (int j = j0; j <= j1; j++) {
+      const float v = ((H - ((float)j + 0.5f) * py) - y) / raio;
+      for (int i = i0; i <= i1; i++) {
+        const float u = (((float)i + 0.5f) * px - x) / raio;
+        const float r2 = u * u + v * v;
+        if (r2 >= 1.0f) continue;
+        const float wt = (1.0f - r2) * (1.0f - r2);
+        const size_t q = (size_t)j * w + i;
+        acc[q] += fixo(wt);
+        for (int c = 0; c < 4; c++)
+          if (e[c] != 0.0f) acc[(c + 1) * plano + q] += fixo(wt * e[c]);
+      }
+    }
+  }
+  for (size_t q = 0; q < 5 * plano; q++) out[q] = (float)((double)acc[q] * (1.0 / 4294967296.0));
+}
+
 // passoMaximo, js/constantes.js:167-175
 double tqo_passo_maximo(double h, double altura, double vmax, int32_t has_vmax, double dt_frame) {
   double queda = std::sqrt(2 * GRAVIDADE * altura) * 1.15 + 0.5;

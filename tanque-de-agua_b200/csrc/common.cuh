@@ -24,6 +24,7 @@ constexpr double PARTICULAS_POR_CELULA = 4;
 constexpr int RES_MASCARA = 2;
 constexpr double SDF_MAX = 10;
 constexpr int MOLDURA = 2;
+constexpr double RAIO_MANCHA = 2.1;  // splat radius in cells (js/constantes.js:120)
 constexpr double RAIO_PARTICULA = 0.3;
 constexpr double MICROPASSO = 0.8;
 constexpr double MAX_MICROPASSOS = 4;

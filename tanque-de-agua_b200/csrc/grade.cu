@@ -24,6 +24,41 @@ __global__ void k_solidos(Dev d) {
   d.solido[c] = soma < 0 ? 1 : 0;
 }
 
+// Cena#moldura (js/cena.js:131-137): distance (cells) from mask point (x, y) to the frame's
+// inner edge, positive inside the tank, clamped to +-SDF_MAX.
+__device__ double molduraMascara(int x, int y, int mw, int mh) {
+  const double m = MOLDURA * RES_MASCARA - 0.5;
+  const double d = fmin(fmin(x - m, (double)(mw - 1) - m - x), fmin(y - m, (double)(mh - 1) - m - y)) / RES_MASCARA;
+  return d > SDF_MAX ? SDF_MAX : d < -SDF_MAX ? -SDF_MAX : d;
+}
+
+// Cena.tracar (js/cena.js:43-72) on the device mask: one thread per mask point of the
+// segment's box (x0, y0, nbx x nby), the capsule distance in double precision as the reference
+// computes it, min into the mask (draw) or max of its negation capped by the frame (erase).
+__global__ void k_tracar(float* sdf, int mw, int mh, int x0, int y0, int nbx, int nby, double ax, double ay, double dx,
+                         double dy, double len2, double rp, int apagar) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nbx * nby) return;
+  const int x = x0 + idx % nbx, y = y0 + idx / nbx;
+  double t = len2 > 0 ? ((x - ax) * dx + (y - ay) * dy) / len2 : 0;
+  t = t < 0 ? 0 : t > 1 ? 1 : t;
+  const double px = ax + t * dx - x, py = ay + t * dy - y;
+  double d = (sqrt(px * px + py * py) - rp) / RES_MASCARA;
+  if (d > SDF_MAX) d = SDF_MAX;
+  else if (d < -SDF_MAX) d = -SDF_MAX;
+  const size_t k = (size_t)y * mw + x;
+  double v = apagar ? fmax((double)sdf[k], -d) : fmin((double)sdf[k], d);
+  if (apagar) v = fmin(v, molduraMascara(x, y, mw, mh));
+  sdf[k] = (float)v;
+}
+
+// Cena#zerar (js/cena.js:139-144): the mask of an empty tank, the frame alone.
+__global__ void k_zerar_mascara(float* sdf, int mw, int mh) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= mw * mh) return;
+  sdf[idx] = (float)molduraMascara(idx % mw, idx / mw, mw, mh);
+}
+
 // #tipos (js/fisica-cpu.js:293-299); with `ar`, the first step of #propagarRotulos (:412,
 // non-air cells lose their label) and the initial water fraction of #superficie (:309).
 __global__ void k_tipos(Dev d, int ar, int fase) {
@@ -341,6 +376,24 @@ __global__ void k_extrapolar(Dev d, int volta) {
 
 // ---------------------------------------------------------------- host launchers
 void lancarSolidos(const Dev& d, cudaStream_t s) { lanca(k_solidos, blocos(d.N, 256), 256, 0, s, d); }
+void lancarTracar(const Dev& d, double x0m, double y0m, double x1m, double y1m, double raio, bool apagar,
+                  cudaStream_t s) {
+  // the box and the segment in mask points, on the host in the same double arithmetic
+  const double r = RES_MASCARA, esc = r / d.h;
+  const double ax = x0m * esc - 0.5, ay = y0m * esc - 0.5, bx = x1m * esc - 0.5, by = y1m * esc - 0.5;
+  const double rp = raio * esc;
+  const double alc = rp + SDF_MAX * r + 1;
+  const double xmin = fmax(0.0, floor(fmin(ax, bx) - alc)), xmax = fmin((double)(d.mw - 1), ceil(fmax(ax, bx) + alc));
+  const double ymin = fmax(0.0, floor(fmin(ay, by) - alc)), ymax = fmin((double)(d.mh - 1), ceil(fmax(ay, by) + alc));
+  if (!(xmin <= xmax) || !(ymin <= ymax)) return;
+  const int nbx = (int)(xmax - xmin) + 1, nby = (int)(ymax - ymin) + 1;
+  const double dx = bx - ax, dy = by - ay;
+  lanca(k_tracar, blocos(nbx * nby, 256), 256, 0, s, (float*)d.sdf, d.mw, d.mh, (int)xmin, (int)ymin, nbx, nby, ax, ay, dx, dy,
+        dx * dx + dy * dy, rp, apagar ? 1 : 0);
+}
+void lancarZerarMascara(const Dev& d, cudaStream_t s) {
+  lanca(k_zerar_mascara, blocos(d.mw * d.mh, 256), 256, 0, s, (float*)d.sdf, d.mw, d.mh);
+}
 void lancarTipos(const Dev& d, bool ar, cudaStream_t s) {
   lanca(k_tipos, blocos(d.N, 256), 256, 0, s, d, ar ? 1 : 0, 1);
 }

@@ -17,6 +17,9 @@ void lancarFerramenta(const Dev& d, int nHint, const tq_tool& f, cudaStream_t s)
 
 // grade.cu
 void lancarSolidos(const Dev& d, cudaStream_t s);
+void lancarTracar(const Dev& d, double x0, double y0, double x1, double y1, double raio, bool apagar, cudaStream_t s);
+void lancarZerarMascara(const Dev& d, cudaStream_t s);
+void lancarMancha(const Dev& d, int n, int w, int hp, unsigned long long* acc, float* out, cudaStream_t s);
 void lancarTipos(const Dev& d, bool ar, cudaStream_t s);
 void lancarPropagarRotulos(const Dev& d, cudaStream_t s);
 void lancarSuperficie(const Dev& d, cudaStream_t s);

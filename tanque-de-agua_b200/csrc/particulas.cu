@@ -460,6 +460,56 @@ __global__ void k_ferramenta(Dev d, tq_tool f) {
 }
 
 // ---------------------------------------------------------------- host launchers
+// ---------------------------------------------------------------- headless splat
+// WGSL_MANCHA (js/gpu/render.js:11-43) without a graphics pipeline: every live particle adds,
+// at each pixel centre of a w x h target covering the tank (row 0 at the top, as the render
+// target), the weight (1 - r^2)^2 with r the distance over raio = RAIO_MANCHA h, and that
+// weight times its foam and its three absorptions.  The f32 operations are the restatement's
+// (no fused multiply-add in this file); the sums are 64-bit fixed point (2^32), so they do
+// not depend on the order of the atomics.
+__device__ __forceinline__ long long fixoMancha(float v) { return __double2ll_rn((double)v * 4294967296.0); }
+
+__global__ void k_mancha(Dev d, int n, int w, int hp, float W, float H, float raio, unsigned long long* acc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float4 a = d.p0[k], e = d.p2[k];
+  const float x = a.x, y = a.y;
+  if (!(x == x) || !(y == y) || x < 0.0f) return;
+  const float px = W / (float)w, py = H / (float)hp;
+  const int i0 = max(0, (int)floorf((x - raio) / px - 0.5f) - 1), i1 = min(w - 1, (int)ceilf((x + raio) / px - 0.5f) + 1);
+  const int j0 = max(0, (int)floorf((H - (y + raio)) / py - 0.5f) - 1);
+  const int j1 = min(hp - 1, (int)ceilf((H - (y - raio)) / py - 0.5f) + 1);
+  const size_t plano = (size_t)w * hp;
+  for (int j = j0; j <= j1; j++) {
+    const float v = ((H - ((float)j + 0.5f) * py) - y) / raio;
+    for (int i = i0; i <= i1; i++) {
+      const float u = (((float)i + 0.5f) * px - x) / raio;
+      const float r2 = u * u + v * v;
+      if (r2 >= 1.0f) continue;
+      const float wt = (1.0f - r2) * (1.0f - r2);
+      unsigned long long* q = acc + (size_t)j * w + i;
+      atomicAdd(q, (unsigned long long)fixoMancha(wt));
+      if (e.x != 0.0f) atomicAdd(q + plano, (unsigned long long)fixoMancha(wt * e.x));
+      if (e.y != 0.0f) atomicAdd(q + 2 * plano, (unsigned long long)fixoMancha(wt * e.y));
+      if (e.z != 0.0f) atomicAdd(q + 3 * plano, (unsigned long long)fixoMancha(wt * e.z));
+      if (e.w != 0.0f) atomicAdd(q + 4 * plano, (unsigned long long)fixoMancha(wt * e.w));
+    }
+  }
+}
+
+__global__ void k_mancha_float(const long long* acc, float* out, size_t total) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < total) out[k] = (float)((double)acc[k] * (1.0 / 4294967296.0));
+}
+
+void lancarMancha(const Dev& d, int n, int w, int hp, unsigned long long* acc, float* out, cudaStream_t s) {
+  const size_t total = (size_t)5 * w * hp;
+  cudaMemsetAsync(acc, 0, total * sizeof(unsigned long long), s);
+  const float W = (float)(d.nx * d.h), H = (float)(d.ny * d.h), raio = (float)(RAIO_MANCHA * d.h);
+  if (n > 0) lanca(k_mancha, blocos(n, 256), 256, 0, s, d, n, w, hp, W, H, raio, acc);
+  lanca(k_mancha_float, (unsigned)((total + 255) / 256), 256, 0, s, (const long long*)acc, out, total);
+}
+
 void lancarP2G(const Dev& d, int nHint, cudaStream_t s) {
   if (nHint > 0) lanca(k_p2g, blocos(nHint, 256), 256, 0, s, d);
 }

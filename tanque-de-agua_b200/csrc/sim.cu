@@ -66,6 +66,8 @@ struct tq_sim {
   int *cont = nullptr, *offs = nullptr, *estado = nullptr;
   float* staging = nullptr;
   size_t stagingCap = 0;
+  unsigned long long* mancha = nullptr;  // tq_splat's fixed-point sums (5 planes), grown on demand
+  size_t manchaCap = 0;
   std::vector<void*> alocados;
   // Stage timing (tq_set_timing): a pool of events recorded at the stage boundaries of every
   // substep and relabel, read back once by tq_get_timing.
@@ -362,6 +364,7 @@ int tq_destroy(tq_sim* s) {
   destruirRastreador(s->ar);
   for (void* p : s->alocados) cudaFree(p);
   if (s->staging) cudaFree(s->staging);
+  if (s->mancha) cudaFree(s->mancha);
   for (auto& e : s->pool) cudaEventDestroy(e);
   if (s->s) cudaStreamDestroy(s->s);
   delete s;
@@ -373,6 +376,43 @@ int tq_set_walls(tq_sim* s, const float* sdf, int32_t mw, int32_t mh) {
   if (mw != s->mw || mh != s->mh) return falha(TQ_E_ARG, "sdf must be (2*nx) x (2*ny)");
   CK(cudaMemcpyAsync((void*)s->d.sdf, sdf, (size_t)mw * mh * 4, cudaMemcpyHostToDevice, s->s));
   lancarSolidos(s->d, s->s);
+  CK(cudaStreamSynchronize(s->s));
+  return TQ_OK;
+}
+
+int tq_trace_wall(tq_sim* s, double x0, double y0, double x1, double y1, double radius, int32_t erase) {
+  if (!s) return falha(TQ_E_ARG, "null handle");
+  if (!std::isfinite(x0) || !std::isfinite(y0) || !std::isfinite(x1) || !std::isfinite(y1) || !std::isfinite(radius))
+    return falha(TQ_E_ARG, "non-finite wall segment");
+  lancarTracar(s->d, x0, y0, x1, y1, radius, erase != 0, s->s);
+  lancarSolidos(s->d, s->s);
+  CK(cudaStreamSynchronize(s->s));
+  return TQ_OK;
+}
+
+int tq_clear_walls(tq_sim* s) {
+  if (!s) return falha(TQ_E_ARG, "null handle");
+  lancarZerarMascara(s->d, s->s);
+  lancarSolidos(s->d, s->s);
+  CK(cudaStreamSynchronize(s->s));
+  return TQ_OK;
+}
+
+int tq_splat(tq_sim* s, int32_t w, int32_t h, float* out) {
+  if (!s || !out) return falha(TQ_E_ARG, "null argument");
+  if (w < 1 || h < 1 || (long long)w * h > (1LL << 26)) return falha(TQ_E_ARG, "target must be 1..2^26 pixels");
+  const size_t total = (size_t)5 * w * h;
+  if (total > s->manchaCap) {
+    if (s->mancha) cudaFree(s->mancha);
+    s->mancha = nullptr;
+    s->manchaCap = 0;
+    CK(cudaMalloc(&s->mancha, total * sizeof(unsigned long long)));
+    s->manchaCap = total;
+  }
+  int n = 0;
+  int st = lerContagem(s, &n);
+  if (st) return st;
+  lancarMancha(s->d, n, w, h, s->mancha, out, s->s);
   CK(cudaStreamSynchronize(s->s));
   return TQ_OK;
 }

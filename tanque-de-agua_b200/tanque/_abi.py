@@ -105,6 +105,9 @@ SO_PRODUTO = {
     "get_timing": (C.c_int, [_P, C.POINTER(_D), _I, C.POINTER(_I)]),
     "options_default": (None, [C.POINTER(TqOptions), _I, _I, _D]),
     "status_string": (C.c_char_p, [C.c_int]),
+    "trace_wall": (C.c_int, [_P, _D, _D, _D, _D, _D, _I]),
+    "clear_walls": (C.c_int, [_P]),
+    "splat": (C.c_int, [_P, _I, _I, _P]),
     "last_error": (C.c_char_p, []),
 }
 

@@ -223,6 +223,27 @@ class SimulacaoGPU(Simulacao):
     def sincronizar(self):
         self._lig("sync", self._h)
 
+    def tracarParede(self, x0, y0, x1, y1, raio, apagar: bool = False):
+        """Cena.tracar (js/cena.js:43-72) + atualizarParedes on the device mask (tq_trace_wall).
+        The handle's mask then differs from self.cena's until the scene draws the same segment."""
+        self._lig("trace_wall", self._h, float(x0), float(y0), float(x1), float(y1), float(raio), 1 if apagar else 0)
+
+    def limparParedes(self):
+        """Cena.limpar (js/cena.js:74-77) + atualizarParedes on the device (tq_clear_walls)."""
+        self._lig("clear_walls", self._h)
+
+    def mancha(self, largura: int, altura: int, saida=None):
+        """The renderer's particle splat (WGSL_MANCHA, tq_splat) as a (5, altura, largura) array:
+        sum of weights, weight x foam, weight x the three absorptions; row 0 at the top.  With
+        `saida` (a CUDA torch tensor of 5 * largura * altura float32) the image stays on the
+        device and `saida` is returned."""
+        import torch
+        buf = saida if saida is not None else torch.empty(5 * largura * altura, dtype=torch.float32, device="cuda")
+        if buf.dtype != torch.float32 or not buf.is_cuda or buf.numel() != 5 * largura * altura:
+            raise ValueError("saida must be a CUDA float32 tensor of 5 * largura * altura elements")
+        self._lig("splat", self._h, largura, altura, buf.data_ptr())
+        return buf if saida is not None else buf.cpu().numpy().reshape(5, altura, largura)
+
     ETAPAS = ["p2g", "tipos_rotulos", "superficie", "divergencia_bolhas", "pressao", "gradiente_extrapolacao", "g2p"]
 
     def tempos(self, ligar: bool | None = None):

@@ -33,6 +33,7 @@ ASSINATURAS_ORACULO.update({
     "scene_solid_cell": (_I, [_P, _I, _I]),
     "passo_maximo": (_D, [_D, _D, _D, _I, _D]),
     "semear_retangulo": (_I, [_D, _D, _D, _D, _D, C.POINTER(_D), C.POINTER(C.c_uint32), _P, _I]),
+    "splat": (None, [_P, _I, _I, _I, _D, _I, _I, _P]),
 })
 
 
@@ -56,7 +57,7 @@ def carregar_oraculo() -> _abi.Ligacao:
         lib = C.CDLL(SO)
         lig = _abi.Ligacao(lib, "tqo_", ASSINATURAS_ORACULO)
         for nome in ["scene_new", "scene_free", "scene_trace", "scene_clear", "scene_sdf", "scene_distance",
-                     "scene_normal", "scene_solid_cell", "passo_maximo", "semear_retangulo"]:
+                     "scene_normal", "scene_solid_cell", "passo_maximo", "semear_retangulo", "splat"]:
             fn = getattr(lib, "tqo_" + nome)
             fn.restype, fn.argtypes = ASSINATURAS_ORACULO[nome]
         lig.cru = _Crua(lib)
@@ -117,6 +118,14 @@ class SimulacaoOraculo(Simulacao):
         opcoes = dict(opcoes or {})
         opcoes.setdefault("p2g_mode", _abi.TQ_P2G_FLOAT)
         super().__init__(carregar_oraculo(), cena, opcoes, criar="create_fp64" if fp64 else "create")
+
+
+def mancha_oraculo(particulas, nx, ny, h, largura, altura):
+    """tqo_splat: the oracle's splat of a particle list (rows of 12 floats), (5, altura, largura)."""
+    p = np.ascontiguousarray(particulas, dtype=np.float32).ravel()
+    out = np.zeros(5 * largura * altura, dtype=np.float32)
+    carregar_oraculo().cru.splat(p.ctypes.data, p.size // 12, nx, ny, h, largura, altura, out.ctypes.data)
+    return out.reshape(5, altura, largura)
 
 
 def resolver_pressao_oraculo(tipo, div, q, iteracoes=3, tolerancia=0.0, bolhas=None):
