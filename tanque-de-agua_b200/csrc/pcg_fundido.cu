@@ -19,6 +19,7 @@
 // redundantly by every CTA after the barrier, so all CTAs hold the same bits without another
 // barrier; per-bubble sums are 64-bit fixed point as in the plain engine.
 #include <cstdio>
+#include <cstdlib>
 #include <type_traits>
 
 #include "common.cuh"
@@ -68,8 +69,16 @@ struct NivelF {
   void *b, *x, *tmp;
 };
 
+// Blocks of a level for a smoother pass with shift `desl`.
+__host__ __device__ __forceinline__ int blocosNivel(int nx, int ny, int desl) {
+  return ((nx + desl + 15) >> 4) * ((ny + desl + 15) >> 4);
+}
+
 struct Fundido {
   int G = 0, Lc = 0;
+  uint8_t* solidos = nullptr;  // wall-block flags (Args::sol) of the levels that use them
+  bool comParedes[MAX_NIVEIS] = {};  // level l skips wall blocks (its flags exist)
+  uint8_t* sol[MAX_NIVEIS] = {};      // level l's flags in `solidos` (Args::sol)
   size_t smem = 0;
   NivelF* niveis = nullptr;  // level table (device)
   double* parc = nullptr;
@@ -120,6 +129,9 @@ struct Args {
   // bubble), 12-23 / 24-35 / 36-47 / 48-59 its left / right / down / up neighbour's (0: none)
   unsigned long long* rotB;
   unsigned long long* perfil;  // [0] count, [1..] %globaltimer at each barrier (null: off)
+  // per level: 1 per 16x16 block whose cells are all wall (out-of-grid cells count as wall), the
+  // blocks of shift 0 then those of shift 8; null where the level does not skip wall blocks
+  uint8_t* sol[MAX_NIVEIS];
 };
 
 // The level table, copied into shared memory at kernel start: every phase reads its level's
@@ -638,9 +650,24 @@ __device__ __noinline__ void faseSuavizarT(const Args& a, int l, int desl, int o
   // blocks of the row-major order, the top rows: air above the water in a tank, whose blocks
   // skip their sweeps, so the pass lasts about one water block
   const int tot = WARPS * gridDim.x, exc = nb - tot;
-  for (int t = w * gridDim.x + blockIdx.x; t < nb; t += tot) {
-    const int blk = exc > 0 ? nb - 1 - (t + exc) % nb : t;
-    suavizarBloco<T, MODO>(a, n, blk, nbx, desl, ordem, src, dst, area, g, xcSecao, ru, s0, s1);
+  const int tw = w * gridDim.x + blockIdx.x;  // the warp's first block index
+  auto blocoDe = [&](int t) { return exc > 0 ? nb - 1 - (t + exc) % nb : t; };
+  if (a.sol[l]) {
+    // Blocks of wall alone are skipped: their cells hold x = 0 in both snapshots (zeroed before
+    // the solve, and a pass writes 0 off water) and b = 0, so a pass would rewrite the same
+    // zeros.  The flags of the warp's first 32 blocks come in one load, lane k's for its k-th.
+    const uint8_t* fl = a.sol[l] + (desl ? blocosNivel(n.nx, n.ny, 0) : 0);
+    const int tk = tw + (threadIdx.x & 31) * tot;
+    const unsigned paredes = __ballot_sync(0xffffffffu, tk < nb && ldcg8(fl + blocoDe(tk)) != 0);
+    int k = 0;
+    for (int t = tw; t < nb; t += tot, k++) {
+      const int blk = blocoDe(t);
+      if (k < 32 ? (paredes >> k) & 1u : ldcg8(fl + blk) != 0) continue;
+      suavizarBloco<T, MODO>(a, n, blk, nbx, desl, ordem, src, dst, area, g, xcSecao, ru, s0, s1);
+    }
+  } else {
+    for (int t = tw; t < nb; t += tot)
+      suavizarBloco<T, MODO>(a, n, blocoDe(t), nbx, desl, ordem, src, dst, area, g, xcSecao, ru, s0, s1);
   }
   if (MODO == M_JUNTAR) {
     const double t0 = somaBloco(s0, sh);
@@ -694,7 +721,24 @@ __device__ __forceinline__ void faseRestringirR(const Args& a, int l, float* are
   const float pes[4] = {0.25f, 0.75f, 0.75f, 0.25f};
   const int nseg = (g.nx + 31) >> 5;
   const int total = nseg * ((g.ny + R - 1) / R);
-  for (int seg = w * gridDim.x + blockIdx.x; seg < total; seg += WARPS * gridDim.x) {
+  // A region whose coarse cells lie in wall blocks of the coarse level (its shift-0 flags; its
+  // 32 columns span two blocks, its rows one) is skipped: those cells keep b = 0.  The flags of
+  // the warp's first 32 regions come in one load, lane k's for its k-th.
+  const uint8_t* flg = a.sol[l + 1];
+  const int gbx = (g.nx + 15) >> 4;
+  auto paredeReg = [&](int seg) {
+    const int by = ((seg / nseg) * R) >> 4, bx = ((seg % nseg) * 32) >> 4;
+    return ldcg8(flg + by * gbx + bx) != 0 && (bx + 1 >= gbx || ldcg8(flg + by * gbx + bx + 1) != 0);
+  };
+  const int t0 = w * gridDim.x + blockIdx.x, tot = WARPS * gridDim.x;
+  unsigned paredes = 0;
+  if (flg) {
+    const int tk = t0 + lane * tot;
+    paredes = __ballot_sync(0xffffffffu, tk < total && paredeReg(tk));
+  }
+  int kr = 0;
+  for (int seg = t0; seg < total; seg += tot, kr++) {
+    if (flg && (kr < 32 ? (paredes >> kr) & 1u : paredeReg(seg))) continue;
     const int J0 = (seg / nseg) * R, I0 = (seg % nseg) * 32;
     const int fi0 = 2 * I0 - 2, fj0 = 2 * J0 - 2;  // x window origin (fine)
     const int I = I0 + lane;
@@ -1364,6 +1408,31 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
   if (threadIdx.x == 0) a.parc[blockIdx.x * NPARC + 0] = tb;
 }
 
+// The wall-block flags of the levels that have them (Args::sol), both shifts: one warp per
+// block, 8 cells a lane; a block is wall when every cell of it in the grid is.
+__device__ __noinline__ void marcarParedes(const Args& a) {
+  const int lane = threadIdx.x & 31, wg = (threadIdx.x >> 5) * gridDim.x + blockIdx.x, nw = WARPS * gridDim.x;
+  for (int l = 0; l < a.Lc; l++) {
+    const NivelF n = s_niv[l];
+    if (!a.sol[l]) continue;
+    for (int desl = 0; desl <= 8; desl += 8) {
+      const int nbx = (n.nx + desl + 15) >> 4, nb = blocosNivel(n.nx, n.ny, desl);
+      uint8_t* fl = a.sol[l] + (desl ? blocosNivel(n.nx, n.ny, 0) : 0);
+      for (int blk = wg; blk < nb; blk += nw) {
+        const int ox = (blk % nbx) * 16 - desl, oy = (blk / nbx) * 16 - desl;
+        const int gy = oy + (lane >> 1), gx0 = ox + (lane & 1) * 8;
+        bool parede = true;
+        for (int k = 0; k < 8; k++) {
+          const int gx = gx0 + k;
+          if (gx >= 0 && gy >= 0 && gx < n.nx && gy < n.ny) parede &= ldcg8(n.tipo + gx + gy * n.nx) == SOLIDO;
+        }
+        const bool todos = __all_sync(0xffffffffu, parede);
+        if (lane == 0) fl[blk] = todos ? 1 : 0;
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- the kernel
 template <class T>
 __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a) {
@@ -1439,6 +1508,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       n.viz[c] = (uint8_t)m;
     }
   }
+  marcarParedes(a);
   for (int c = gt0; c < N; c += GT) {  // the operator descriptor (bubble faces are complete)
     const int i = c % nx, j = c / nx;
     const int t = d.tipo[c];
@@ -1777,6 +1847,19 @@ Fundido* criarFundido(Pcg* p) {
          cudaMalloc(&f->z2, N * 4) == cudaSuccess && cudaMalloc(&f->xc, nLc * 4) == cudaSuccess &&
          cudaMalloc(&f->bc, nLc * 4) == cudaSuccess && cudaMalloc(&f->op, N * sizeof(uint16_t)) == cudaSuccess &&
          cudaMalloc(&f->rotB, N * sizeof(unsigned long long)) == cudaSuccess;
+    // Wall blocks are skipped on levels of at least two full rounds of the grid's warps (a
+    // tank atlas's finest levels): there the flags' one extra load per warp and pass is paid
+    // back; a level of one round (the 450k-cell scene's) keeps no flags.
+    // TQ_WALL_SKIP_MIN_BLOCKS in the environment (read when the handle is created) sets the
+    // threshold in blocks; the tests use 1 to skip on every grid level and 0x7fffffff for none.
+    long long limiar = 2LL * WARPS * f->G;
+    if (const char* e = getenv("TQ_WALL_SKIP_MIN_BLOCKS")) limiar = atoll(e);
+    size_t nFlags = 0;
+    for (int l = 0; l < Lc; l++) {
+      f->comParedes[l] = blocosNivel(p->nxL[l], p->nyL[l], 0) >= limiar;
+      if (f->comParedes[l]) nFlags += blocosNivel(p->nxL[l], p->nyL[l], 0) + blocosNivel(p->nxL[l], p->nyL[l], 8);
+    }
+    ok = ok && (nFlags == 0 || cudaMalloc(&f->solidos, nFlags) == cudaSuccess);
     if (ok && f->secaoDensa)
       ok = cudaMalloc(&f->mSecao, nLc * nLc * 4) == cudaSuccess && cudaMalloc(&f->wSecao, nLc * 4) == cudaSuccess &&
            cudaMalloc(&f->wInv, nLc * 4) == cudaSuccess && cudaMalloc(&f->nW, 4) == cudaSuccess &&
@@ -1795,6 +1878,12 @@ Fundido* criarFundido(Pcg* p) {
       n.x = p->xL[l];
       n.tmp = p->tmpL[l];
     }
+    size_t off = 0;
+    for (int l = 0; l < Lc; l++) {
+      if (!f->comParedes[l]) continue;
+      f->sol[l] = f->solidos + off;
+      off += blocosNivel(p->nxL[l], p->nyL[l], 0) + blocosNivel(p->nxL[l], p->nyL[l], 8);
+    }
     ok = cudaMemcpy(f->niveis, tab, sizeof tab, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemset(f->bar, 0, 2 * sizeof(unsigned)) == cudaSuccess && cudaMemset(f->erro, 0, sizeof(int)) == cudaSuccess;
   }
@@ -1810,7 +1899,7 @@ void destruirFundido(Fundido* f) {
   if (!f) return;
   void* ps[] = {f->niveis, f->parc, f->bar, f->erro, f->accZ, f->zb2, f->pb2, f->ativos,
                 f->nAtivos, f->p2, f->z2, f->xc, f->bc, f->perfil, f->op, f->rotB, f->mSecao, f->wSecao, f->wInv, f->nW,
-                f->densoG};
+                f->densoG, f->solidos};
   for (void* q : ps)
     if (q) cudaFree(q);
   delete f;
@@ -1838,6 +1927,7 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   a.nAtivos = f->nAtivos;
   a.p2 = f->p2;
   a.z2 = f->z2;
+  for (int l = 0; l < MAX_NIVEIS; l++) a.sol[l] = f->sol[l];
   a.xc = f->xc;
   a.bc = f->bc;
   a.offDenso = f->offDenso;
@@ -1859,6 +1949,19 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
   cudaMemsetAsync(f->bar, 0, 2 * sizeof(unsigned), s);
   cudaMemsetAsync(f->erro, 0, sizeof(int), s);
+  // The levels that skip wall blocks start the solve with their snapshots and right side at 0,
+  // and with level 0 so do both z vectors (a pass never writes anything else off water).
+  for (int l = 0; l < f->Lc; l++) {
+    if (!f->comParedes[l]) continue;
+    const size_t bytes = (size_t)p->nxL[l] * p->nyL[l] * (p->meia[l] ? 2 : 4);
+    cudaMemsetAsync(p->xL[l], 0, bytes, s);
+    cudaMemsetAsync(p->tmpL[l], 0, bytes, s);
+    cudaMemsetAsync(p->bL[l], 0, bytes, s);
+  }
+  if (f->comParedes[0]) {
+    cudaMemsetAsync(d.z, 0, (size_t)d.N * 4, s);
+    cudaMemsetAsync(f->z2, 0, (size_t)d.N * 4, s);
+  }
   void* args[] = {&a};
   contarLancamento();
   cudaError_t e = cudaLaunchCooperativeKernel(f->kern, dim3(f->G), dim3(TF), args, f->smem, s);

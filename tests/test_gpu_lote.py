@@ -1,6 +1,8 @@
 """Batched tanks on the GPU: atlases (tanque.lote) against the oracle on the same atlas, for the
-FP32 plain engine and the FP16 fused one: 8 tanks, and 12 wide flat ones whose coarsest
-multigrid level is large enough for the coarsest sweeps to run on a whole CTA.
+FP32 plain engine and the FP16 fused one (also with its skipping of wall blocks forced on every
+level): 8 tanks, and 12 wide flat ones whose coarsest multigrid level is large enough for the
+coarsest sweeps to run on a whole CTA.  Skipping wall blocks must not change a bit of the
+fused solve.
 
 From the same state, one air relabel and two substeps, every pressure solve to
 ||r|| <= 1e-6 ||r0||: integers bit for bit (particle-to-grid sums, flags, counts, air labels,
@@ -20,7 +22,12 @@ pytestmark = pytest.mark.gpu
 H = 1 / 128
 SOLVE = {"tolerance": 1e-6, "iterations": 200}
 MOTORES = [pytest.param({"precision": _abi.TQ_PREC_FP32, "engine": _abi.TQ_ENGINE_PLAIN}, id="fp32-plain"),
-           pytest.param({"precision": _abi.TQ_PREC_FP16, "engine": _abi.TQ_ENGINE_FUSED}, id="fp16-fused")]
+           pytest.param({"precision": _abi.TQ_PREC_FP16, "engine": _abi.TQ_ENGINE_FUSED}, id="fp16-fused"),
+           pytest.param({"precision": _abi.TQ_PREC_FP16, "engine": _abi.TQ_ENGINE_FUSED, "paredes": True},
+                        id="fp16-fused-pulando-paredes")]
+# The fused engine skips blocks of wall alone on levels of at least two rounds of its warps;
+# a threshold of 1 block (read when a handle is created) makes every grid level skip them.
+LIMIAR = "TQ_WALL_SKIP_MIN_BLOCKS"
 
 
 def _tanques():
@@ -35,7 +42,10 @@ def _largos():
 
 @pytest.mark.parametrize("tanques", [_tanques, _largos], ids=["8-tanques", "largo"])
 @pytest.mark.parametrize("opcoes", MOTORES)
-def test_atlas_contra_o_oraculo(lib_gpu, opcoes, tanques):
+def test_atlas_contra_o_oraculo(lib_gpu, opcoes, tanques, monkeypatch):
+    opcoes = dict(opcoes)
+    if opcoes.pop("paredes", False):
+        monkeypatch.setenv(LIMIAR, "1")
     at = montar_atlas(Cena, tanques(), H)
     o = SimulacaoOraculo(at["cena"], dict(SOLVE, p2g_mode=_abi.TQ_P2G_FIXED))
     g = SimulacaoGPU(at["cena"], dict(SOLVE, **opcoes))
@@ -53,6 +63,27 @@ def test_atlas_contra_o_oraculo(lib_gpu, opcoes, tanques):
         g.avancar(1 / 240, 1)
         comparar_passo(o, g, f"substep {quadro}")
     g.fechar()
+
+
+def test_pular_paredes_nao_muda_nada(lib_gpu, monkeypatch):
+    """Skipping wall blocks rewrites no value a pass would have written (their cells stay 0),
+    so the fused solve gives the same bits with and without it."""
+    at = montar_atlas(Cena, _largos(), H)
+    sims = []
+    for limiar in ["1", "2147483647"]:
+        monkeypatch.setenv(LIMIAR, limiar)
+        g = SimulacaoGPU(at["cena"], dict(SOLVE, precision=_abi.TQ_PREC_FP16, engine=_abi.TQ_ENGINE_FUSED))
+        g.adicionar(at["particulas"], False)
+        sims.append(g)
+    for _ in range(2):
+        for g in sims:
+            g.avancar(1 / 240, 2)
+        for campo in ["q", "u", "v", "rotulo"]:
+            a, b = sims[0].campo(campo), sims[1].campo(campo)
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), campo
+        assert np.array_equal(sims[0].p.view(np.uint32), sims[1].p.view(np.uint32))
+    for g in sims:
+        g.fechar()
 
 
 def test_lote_no_gpu(lib_gpu):
