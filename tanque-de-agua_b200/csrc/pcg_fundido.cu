@@ -465,14 +465,31 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   float cv[4];
   int cz[4];
   if (PROL) {
+    int C[4];
+    bool ok[4];
 #pragma unroll
     for (int kk = 0; kk < 4; kk++) {
       const int s = lane + 32 * kk;
       const int I = cx0 + s % 11, J = cy0 + s / 11;
-      const bool ok = s < CT && I >= 0 && J >= 0 && I < g.nx && J < g.ny;
-      const int C = ok ? I + J * g.nx : 0;
-      cz[kk] = ok ? ldcg8(g.viz + C) : 0;
-      cv[kk] = ok ? (xcSecao ? __ldcg(xcSecao + C) : lerN(g.meia, g.x, C)) : 0.0f;
+      ok[kk] = s < CT && I >= 0 && J >= 0 && I < g.nx && J < g.ny;
+      C[kk] = ok[kk] ? I + J * g.nx : 0;
+      cz[kk] = ok[kk] ? ldcg8(g.viz + C[kk]) : 0;
+    }
+    // the coarse values' storage type is chosen once (warp-uniform), so the four loads are
+    // straight-line code in flight together
+    if (xcSecao) {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) cv[kk] = ok[kk] ? __ldcg(xcSecao + C[kk]) : 0.0f;
+    } else if (g.meia == 1) {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) cv[kk] = ok[kk] ? __half2float(ldcg((const __half*)g.x + C[kk])) : 0.0f;
+    } else if (g.meia == 2) {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++)
+        cv[kk] = ok[kk] ? __bfloat162float(ldcg((const __nv_bfloat16*)g.x + C[kk])) : 0.0f;
+    } else {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) cv[kk] = ok[kk] ? __ldcg((const float*)g.x + C[kk]) : 0.0f;
     }
   }
   float x[2][4], bq[2][4];  // [colour][m], see meiaReg
@@ -579,16 +596,38 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     const float inv = 1.0f / ru.escala;
     float rv[2][4], zv[2][4];
     int lb[2][4];
+    // the warp-uniform tests (bubbles, a previous z) outside the loads, so each group of loads
+    // is straight-line code in flight together
 #pragma unroll
     for (int cr = 0; cr < 2; cr++)
 #pragma unroll
       for (int m = 0; m < 4; m++) {
         const int c = cel[cr][m] < 0 ? 0 : cel[cr][m];
         om[cr][m] = cel[cr][m] < 0 ? 0 : __ldcg(a.op + c);
-        lb[cr][m] = (a.bolhas && cel[cr][m] >= 0) ? (int)(__ldcg(a.rotB + c) & 0xfff) : 0;
         rv[cr][m] = __ldcg(a.d.r + c);
-        zv[cr][m] = ru.zVelho ? __ldcg(ru.zVelho + c) : 0.0f;
       }
+    if (a.bolhas) {
+#pragma unroll
+      for (int cr = 0; cr < 2; cr++)
+#pragma unroll
+        for (int m = 0; m < 4; m++) lb[cr][m] = cel[cr][m] >= 0 ? (int)(__ldcg(a.rotB + cel[cr][m]) & 0xfff) : 0;
+    } else {
+#pragma unroll
+      for (int cr = 0; cr < 2; cr++)
+#pragma unroll
+        for (int m = 0; m < 4; m++) lb[cr][m] = 0;
+    }
+    if (ru.zVelho) {
+#pragma unroll
+      for (int cr = 0; cr < 2; cr++)
+#pragma unroll
+        for (int m = 0; m < 4; m++) zv[cr][m] = __ldcg(ru.zVelho + (cel[cr][m] < 0 ? 0 : cel[cr][m]));
+    } else {
+#pragma unroll
+      for (int cr = 0; cr < 2; cr++)
+#pragma unroll
+        for (int m = 0; m < 4; m++) zv[cr][m] = 0.0f;
+    }
     unsigned cels[2][4];
 #pragma unroll
     for (int cr = 0; cr < 2; cr++)
