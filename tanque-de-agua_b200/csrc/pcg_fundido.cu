@@ -181,11 +181,6 @@ __device__ __forceinline__ __nv_bfloat16 ldcg<__nv_bfloat16>(const __nv_bfloat16
 }
 __device__ __forceinline__ int ldcg8(const uint8_t* p) { return (int)__ldcg((const unsigned char*)p); }
 
-__device__ __forceinline__ float lerN(int meia, const void* v, int c) {
-  return meia == 0 ? __ldcg((const float*)v + c)
-                   : (meia == 1 ? __half2float(ldcg((const __half*)v + c))
-                                : __bfloat162float(ldcg((const __nv_bfloat16*)v + c)));
-}
 __device__ __forceinline__ void gravarN(int meia, void* v, int c, float x) {
   if (meia == 0) ((float*)v)[c] = x;
   else if (meia == 1) ((__half*)v)[c] = __float2half_rn(x);
