@@ -517,10 +517,16 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     const bool okR = k == 7 && gxR < nx && gy >= 0 && gy < ny;
     f.esq[m] = (!ZERO && okL) ? carregar(ldcg(src + gxL + gy * nx)) : 0.0f;
     f.dir[m] = (!ZERO && okR) ? carregar(ldcg(src + gxR + gy * nx)) : 0.0f;
-    if (PROL) {
-      aguaF |= (unsigned)((okL ? ldcg8(n.viz + gxL + gy * nx) : 0) >> 4 & 1) << m;
-      aguaF |= (unsigned)((okR ? ldcg8(n.viz + gxR + gy * nx) : 0) >> 4 & 1) << (4 + m);
-    }
+  }
+  // PROL: the frame's water flags, two cells a lane (lane i: the left (i < 16) or right column's
+  // row i & 15, and the bottom (i < 16) or top row's column i & 15), gathered by ballot below
+  int vzLR = 0, vzBT = 0;
+  if (PROL) {
+    const int fr = lane & 15;
+    const int gxA = lane < 16 ? ox - 1 : ox + 16, gyA = oy + fr;
+    const int gxB = ox + fr, gyB = lane < 16 ? oy - 1 : oy + 16;
+    vzLR = (gxA >= 0 && gxA < nx && gyA >= 0 && gyA < ny) ? ldcg8(n.viz + gxA + gyA * nx) : 0;
+    vzBT = (gxB >= 0 && gxB < nx && gyB >= 0 && gyB < ny) ? ldcg8(n.viz + gxB + gyB * nx) : 0;
   }
 #pragma unroll
   for (int j = 0; j < 2; j++) {
@@ -530,10 +536,6 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     const bool okT = gl == 3 && gx >= 0 && gx < nx && gyT < ny;
     f.bai[j] = (!ZERO && okB) ? carregar(ldcg(src + gx + gyB * nx)) : 0.0f;
     f.cim[j] = (!ZERO && okT) ? carregar(ldcg(src + gx + gyT * nx)) : 0.0f;
-    if (PROL) {
-      aguaF |= (unsigned)((okB ? ldcg8(n.viz + gx + gyB * nx) : 0) >> 4 & 1) << (8 + j);
-      aguaF |= (unsigned)((okT ? ldcg8(n.viz + gx + gyT * nx) : 0) >> 4 & 1) << (10 + j);
-    }
   }
   if (MODO == M_ESPALHAR) {
     // cells of active bubbles take their bubble's mean residual; b is stored in the storage
@@ -551,6 +553,14 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
       }
   }
   if (PROL) {
+    // the frame's water flags of this lane's frame cells: bits 0-3 left rows 4g..4g+3 (k = 0),
+    // 4-7 right (k = 7), 8-9 below columns 2k, 2k+1 (g = 0), 10-11 above (g = 3)
+    const unsigned mLR = __ballot_sync(0xffffffffu, (vzLR & 16) != 0);
+    const unsigned mBT = __ballot_sync(0xffffffffu, (vzBT & 16) != 0);
+    if (k == 0) aguaF |= (mLR >> (4 * gl)) & 0xFu;
+    if (k == 7) aguaF |= ((mLR >> (16 + 4 * gl)) & 0xFu) << 4;
+    if (gl == 0) aguaF |= ((mBT >> (2 * k)) & 3u) << 8;
+    if (gl == 3) aguaF |= ((mBT >> (16 + 2 * k)) & 3u) << 10;
     // coarse tile: columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11, water x or 0; the
     // snapshot of every fine water cell, frame included, is x + P(x_coarse)
     float* ct = area;
