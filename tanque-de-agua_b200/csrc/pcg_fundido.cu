@@ -509,33 +509,34 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
         bq[cr][m] = dentro ? carregar(ldcg(b + c)) : 0.0f;
       }
     }
-#pragma unroll
-  for (int m = 0; m < 4; m++) {
-    const int gy = oy + 4 * gl + m;
-    const int gxL = ox - 1, gxR = ox + 16;
-    const bool okL = k == 0 && gxL >= 0 && gy >= 0 && gy < ny;
-    const bool okR = k == 7 && gxR < nx && gy >= 0 && gy < ny;
-    f.esq[m] = (!ZERO && okL) ? carregar(ldcg(src + gxL + gy * nx)) : 0.0f;
-    f.dir[m] = (!ZERO && okR) ? carregar(ldcg(src + gxR + gy * nx)) : 0.0f;
-  }
-  // PROL: the frame's water flags, two cells a lane (lane i: the left (i < 16) or right column's
-  // row i & 15, and the bottom (i < 16) or top row's column i & 15), gathered by ballot below
+  // The block's frame: lane i loads the left (i < 16) or right column's row i & 15 and the
+  // bottom (i < 16) or top row's column i & 15; the lanes next to the frame (k = 0 / 7 for the
+  // columns, g = 0 / 3 for the rows) take their values by shuffle.  With PROL the same two cells'
+  // water flags come along (gathered by ballot below).
   int vzLR = 0, vzBT = 0;
-  if (PROL) {
+  {
     const int fr = lane & 15;
     const int gxA = lane < 16 ? ox - 1 : ox + 16, gyA = oy + fr;
     const int gxB = ox + fr, gyB = lane < 16 ? oy - 1 : oy + 16;
-    vzLR = (gxA >= 0 && gxA < nx && gyA >= 0 && gyA < ny) ? ldcg8(n.viz + gxA + gyA * nx) : 0;
-    vzBT = (gxB >= 0 && gxB < nx && gyB >= 0 && gyB < ny) ? ldcg8(n.viz + gxB + gyB * nx) : 0;
-  }
+    const bool okA = gxA >= 0 && gxA < nx && gyA >= 0 && gyA < ny;
+    const bool okB = gxB >= 0 && gxB < nx && gyB >= 0 && gyB < ny;
+    if (PROL) {
+      vzLR = okA ? ldcg8(n.viz + gxA + gyA * nx) : 0;
+      vzBT = okB ? ldcg8(n.viz + gxB + gyB * nx) : 0;
+    }
+    if (ZERO) {
 #pragma unroll
-  for (int j = 0; j < 2; j++) {
-    const int gx = ox + 2 * k + j;
-    const int gyB = oy - 1, gyT = oy + 16;
-    const bool okB = gl == 0 && gx >= 0 && gx < nx && gyB >= 0;
-    const bool okT = gl == 3 && gx >= 0 && gx < nx && gyT < ny;
-    f.bai[j] = (!ZERO && okB) ? carregar(ldcg(src + gx + gyB * nx)) : 0.0f;
-    f.cim[j] = (!ZERO && okT) ? carregar(ldcg(src + gx + gyT * nx)) : 0.0f;
+      for (int m = 0; m < 4; m++) f.esq[m] = f.dir[m] = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 2; j++) f.bai[j] = f.cim[j] = 0.0f;
+    } else {
+      const float xA = okA ? carregar(ldcg(src + gxA + gyA * nx)) : 0.0f;
+      const float xB = okB ? carregar(ldcg(src + gxB + gyB * nx)) : 0.0f;
+#pragma unroll
+      for (int m = 0; m < 4; m++) f.esq[m] = f.dir[m] = __shfl_sync(0xffffffffu, xA, (k == 7 ? 16 : 0) + 4 * gl + m);
+#pragma unroll
+      for (int j = 0; j < 2; j++) f.bai[j] = f.cim[j] = __shfl_sync(0xffffffffu, xB, (gl == 3 ? 16 : 0) + 2 * k + j);
+    }
   }
   if (MODO == M_ESPALHAR) {
     // cells of active bubbles take their bubble's mean residual; b is stored in the storage
