@@ -612,11 +612,12 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
         om[cr][m] = cel[cr][m] < 0 ? 0 : __ldcg(a.op + c);
         rv[cr][m] = __ldcg(a.d.r + c);
       }
-    if (a.bolhas) {
+    if (a.bolhas) {  // a cell's own label is set only on bubble air (OP_BOLHA): load it there alone
 #pragma unroll
       for (int cr = 0; cr < 2; cr++)
 #pragma unroll
-        for (int m = 0; m < 4; m++) lb[cr][m] = cel[cr][m] >= 0 ? (int)(__ldcg(a.rotB + cel[cr][m]) & 0xfff) : 0;
+        for (int m = 0; m < 4; m++)
+          lb[cr][m] = (om[cr][m] & OP_BOLHA) ? (int)(__ldcg(a.rotB + cel[cr][m]) & 0xfff) : 0;
     } else {
 #pragma unroll
       for (int cr = 0; cr < 2; cr++)
