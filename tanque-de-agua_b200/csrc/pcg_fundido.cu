@@ -455,10 +455,11 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   const int nx = n.nx, ny = n.ny;
   const T* b = (const T*)n.b;
   // PROL: the coarse tile (columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11) is loaded first,
-  // so that every load of the block is in flight before any result is used
+  // so that every load of the block is in flight before any result is used.  Coarse x is 0 off
+  // water (a grid level's snapshot, or the section's output, zeroed before the solve off water),
+  // so the tile needs no water flags.
   const int cx0 = (ox - 2) >> 1, cy0 = (oy - 2) >> 1;
   float cv[4];
-  int cz[4];
   if (PROL) {
     int C[4];
     bool ok[4];
@@ -468,7 +469,6 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
       const int I = cx0 + s % 11, J = cy0 + s / 11;
       ok[kk] = s < CT && I >= 0 && J >= 0 && I < g.nx && J < g.ny;
       C[kk] = ok[kk] ? I + J * g.nx : 0;
-      cz[kk] = ok[kk] ? ldcg8(g.viz + C[kk]) : 0;
     }
     // the coarse values' storage type is chosen once (warp-uniform), so the four loads are
     // straight-line code in flight together
@@ -562,13 +562,13 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
     if (k == 7) aguaF |= ((mLR >> (16 + 4 * gl)) & 0xFu) << 4;
     if (gl == 0) aguaF |= ((mBT >> (2 * k)) & 3u) << 8;
     if (gl == 3) aguaF |= ((mBT >> (16 + 2 * k)) & 3u) << 10;
-    // coarse tile: columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11, water x or 0; the
-    // snapshot of every fine water cell, frame included, is x + P(x_coarse)
+    // coarse tile: columns from (ox-2)>>1, rows from (oy-2)>>1, 11x11 (x, 0 off water and off
+    // the grid); the snapshot of every fine water cell, frame included, is x + P(x_coarse)
     float* ct = area;
 #pragma unroll
     for (int kk = 0; kk < 4; kk++) {
       const int s = lane + 32 * kk;
-      if (s < CT) ct[s] = (cz[kk] & 16) ? cv[kk] : 0.0f;
+      if (s < CT) ct[s] = cv[kk];
     }
     __syncwarp();
 #pragma unroll
