@@ -329,6 +329,8 @@ __device__ __forceinline__ bool bolhaAtiva(const Args& a, uint32_t r) {
 // air of an active bubble; OP_BOLHA air of an active bubble; bits 8-10 the number of free
 // (non-wall) neighbours.
 constexpr int OP_AGUA = 16, OP_FACE = 32, OP_VIZ_BOLHA = 64, OP_BOLHA = 128;
+// Level 0's neighbour masks also carry, above bits 0-4, the cell's OP_BOLHA and OP_AGUA.
+constexpr int V0_BOLHA = 32, V0_AGUA = 64;
 
 __device__ __forceinline__ int grossoBaseF(int i) { return (i & 1) == 0 ? (i >> 1) - 1 : (i - 1) >> 1; }
 __device__ __forceinline__ float pesoBaseF(int i) { return (i & 1) == 0 ? 0.25f : 0.75f; }
@@ -504,7 +506,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
       x[cr][m] = (!ZERO && dentro) ? carregar(ldcg(src + c)) : 0.0f;
       if (MODO == M_ESPALHAR) {
         bq[cr][m] = dentro ? __ldcg(a.d.r + c) : 0.0f;
-        om[cr][m] = (a.bolhas && dentro) ? (int)(__ldcg(a.rotB + c) & 0xfff) : 0;  // own bubble label
+        om[cr][m] = (v[cr][m] & V0_BOLHA) ? (int)(__ldcg(a.rotB + c) & 0xfff) : 0;  // own bubble label
       } else {
         bq[cr][m] = dentro ? carregar(ldcg(b + c)) : 0.0f;
       }
@@ -607,23 +609,13 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
 #pragma unroll
     for (int cr = 0; cr < 2; cr++)
 #pragma unroll
-      for (int m = 0; m < 4; m++) {
-        const int c = cel[cr][m] < 0 ? 0 : cel[cr][m];
-        om[cr][m] = cel[cr][m] < 0 ? 0 : __ldcg(a.op + c);
-        rv[cr][m] = __ldcg(a.d.r + c);
-      }
-    if (a.bolhas) {  // a cell's own label is set only on bubble air (OP_BOLHA): load it there alone
+      for (int m = 0; m < 4; m++) rv[cr][m] = __ldcg(a.d.r + (cel[cr][m] < 0 ? 0 : cel[cr][m]));
+    // a cell's own label is set only on bubble air (V0_BOLHA in its mask): loaded there alone
 #pragma unroll
-      for (int cr = 0; cr < 2; cr++)
+    for (int cr = 0; cr < 2; cr++)
 #pragma unroll
-        for (int m = 0; m < 4; m++)
-          lb[cr][m] = (om[cr][m] & OP_BOLHA) ? (int)(__ldcg(a.rotB + cel[cr][m]) & 0xfff) : 0;
-    } else {
-#pragma unroll
-      for (int cr = 0; cr < 2; cr++)
-#pragma unroll
-        for (int m = 0; m < 4; m++) lb[cr][m] = 0;
-    }
+      for (int m = 0; m < 4; m++)
+        lb[cr][m] = (v[cr][m] & V0_BOLHA) ? (int)(__ldcg(a.rotB + cel[cr][m]) & 0xfff) : 0;
     if (ru.zVelho) {
 #pragma unroll
       for (int cr = 0; cr < 2; cr++)
@@ -663,7 +655,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
           continue;
         }
         ru.zNovo[c] = xz;
-        if (om[cr][m] & OP_AGUA) {
+        if (v[cr][m] & V0_AGUA) {
           s0 += (double)rv[cr][m] * (double)xz;
           if (ru.zVelho) s1 += (double)rv[cr][m] * (double)zv[cr][m];
         }
@@ -1551,6 +1543,12 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       if (j > 0 && ldcg8(tp + c - n.nx) != SOLIDO) m |= 4;
       if (j < n.ny - 1 && ldcg8(tp + c + n.nx) != SOLIDO) m |= 8;
       if (ldcg8(tp + c) == AGUA) m |= 16;
+      if (l == 0) {  // the descriptor's water and bubble-air bits (OP_AGUA, OP_BOLHA) for the
+                     // spread and the gather; every other reader masks bits 0-4
+        const int t = d.tipo[c];
+        if (t == AGUA) m |= V0_AGUA;
+        else if (a.bolhas && t == AR && bolhaAtiva(a, d.rotulo[c])) m |= V0_BOLHA;
+      }
       n.viz[c] = (uint8_t)m;
     }
   }
