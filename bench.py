@@ -10,12 +10,18 @@ step is one simulated 1/60 s frame: one air relabel and 14 substeps of 1/840 s (
 capillary limit of 1.197 ms at this h).  Every pressure solve runs to ||r|| <= 1e-6 ||r0||.
 The metric is substeps per second.
 
-`value` is the mixed-precision configuration (FP16 V-cycle storage) timed on the device with
-inputs resident; `fp32_plain` is the one-launch-per-step FP32 engine on the same frames; `e2e`
-is the mixed configuration through the C-ABI with host buffers (faucet particles in, every
-particle out, each frame).  --impl reference times the CPU oracle (the reference engine's
-algorithm restated in C++, single-threaded as the reference is) on the same scene.
-With --gpus N > 1 (torchrun) each rank advances its own replica (a tank does not shard).
+Every pressure solve stops on the TRUE residual ||b - A q|| <= 1e-6 ||r0|| (FP64, q accumulated in
+FP64), with an iteration cap of 1000; each arm reports the fraction of its solves that converged
+and the largest true relative residual.  `value` is the mixed-precision configuration (fused
+engine, FP16 V-cycle storage, block preconditioner, frames replayed from a CUDA graph) timed on
+the device, the faucet's particles added from pinned host memory each frame; `fp32_fused` is the
+same engine with FP32 storage; `fp32_plain` is the one-launch-per-step FP32 engine with the
+reference's preconditioner (the reference's algorithm on the GPU); `e2e` is the mixed
+configuration through the C-ABI with host buffers (faucet particles in, every particle out, each
+frame).  --impl reference times the CPU oracle (the reference engine's algorithm restated in C++,
+single-threaded as the reference is) on the same scene.
+With --gpus N > 1 each rank (relaunched under torch.distributed.run when WORLD_SIZE is unset)
+advances its own replica (a tank does not shard).
 """
 from __future__ import annotations
 
@@ -40,7 +46,7 @@ NX, NY, H = 840, 536, 0.0016
 SUB = 14
 DT_QUADRO = 1 / 60
 TOL = 1e-6
-MAX_ITER = 200
+MAX_ITER = 1000
 # Algorithmic HBM bytes of one PCG iteration per fine cell (5-point operator, V-cycle with
 # 4 smoother passes per level, restriction and prolongation, dots and vector updates) for
 # FP32 V-cycle storage and for 16-bit storage, plus the setup of a solve (initial residual,
@@ -204,6 +210,17 @@ def vazao_replicas(mundo, passos, subpassos, ms):
 
 
 # ------------------------------------------------------------------ GPU arm
+def estatisticas_solve(s):
+    """Convergence record of the handle's solves since the last reset (device counters)."""
+    from tanque import _abi
+    n = s.escalar(_abi.TQ_SCALAR_SOLVES)
+    cap = s.escalar(_abi.TQ_SCALAR_SOLVES_CAPPED)
+    return {"solves": int(n), "converged_frac": round(1.0 - cap / n, 4) if n else None,
+            "max_true_rel_residual": s.escalar(_abi.TQ_SCALAR_SOLVE_MAX_REL),
+            "mean_iters": round(s.escalar(_abi.TQ_SCALAR_SOLVE_ITERS) / n, 2) if n else None,
+            "replacements": int(s.escalar(_abi.TQ_SCALAR_SOLVE_REPLACEMENTS))}
+
+
 def executar_gpu(args, rank, mundo, dist):
     import torch
     from tanque import Cena, SimulacaoGPU, _abi
@@ -214,10 +231,17 @@ def executar_gpu(args, rank, mundo, dist):
     cena, _, agua, torneira = construir_cena(Cena, semente, labirinto, semear_retangulo_rapido)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     hbm, origem_pico = picos()
+    # the faucet's particles of every frame, in pinned host memory (the jet is the scene's input)
+    jatos = []
+    for q in range(args.warmup + args.steps):
+        j = jato(torneira, q)
+        buf = torch.empty(j.size, dtype=torch.float32, pin_memory=True).numpy()
+        buf[:] = j
+        jatos.append(buf)
 
-    def nova(precisao, motor):
+    def nova(precisao, motor, precond):
         s = SimulacaoGPU(cena, {"tolerance": TOL, "iterations": MAX_ITER, "precision": precisao, "engine": motor,
-                                "device": dev})
+                                "preconditioner": precond, "device": dev})
         s.adicionar(agua, False)
         return s
 
@@ -226,94 +250,66 @@ def executar_gpu(args, rank, mundo, dist):
         if dist is not None:
             dist.barrier()
 
-    def medir(precisao, motor, com_relogio=False):
-        """Device-timed frames with inputs resident; returns a dict of results."""
-        s = nova(precisao, motor)
+    def medir(precisao, motor, precond, grafo=False, etapas=False, com_relogio=False, e2e=False):
+        """Frames of the scene with the faucet: warm-up, then `steps` timed frames with CUDA
+        events on the handle's stream (L2 flushed before each, outside the events).  e2e adds
+        the read-back of every particle to the host inside the events."""
+        import ctypes as C
+        s = nova(precisao, motor, precond)
         ext = torch.cuda.ExternalStream(s.stream())
+        avancar = s.avancarGrafo if grafo else s.avancar
+        lig = _abi.carregar()
+        cap = s.opcoes.capacity or math.ceil(NX * NY * 4.6)
+        saida = torch.empty(cap * 12, dtype=torch.float32, pin_memory=True).numpy() if e2e else None
         for q in range(args.warmup):
-            s.avancar(DT_QUADRO, SUB)
+            s.adicionar(jatos[q], True)
+            avancar(DT_QUADRO, SUB)
         s.sincronizar()
         barreira()
-        s.tempos(True)
+        s.definirEscalar(_abi.TQ_SCALAR_SOLVES, 0)
+        if etapas:
+            s.tempos(True)
         l0 = SimulacaoGPU.lancamentos()
-        eventos = []
+        eventos, h2d, d2h = [], 0, 0
         rel = Relogios(dev) if com_relogio else None
         if rel:
             rel.__enter__()
         for q in range(args.steps):
             with torch.cuda.stream(ext):
                 flush.zero_()  # L2 flush between timed steps (outside the events)
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(ext)
-            s.avancar(DT_QUADRO, SUB)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            ent = jatos[args.warmup + q]
+            s.adicionar(ent, True)
+            avancar(DT_QUADRO, SUB)
+            if e2e:
+                n = C.c_int32(0)
+                lig("get_particles", s._h, saida.ctypes.data, cap, C.byref(n))
+                d2h += n.value * 48
             e1.record(ext)
             eventos.append((e0, e1))
+            h2d += ent.nbytes
         s.sincronizar()
         torch.cuda.synchronize()
         if rel:
             rel.__exit__()
-        lanc = SimulacaoGPU.lancamentos() - l0
-        ms = sum(a.elapsed_time(b) for a, b in eventos)
-        et = s.tempos()
-        n_part = s.n
+        res = dict(ms=sum(a.elapsed_time(b) for a, b in eventos), lancamentos=SimulacaoGPU.lancamentos() - l0,
+                   particulas=s.n, relogios=rel.resumo() if rel else None, solve=estatisticas_solve(s),
+                   etapas=s.tempos() if etapas else None, h2d=h2d / args.steps, d2h=d2h / args.steps)
         s.fechar()
-        return dict(ms=ms, etapas=et, lancamentos=lanc, particulas=n_part, relogios=rel.resumo() if rel else None)
+        return res
 
-    def medir_e2e(precisao, motor):
-        s = nova(precisao, motor)
-        ext = torch.cuda.ExternalStream(s.stream())
-        cap = s.opcoes.capacity or math.ceil(NX * NY * 4.6)
-        saida = torch.empty(cap * 12, dtype=torch.float32, pin_memory=True).numpy()
-        entradas = []
-        for q in range(args.warmup + args.steps):
-            j = jato(torneira, q)
-            buf = torch.empty(j.size, dtype=torch.float32, pin_memory=True).numpy()
-            buf[:] = j
-            entradas.append(buf)
-        h2d = d2h = 0
-        for q in range(args.warmup):
-            s.adicionar(entradas[q], True)
-            s.avancar(DT_QUADRO, SUB)
-        s.sincronizar()
-        barreira()
-        eventos = []
-        import ctypes as C
-        lig = _abi.carregar()
-        for q in range(args.steps):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            with torch.cuda.stream(ext):
-                flush.zero_()
-            e0.record(ext)
-            ent = entradas[args.warmup + q]
-            s.adicionar(ent, True)
-            s.avancar(DT_QUADRO, SUB)
-            n = C.c_int32(0)
-            lig("get_particles", s._h, saida.ctypes.data, cap, C.byref(n))
-            e1.record(ext)
-            eventos.append((e0, e1))
-            h2d += ent.nbytes
-            d2h += n.value * 48
-        torch.cuda.synchronize()
-        ms = sum(a.elapsed_time(b) for a, b in eventos)
-        s.fechar()
-        return dict(ms=ms, h2d=h2d / args.steps, d2h=d2h / args.steps)
+    FUSED, PLAIN = _abi.TQ_ENGINE_FUSED, _abi.TQ_ENGINE_PLAIN
+    BLOCO, REF = _abi.TQ_PRECOND_BLOCK, _abi.TQ_PRECOND_REFERENCE
+    misto = medir(_abi.TQ_PREC_FP16, FUSED, BLOCO, grafo=True, com_relogio=True)
+    misto_etapas = medir(_abi.TQ_PREC_FP16, FUSED, BLOCO, etapas=True)
+    fundido32 = medir(_abi.TQ_PREC_FP32, FUSED, BLOCO, grafo=True)
+    plano = medir(_abi.TQ_PREC_FP32, PLAIN, REF, etapas=True)
+    e2e = medir(_abi.TQ_PREC_FP16, FUSED, BLOCO, grafo=True, e2e=True)
 
-    precisao_mista = _abi.TQ_PREC_FP16
-    motor_misto = _abi.TQ_ENGINE_FUSED if getattr(args, "fused", True) else _abi.TQ_ENGINE_PLAIN
-    try:
-        misto = medir(precisao_mista, motor_misto, com_relogio=True)
-    except _abi.ErroTanque as e:
-        if e.status != _abi.TQ_E_ARG:
-            raise
-        motor_misto = _abi.TQ_ENGINE_PLAIN
-        misto = medir(precisao_mista, motor_misto, com_relogio=True)
-    plano = medir(_abi.TQ_PREC_FP32, _abi.TQ_ENGINE_PLAIN)
-    e2e = medir_e2e(precisao_mista, motor_misto)
-
-    tempos = tempos_max_ranks([misto["ms"], plano["ms"], e2e["ms"]], dist, "cuda")
-    valor, valor_plano, valor_e2e = (vazao_replicas(mundo, args.steps, SUB, t) for t in tempos)
+    tempos = tempos_max_ranks([misto["ms"], fundido32["ms"], plano["ms"], e2e["ms"]], dist, "cuda")
+    valor, valor_f32, valor_plano, valor_e2e = (vazao_replicas(mundo, args.steps, SUB, t) for t in tempos)
 
     def roofline(res, rotulo):
         et = res["etapas"]
@@ -324,7 +320,7 @@ def executar_gpu(args, rank, mundo, dist):
         gbs = b / t_solve / 1e9 if t_solve > 0 else 0.0
         return dict(iters=iters, ms_solve=t_solve * 1000, gbs=gbs, bytes=b)
 
-    r_m = roofline(misto, "fp16")
+    r_m = roofline(misto_etapas, "fp16")
     r_p = roofline(plano, "fp32")
     if rank != 0:
         return None
@@ -342,25 +338,30 @@ def executar_gpu(args, rank, mundo, dist):
         "dtype": "f32",
         "data": "synthetic",
         "config": {
-            "workload": "ultra scene 840x536 h=1.6mm, labyrinth 8-cell corridors/4-cell walls, faucet 12 cells at 1.2 m/s, "
-                        "sigma=0.0728; one step = 1 relabel + 14 substeps of 1/840 s",
-            "particles": misto["particulas"], "tolerance": TOL, "mixed_precision": "fp16 V-cycle storage",
-            "mixed_engine": "fused" if motor_misto == _abi.TQ_ENGINE_FUSED else "plain",
+            "workload": "ultra scene 840x536 h=1.6mm, labyrinth 8-cell corridors/4-cell walls, faucet 12 cells at 1.2 m/s "
+                        "added every frame, sigma=0.0728; one step = 1 relabel + 14 substeps of 1/840 s",
+            "particles": misto["particulas"], "tolerance": TOL, "tolerance_on": "true FP64 residual ||b - A q||",
+            "iteration_cap": MAX_ITER, "mixed_precision": "fp16 V-cycle storage",
+            "mixed_engine": "fused, block preconditioner, frames replayed from a CUDA graph",
             "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{mundo}",
         },
-        "fp32_plain": {"value": round(valor_plano, 2), "unit": "steps/s", "mgpcg_gbs": round(r_p["gbs"], 1),
-                       "pcg_iters": round(r_p["iters"], 2), "ms_solve": round(r_p["ms_solve"], 4)},
-        "mixed": {"mgpcg_gbs": round(r_m["gbs"], 1), "pcg_iters": round(r_m["iters"], 2),
-                  "ms_solve": round(r_m["ms_solve"], 4), "speedup_vs_fp32_plain": round(valor / valor_plano, 3)},
-        "stages_ms_per_substep": {k: round(misto["etapas"][k] / max(misto["etapas"]["subpassos"], 1), 4)
+        "mixed": {"solve": misto["solve"], "mgpcg_gbs": round(r_m["gbs"], 1), "pcg_iters": round(r_m["iters"], 2),
+                  "ms_solve": round(r_m["ms_solve"], 4), "speedup_vs_fp32_plain": round(valor / valor_plano, 3),
+                  "speedup_vs_fp32_fused": round(valor / valor_f32, 3)},
+        "fp32_fused": {"value": round(valor_f32, 2), "unit": "steps/s", "solve": fundido32["solve"],
+                       "engine": "fused, block preconditioner, CUDA graph"},
+        "fp32_plain": {"value": round(valor_plano, 2), "unit": "steps/s", "solve": plano["solve"],
+                       "mgpcg_gbs": round(r_p["gbs"], 1), "pcg_iters": round(r_p["iters"], 2),
+                       "ms_solve": round(r_p["ms_solve"], 4),
+                       "engine": "plain (one launch per reference dispatch), reference preconditioner"},
+        "stages_ms_per_substep": {k: round(misto_etapas["etapas"][k] / max(misto_etapas["etapas"]["subpassos"], 1), 4)
                                   for k in SimulacaoGPU.ETAPAS},
-        "roofline": {"kernel": "MGPCG pressure solve", "bound": "hbm", "achieved": round(r_m["gbs"], 1),
+        "roofline": {"kernel": "MGPCG pressure solve (k_mgpcg)", "bound": "hbm", "achieved": round(r_m["gbs"], 1),
                      "peak": hbm, "peak_source": origem_pico, "unit": "GB/s",
-                     "frac": round(r_m["gbs"] / hbm, 4),
-                     "traffic": TRAFEGO_SOLVE_BYTES if motor_misto == _abi.TQ_ENGINE_FUSED else None,
+                     "frac": round(r_m["gbs"] / hbm, 4), "traffic": TRAFEGO_SOLVE_BYTES,
                      "bytes_per_launch": round(r_m["bytes"])},
         "e2e": {"value": round(valor_e2e, 2), "unit": "steps/s", "h2d_bytes_per_step": int(e2e["h2d"]),
-                "d2h_bytes_per_step": int(e2e["d2h"])},
+                "d2h_bytes_per_step": int(e2e["d2h"]), "solve": e2e["solve"]},
         "gpu_launches": int(misto["lancamentos"]),
         "clocks": misto["relogios"],
     }
@@ -396,8 +397,10 @@ def executar_lote(args, rank, mundo, dist):
             dist.barrier()
 
     def medir(precisao, motor, com_relogio=False, e2e=False):
+        precond = _abi.TQ_PRECOND_BLOCK if motor == _abi.TQ_ENGINE_FUSED else _abi.TQ_PRECOND_REFERENCE
         lote = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H,
-                    {"tolerance": TOL, "iterations": MAX_ITER, "precision": precisao, "engine": motor, "device": dev})
+                    {"tolerance": TOL, "iterations": MAX_ITER, "precision": precisao, "engine": motor,
+                     "preconditioner": precond, "device": dev})
         fluxos = [torch.cuda.ExternalStream(s.stream()) for s in lote.sims]
         lig = _abi.carregar()
         saidas = []
@@ -516,8 +519,19 @@ def main():
                     help="ultra: the 450k-cell scene (default); lote: the 256-tank batch")
     args = ap.parse_args()
 
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: relaunch this command under torch.distributed.run
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            porta = so.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr=127.0.0.1", f"--master-port={porta}", os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
     mundo = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "ours" and mundo != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE {mundo}")
 
     if args.impl == "reference" and args.workload == "lote":
         if rank != 0:

@@ -51,6 +51,22 @@ extern "C" {
 #define TQ_ENGINE_PLAIN 0
 #define TQ_ENGINE_FUSED 1
 
+/* Preconditioner of the pressure solve.
+ * REFERENCE: cicloV as js/pressao-cpu.js:241-255 and precondicionar (:352-361): enclosed air
+ *            of an active bubble counts as water in the V-cycle, the bubble's residual is
+ *            spread evenly over its cells and its correction is their mean.
+ * BLOCK:     no counterpart in the reference.  A block-diagonal preconditioner: the bubble
+ *            rows take a Jacobi step (z_b = r_b / faces_b), and the V-cycle runs on the water
+ *            alone with enclosed air as free surface; coarse neighbour masks come from the
+ *            fine level's faces (a coarse face is open only where a fine face across it joins
+ *            two non-wall cells), so coarse levels do not connect water through thin walls.
+ *            Same smoother, transfers and coarse solve as REFERENCE.  With a tolerance the
+ *            solve converges to the same q (within the tolerance) in about half the
+ *            iterations on scenes with trapped air; with a fixed iteration count the iterates
+ *            differ from the reference's.  FUSED engine only. */
+#define TQ_PRECOND_REFERENCE 0
+#define TQ_PRECOND_BLOCK 1
+
 /* Particle-to-grid transfer semantics (the oracle implements both; the CUDA library only
  * TQ_P2G_FIXED, the integer accumulation of js/gpu/fisica.js:77-131). */
 #define TQ_P2G_FLOAT 0 /* js/fisica-cpu.js:198-267: float sums in particle order */
@@ -69,13 +85,16 @@ typedef struct tq_options {
   double tau_density;        /* opcoes.tauDensidade, default TAU_DENSIDADE = 0.1 s */
   double surface_tension;    /* opcoes.tensao, default TENSAO_SUPERFICIAL = 0.0728 N/m */
   double tolerance;          /* 0: fixed iteration count as in the reference; > 0: stop when
-                                ||r|| <= tolerance * ||r0|| (same norm as js/pressao-cpu.js:342) */
+                                the TRUE residual ||b - A q|| <= tolerance * ||r0||, both
+                                in FP64 with the norm of js/pressao-cpu.js:342 (see
+                                tq_solve_pressure) */
   int32_t precision;         /* TQ_PREC_* */
   int32_t engine;            /* TQ_ENGINE_* */
   int32_t p2g_mode;          /* TQ_P2G_* */
   int32_t capacity;          /* particle capacity; 0: ceil(nx*ny*PARTICULAS_MAX_POR_CELULA) */
   int32_t device;            /* CUDA device ordinal */
-  int32_t reserved[7];
+  int32_t preconditioner;    /* TQ_PRECOND_*, default TQ_PRECOND_REFERENCE */
+  int32_t reserved[6];
 } tq_options;
 
 /* Fills defaults for an nx x ny tank of cell size h. */
@@ -145,6 +164,16 @@ int tq_advance(tq_sim* s, double dt, int32_t substeps);
 /* SimulacaoCPU.subpasso(dt) (js/fisica-cpu.js:176-189). */
 int tq_substep(tq_sim* s, double dt);
 
+/* avancar(dt, subpassos) (js/fisica-cpu.js:155-159) with the substeps replayed from a CUDA
+ * graph: the air relabel runs as in tq_advance, then the `substeps` substeps are captured into
+ * a graph on the first call and replayed on later calls with the same dt and substep count
+ * (recaptured when they, or the gravity, change, or the particle count grows past the captured
+ * launch bound).
+ * Results are bit-identical to tq_advance.  Stage timing is not recorded for the replayed
+ * substeps.  The PLAIN engine in tolerance mode reads its stop flag on the host and cannot be
+ * captured: TQ_E_STATE.  No counterpart in the reference (it has no graph API). */
+int tq_advance_graph(tq_sim* s, double dt, int32_t substeps);
+
 /* SimulacaoCPU.atualizarAr() (js/fisica-cpu.js:162-167) — RastreadorDeAr.atualizar
  * (js/ar.js:56-153) on the device. */
 int tq_update_air(tq_sim* s);
@@ -210,7 +239,19 @@ enum tq_scalar {
   TQ_SCALAR_LAUNCHES = 6,       /* kernels launched by this process so far (all handles) */
   TQ_SCALAR_GRAVITY_X = 7,      /* sim.gravidade[0] (m/s^2) — writable, used from the next */
   TQ_SCALAR_GRAVITY_Y = 8,      /* sim.gravidade[1]   substep (MotorCPU.gravidade, js/motor.js:96) */
-  TQ_SCALAR_COUNT_ = 9
+  /* Convergence of the pressure solves (tolerance mode; no counterpart in the reference,
+   * whose solve runs a fixed count).  The solves record these on the device: reading them
+   * waits for the handle's stream, the solves themselves never wait for the host. */
+  TQ_SCALAR_PCG_TRUE_RES = 9,   /* ||b - A q|| (FP64) of the last solve's iterate; -1 without
+                                   a tolerance */
+  TQ_SCALAR_PCG_CONVERGED = 10, /* 1: the last solve met its tolerance on the true residual;
+                                   0: it stopped at the iteration cap */
+  TQ_SCALAR_SOLVES = 11,        /* solves since the last reset — writing 0 resets 11-15 */
+  TQ_SCALAR_SOLVES_CAPPED = 12, /* of them, stopped at the cap without converging */
+  TQ_SCALAR_SOLVE_ITERS = 13,   /* their iterations in total */
+  TQ_SCALAR_SOLVE_MAX_REL = 14, /* largest true ||b - A q|| / ||r0|| among them */
+  TQ_SCALAR_SOLVE_REPLACEMENTS = 15, /* residual replacements among them (see tq_solve_pressure) */
+  TQ_SCALAR_COUNT_ = 16
 };
 int tq_get_scalar(tq_sim* s, int32_t which, double* out);
 int tq_set_scalar(tq_sim* s, int32_t which, double value);
@@ -249,14 +290,33 @@ typedef struct tq_bubbles {
   float* y;               /* 4096 */
 } tq_bubbles;
 
+/* What a solve reports beside q (tq_solve_pressure's `info`, may be NULL). */
+typedef struct tq_solve_info {
+  int32_t iterations;    /* iterations run */
+  int32_t converged;     /* tolerance mode: 1 when ||b - A q|| <= tolerance * ||r0||; else 0 */
+  int32_t replacements;  /* residual replacements (tolerance mode) */
+  int32_t pad;
+  double residual0;      /* ||r0|| */
+  double residual;       /* the last recursive ||r|| */
+  double true_residual;  /* ||b - A q|| in FP64 of the final iterate (tolerance mode), else -1 */
+} tq_solve_info;
+
 /* resolverPCG(niveis, tipo, div, q, iteracoes, bolhas) (js/pressao-cpu.js:296-402) on the
- * device: solves n*q - sum(q_nb) = -div on water cells starting from q.  tolerance = 0 runs
- * exactly `iterations`; > 0 stops at ||r|| <= tolerance*||r0|| (cap `iterations`).
- * norms receives the residual history (initial, then one per iteration). */
+ * device: solves n*q - sum(q_nb) = -div on water cells starting from q.
+ * tolerance = 0 runs exactly `iterations`, as the reference does (ITERACOES_PCG = 3).
+ * tolerance > 0 (no counterpart in the reference) accumulates q in FP64 during the solve and
+ * stops when the TRUE residual ||b - A q||, recomputed in FP64 from the FP64 iterate and the
+ * bubble pressures, is <= tolerance * ||r0||, or at `iterations` (the cap).  The true residual
+ * is recomputed whenever the recursive FP32 one meets the tolerance; if the true one does
+ * not, it replaces the recursive one and CG restarts from it (residual replacement).
+ * q is returned rounded to FP32, so b - A q of the returned float q carries their rounding
+ * (about 1e-7 of |A| |q| per cell) on top of the reported true residual.
+ * norms receives the recursive residual history (initial, then one per iteration).
+ * preconditioner: TQ_PRECOND_*; TQ_PRECOND_BLOCK needs engine TQ_ENGINE_FUSED. */
 int tq_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float* div, float* q,
                       int32_t iterations, double tolerance, const tq_bubbles* bubbles,
-                      int32_t precision, int32_t engine, double* norms, int32_t norms_cap,
-                      int32_t* n_norms);
+                      int32_t precision, int32_t engine, int32_t preconditioner, double* norms,
+                      int32_t norms_cap, int32_t* n_norms, tq_solve_info* info);
 
 /* cicloV(niveis) (js/pressao-cpu.js:241-255) on the device: one V-cycle approximately
  * solving A x = b on the level-0 grid described by `tipo` (the types the preconditioner

@@ -67,7 +67,8 @@ int tqo_last_norms(tqo_sim* s, double* out, int32_t cap, int32_t* n);
 /* ---- standalone solver (js/pressao-cpu.js exports) */
 int tqo_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float* div, float* q,
                        int32_t iterations, double tolerance, const tq_bubbles* bubbles,
-                       double* norms, int32_t norms_cap, int32_t* n_norms);
+                       int32_t preconditioner, double* norms, int32_t norms_cap, int32_t* n_norms,
+                       tq_solve_info* info);
 int tqo_vcycle(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float* x);
 
 const char* tqo_last_error(void);

@@ -20,7 +20,7 @@
 // Parity pinning: there is no JavaScript engine on this machine or on the GPU box, so the
 // restatement cannot be diffed against SimulacaoCPU itself.  It is pinned against the
 // reference's own behavioural test suite (testes/fisica.test.js, testes/cena.test.js),
-// ported to tests/test_oracle_reference_suite.py, which it must pass with the reference's
+// ported to tests/test_oracle_suite_referencia.py, which it must pass with the reference's
 // own bounds.
 //
 // One option goes beyond the reference: p2g_mode = TQ_P2G_FIXED replaces the float P2G
@@ -458,11 +458,52 @@ struct BolhasPCG {           // `bolhas` argument: { rotulo, rhs, y }
   S* y;
 };
 
-// resolverPCG, js/pressao-cpu.js:296-402.  tol > 0 adds the relative-residual stop
-// (||r|| <= tol*||r0||) that the reference lacks; tol = 0 is the reference's fixed count.
+// Coarse neighbour masks from the fine level's faces (TQ_PRECOND_BLOCK; no counterpart in the
+// reference): the face between coarse cells C and its right neighbour is open when both are not
+// wall and some fine face across the coarse face (between fine columns 2I+1 and 2I+2, rows 2J and
+// 2J+1) joins two non-wall fine cells; likewise vertically.
+template <class S>
+void vizinhosPorFaces(const Nivel<S>& f, Nivel<S>& g) {
+  auto livre = [&](int i, int j) { return i >= 0 && j >= 0 && i < f.nx && j < f.ny && f.tipo[i + j * f.nx] != SOLIDO; };
+  for (int J = 0; J < g.ny; J++)
+    for (int I = 0; I < g.nx; I++) {
+      int C = I + J * g.nx, m = 0;
+      if (g.tipo[C] != SOLIDO) {
+        auto h = [&](int i0, int i1) {  // a fine face between columns i0, i1 in rows 2J, 2J+1
+          return (livre(i0, 2 * J) && livre(i1, 2 * J)) || (livre(i0, 2 * J + 1) && livre(i1, 2 * J + 1));
+        };
+        auto v = [&](int j0, int j1) {
+          return (livre(2 * I, j0) && livre(2 * I, j1)) || (livre(2 * I + 1, j0) && livre(2 * I + 1, j1));
+        };
+        if (I > 0 && g.tipo[C - 1] != SOLIDO && h(2 * I - 1, 2 * I)) m |= 1;
+        if (I < g.nx - 1 && g.tipo[C + 1] != SOLIDO && h(2 * I + 1, 2 * I + 2)) m |= 2;
+        if (J > 0 && g.tipo[C - g.nx] != SOLIDO && v(2 * J - 1, 2 * J)) m |= 4;
+        if (J < g.ny - 1 && g.tipo[C + g.nx] != SOLIDO && v(2 * J + 1, 2 * J + 2)) m |= 8;
+      }
+      g.viz[C] = (uint8_t)m;
+      g.cnt[C] = (uint8_t)((m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1) + ((m >> 3) & 1));
+    }
+}
+
+// What a solve reports beside q (tq_solve_info).
+struct InfoPCG {
+  int iters = 0, convergiu = 0, trocas = 0;
+  double r0 = 0, r = 0, rv = -1;
+};
+
+// resolverPCG, js/pressao-cpu.js:296-402.  tol = 0 is the reference's fixed count.  tol > 0 (no
+// counterpart in the reference) keeps q in double during the solve and stops when the TRUE
+// residual ||b - A q|| (double, from the double iterate and the bubbles' y) is <= tol*||r0||,
+// or at the cap.  The true residual is recomputed when the recursive one meets the tolerance;
+// when the true one does not, it replaces the recursive one and CG restarts from it.
+// precond = TQ_PRECOND_BLOCK replaces precondicionar (:352-361) by the block-diagonal form:
+// bubble rows z_b = r_b / faces_b, the V-cycle on the water alone (enclosed air stays air) with
+// coarse neighbour masks from the fine faces (vizinhosPorFaces).
 template <class S>
 std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div, S* q,
-                                int iteracoes, const BolhasPCG<S>* bolhas, double tol) {
+                                int iteracoes, const BolhasPCG<S>* bolhas, double tol,
+                                int precond = TQ_PRECOND_REFERENCE, InfoPCG* info = nullptr) {
+  const bool bloco = precond == TQ_PRECOND_BLOCK;
   Nivel<S>& n0 = L.n[0];
   int nx = n0.nx, ny = n0.ny;
   int k = nx * ny;
@@ -477,11 +518,15 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
   std::copy(tipo, tipo + k, op.tipo.begin());
   prepararVizinhos(op);
   std::copy(tipo, tipo + k, n0.tipo.begin());
-  if (bolhas)
+  if (bolhas && !bloco)
     for (int c = 0; c < k; c++)
       if (tipo[c] == AR && bolhas->rotulo[c] >= 2) n0.tipo[c] = AGUA;
   tiposGrossos(L);
-  for (auto& n : L.n) prepararVizinhos(n);
+  prepararVizinhos(L.n[0]);
+  for (size_t l = 1; l < L.n.size(); l++) {
+    if (bloco) vizinhosPorFaces(L.n[l - 1], L.n[l]);
+    else prepararVizinhos(L.n[l]);
+  }
   if (!L.cgPronto) {
     L.r.assign(k, 0);
     L.z.assign(k, 0);
@@ -547,6 +592,41 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
   for (uint32_t b : ativos) rb.set(b, (double)bolhas->rhs[b] - aq.get(b));
   auto norma = [&]() { return std::sqrt(produto(r, r, tipo) + produtoB(rb, rb)); };
   std::vector<double> normas{norma()};
+  // tolerance mode: the double iterate (water cells) and the true residual from it
+  const bool verdade = tol > 0;
+  std::vector<double> qd;
+  if (verdade) qd.assign(qv.begin(), qv.end());
+  auto residuoVerdadeiro = [&](bool substituir) {
+    std::vector<double> g(qd);
+    if (rot)
+      for (int c = 0; c < k; c++) {
+        uint32_t b = rot[c];
+        if (b >= 2 && tipo[c] == AR) g[c] = b < (uint32_t)MAX_BOLHAS && temFace[b] ? yb.get(b) : 0.0;
+      }
+    double s = 0;
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) {
+        int c = i + j * nx;
+        if (tipo[c] != AGUA) continue;
+        int m = op.viz[c];
+        double t = 0;
+        if (m & 1) t += g[c - 1];
+        if (m & 2) t += g[c + 1];
+        if (m & 4) t += g[c - nx];
+        if (m & 8) t += g[c + nx];
+        double rt = -(double)div[c] - (op.cnt[c] * g[c] - t);
+        s += rt * rt;
+        if (substituir) r[c] = (S)rt;
+      }
+    MapaB somaB;
+    for (size_t m = 0; m < pares.size(); m += 2) somaB.set(pares[m], somaB.get(pares[m]) + qd[pares[m + 1]]);
+    for (uint32_t b : ativos) {
+      double rt = (double)bolhas->rhs[b] - (faces[b] * yb.get(b) - somaB.get(b));
+      s += rt * rt;
+      if (substituir) rb.set(b, rt);
+    }
+    return std::sqrt(s);
+  };
   // celulasDe (js/pressao-cpu.js:345-351)
   std::vector<int> celulasDe(MAX_BOLHAS, 0);
   if (rot)
@@ -557,6 +637,12 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
   auto tem = [&](uint32_t b) { return b < (uint32_t)MAX_BOLHAS && celulasDe[b] > 0; };
   auto precondicionar = [&](std::vector<S>& destino, MapaB& destinoB) {
     n0.b = r;
+    if (bloco) {  // bubble air is air to the V-cycle (r = 0 there); bubble rows: Jacobi
+      cicloV(L);
+      destino = n0.x;
+      for (uint32_t b : ativos) destinoB.set(b, rb.get(b) / faces[b]);
+      return;
+    }
     if (rot)
       for (int c = 0; c < k; c++) {
         uint32_t b = rot[c];
@@ -574,6 +660,8 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
         }
       }
   };
+  InfoPCG inf;
+  inf.r0 = normas[0];
   precondicionar(z, zb);
   p = z;
   for (uint32_t b : ativos) pb.set(b, zb.get(b));
@@ -590,7 +678,8 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
     double alfa = std::fabs(pap) < 1e-30 ? 0 : rz / pap;
     for (int c = 0; c < k; c++) {
       if (tipo[c] != AGUA) continue;
-      qv[c] = (S)((double)qv[c] + alfa * (double)p[c]);
+      if (verdade) qd[c] += alfa * (double)p[c];
+      else qv[c] = (S)((double)qv[c] + alfa * (double)p[c]);
       r[c] = (S)((double)r[c] - alfa * (double)ap[c]);
     }
     for (uint32_t b : ativos) {
@@ -598,8 +687,25 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
       rb.set(b, rb.get(b) - alfa * apb.get(b));
     }
     normas.push_back(norma());
+    inf.iters = it + 1;
+    if (verdade && (normas.back() <= tol * normas[0] || it == iteracoes - 1)) {
+      const bool ultima = it == iteracoes - 1;
+      // the true residual; when it misses the tolerance before the cap it replaces r, rb
+      const double rv = residuoVerdadeiro(false);
+      inf.rv = rv;
+      if (rv <= tol * normas[0] || ultima) {
+        inf.convergiu = rv <= tol * normas[0] ? 1 : 0;
+        break;
+      }
+      residuoVerdadeiro(true);
+      inf.trocas++;
+      precondicionar(z, zb);  // restart: p = z
+      p = z;
+      for (uint32_t b : ativos) pb.set(b, zb.get(b));
+      rz = produto(r, z, tipo) + produtoB(rb, zb);
+      continue;
+    }
     if (it == iteracoes - 1) break;
-    if (tol > 0 && normas.back() <= tol * normas[0]) break;
     zVelho = z;
     for (uint32_t b : ativos) zvb.set(b, zb.get(b));
     precondicionar(z, zb);
@@ -610,9 +716,13 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
     for (int c = 0; c < k; c++) p[c] = tipo[c] == AGUA ? (S)((double)z[c] + beta * (double)p[c]) : (S)0;
     for (uint32_t b : ativos) pb.set(b, zb.get(b) + beta * pb.get(b));
   }
+  if (verdade)
+    for (int c = 0; c < k; c++) qv[c] = (S)qd[c];
   for (int c = 0; c < k; c++) q[c] = tipo[c] != AGUA ? (S)0 : qv[c];
   if (bolhas)
     for (uint32_t b : ativos) bolhas->y[b] = (S)yb.get(b);
+  inf.r = normas.back();
+  if (info) *info = inf;
   return normas;
 }
 
@@ -791,11 +901,16 @@ struct Sim : SimBase {
   std::vector<float> p;  // Float32Array of CAMPOS per particle
   double vMax = 0;
   std::vector<double> normas;
+  int precond;
+  InfoPCG info;  // the last solve
+  // accumulated since the last reset (TQ_SCALAR_SOLVES = 0)
+  long long solves = 0, capados = 0, itersAcum = 0, trocasAcum = 0;
+  double maxRel = 0;
 
   Sim(const tq_options& o)
       : cena(o.nx, o.ny, o.h), nx(o.nx), ny(o.ny), h(o.h), iteracoes(o.iterations),
         tauDensidade(o.tau_density), tensao(o.surface_tension), tol(o.tolerance),
-        arAtivo(o.air != 0), p2gMode(o.p2g_mode), rastreador(o.nx, o.ny) {
+        arAtivo(o.air != 0), p2gMode(o.p2g_mode), rastreador(o.nx, o.ny), precond(o.preconditioner) {
     gravidade[0] = o.gravity[0];
     gravidade[1] = o.gravity[1];
     nu = (nx + 1) * ny;
@@ -1293,7 +1408,15 @@ struct Sim : SimBase {
   // #pressao, :498-515
   void pressao(double dt) {
     BolhasPCG<S> b{rastreador.rotulo.data(), rhsBolha.data(), yBolha.data()};
-    normas = resolverPCG(niveis, tipo.data(), div.data(), q.data(), iteracoes, arAtivo ? &b : nullptr, tol);
+    normas = resolverPCG(niveis, tipo.data(), div.data(), q.data(), iteracoes, arAtivo ? &b : nullptr, tol, precond,
+                         &info);
+    solves++;
+    itersAcum += info.iters;
+    trocasAcum += info.trocas;
+    if (tol > 0) {
+      if (!info.convergiu) capados++;
+      if (info.r0 > 0 && info.rv / info.r0 > maxRel) maxRel = info.rv / info.r0;
+    }
     double paraPa = (DENSIDADE_AGUA * h) / dt;
     const uint32_t* rot = rastreador.rotulo.data();
     int N = nx * ny;
@@ -1662,6 +1785,8 @@ static int validar(const tq_options* o) {
   if (o->nx < 3 || o->ny < 3 || !(o->h > 0)) return fail(TQ_E_ARG, "grid must be at least 3x3 with h > 0");
   if (o->iterations < 1) return fail(TQ_E_ARG, "iterations must be >= 1");
   if (o->p2g_mode != TQ_P2G_FLOAT && o->p2g_mode != TQ_P2G_FIXED) return fail(TQ_E_ARG, "bad p2g_mode");
+  if (o->preconditioner != TQ_PRECOND_REFERENCE && o->preconditioner != TQ_PRECOND_BLOCK)
+    return fail(TQ_E_ARG, "bad preconditioner");
   return TQ_OK;
 }
 
@@ -1785,6 +1910,13 @@ int tqo_get_scalar(tqo_sim* s, int32_t which, double* out) {
       case TQ_SCALAR_PCG_RES: *out = S_.normas.empty() ? 0 : S_.normas.back(); break;
       case TQ_SCALAR_GRAVITY_X: *out = S_.gravidade[0]; break;
       case TQ_SCALAR_GRAVITY_Y: *out = S_.gravidade[1]; break;
+      case TQ_SCALAR_PCG_TRUE_RES: *out = S_.info.rv; break;
+      case TQ_SCALAR_PCG_CONVERGED: *out = S_.info.convergiu; break;
+      case TQ_SCALAR_SOLVES: *out = (double)S_.solves; break;
+      case TQ_SCALAR_SOLVES_CAPPED: *out = (double)S_.capados; break;
+      case TQ_SCALAR_SOLVE_ITERS: *out = (double)S_.itersAcum; break;
+      case TQ_SCALAR_SOLVE_MAX_REL: *out = S_.maxRel; break;
+      case TQ_SCALAR_SOLVE_REPLACEMENTS: *out = (double)S_.trocasAcum; break;
       default: return fail(TQ_E_ARG, "unknown scalar");
     }
   });
@@ -1798,6 +1930,11 @@ int tqo_set_scalar(tqo_sim* s, int32_t which, double value) {
       case TQ_SCALAR_TIPOS_PRONTOS: S_.tiposProntos = value != 0; break;
       case TQ_SCALAR_GRAVITY_X: S_.gravidade[0] = value; break;  // sim.gravidade (js/motor.js:96)
       case TQ_SCALAR_GRAVITY_Y: S_.gravidade[1] = value; break;
+      case TQ_SCALAR_SOLVES:  // 0 resets the accumulated solve statistics
+        if (value != 0) return fail(TQ_E_ARG, "TQ_SCALAR_SOLVES can only be reset to 0");
+        S_.solves = S_.capados = S_.itersAcum = S_.trocasAcum = 0;
+        S_.maxRel = 0;
+        break;
       default: return fail(TQ_E_ARG, "scalar not writable");
     }
   });
@@ -1814,8 +1951,11 @@ int tqo_last_norms(tqo_sim* s, double* out, int32_t cap, int32_t* n) {
 
 int tqo_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float* div, float* q,
                        int32_t iterations, double tolerance, const tq_bubbles* bubbles,
-                       double* norms, int32_t norms_cap, int32_t* n_norms) {
+                       int32_t preconditioner, double* norms, int32_t norms_cap, int32_t* n_norms,
+                       tq_solve_info* info) {
   if (nx < 3 || ny < 3 || !tipo || !div || !q || iterations < 1) return fail(TQ_E_ARG, "bad arguments");
+  if (preconditioner != TQ_PRECOND_REFERENCE && preconditioner != TQ_PRECOND_BLOCK)
+    return fail(TQ_E_ARG, "bad preconditioner");
   Niveis<float> L;
   montarNiveis(L, nx, ny);
   BolhasPCG<float> b{};
@@ -1826,7 +1966,17 @@ int tqo_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float*
     b.rhs = bubbles->rhs;
     b.y = bubbles->y;
   }
-  auto normas = resolverPCG<float>(L, tipo, div, q, iterations, bubbles ? &b : nullptr, tolerance);
+  InfoPCG inf;
+  auto normas = resolverPCG<float>(L, tipo, div, q, iterations, bubbles ? &b : nullptr, tolerance, preconditioner, &inf);
+  if (info) {
+    info->iterations = inf.iters;
+    info->converged = inf.convergiu;
+    info->replacements = inf.trocas;
+    info->pad = 0;
+    info->residual0 = inf.r0;
+    info->residual = inf.r;
+    info->true_residual = inf.rv;
+  }
   if (n_norms) *n_norms = (int32_t)normas.size();
   if (norms)
     for (int32_t k = 0; k < norms_cap && k < (int32_t)normas.size(); k++) norms[k] = normas[k];

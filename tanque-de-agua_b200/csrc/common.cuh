@@ -61,10 +61,18 @@ struct Escalares {
   int iters;                  // iterations done by the running solve
   int pronto;                 // the running solve met its tolerance
   int erro;                   // device-side error flag (bounded waits, capacity)
+  int verificar;              // plain engine, tolerance mode: a true-residual check is due
+  int reiniciar;              // plain engine: the true residual replaced r; CG restarts
   int aceitas;                // particles accepted by the last add
   int pendentes;              // label-propagation work list length
   int pad;
   unsigned int tickets[16];   // last-block-done counters of the reductions
+  // convergence of the solves (tolerance mode), written on the device at the end of each solve
+  double normaVerd;           // true ||b - A q|| of the last solve's iterate (-1: fixed count)
+  int convergiu;              // the last solve met its tolerance on the true residual
+  int trocas;                 // residual replacements of the last solve
+  long long solves, capados, itersAcum, trocasAcum;  // accumulated since the last reset
+  double maxRel;              // largest true ||b - A q|| / ||r0|| since the last reset
   double normas[1024];        // residual history of the running solve
 };
 
@@ -75,6 +83,9 @@ struct NivelDev {
   uint8_t* tipo;  // SOLIDO/AGUA/AR as the preconditioner sees them
   uint8_t* viz;   // bits 0-3: free neighbours (left, right, down, up); bit 4: water
   T *b, *x, *tmp;
+  // a solve's stop flag (Escalares::pronto): once set, the V-cycle kernels of the iterations the
+  // host queued past convergence return at once; null outside a solve
+  const int* parar = nullptr;
 };
 
 // ------------------------------------------------------------ device state

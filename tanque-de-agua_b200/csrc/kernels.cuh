@@ -35,10 +35,16 @@ struct Pcg;
 Pcg* criarPcg(int nx, int ny, int precisao, int motor);
 void destruirPcg(Pcg* p);
 // Solves for d.q on the cells d.tipo marks as water; bubbles from d.rotulo / d.rhsB / d.yB when
-// `bolhas`.  Returns TQ_OK or an error status; *iters receives the iterations done.
-int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s);
-int normasPcg(Pcg* p, double* out, int cap);
-int itersPcg(Pcg* p);
+// `bolhas`; precond is TQ_PRECOND_*.  The FUSED engine queues the solve without waiting; the
+// PLAIN engine reads its stop flag every few iterations in tolerance mode.  The iteration count,
+// residual history and convergence record stay in d.esc.  Returns TQ_OK or an error status.
+int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, int precond, cudaStream_t s);
+// The last solve's residual history from the device (waits for the stream); its length, or -1.
+int normasPcg(Pcg* p, const Dev& d, double* out, int cap, cudaStream_t s);
+// TQ_E_TIMEOUT if a fused solve since the last call gave up on a bounded wait (waits for the stream).
+int erroPcg(Pcg* p, cudaStream_t s);
+// The engine a solver actually runs (a FUSED request falls back to PLAIN on one-level grids).
+int motorPcg(Pcg* p);
 // Phase trace of the fused engine (%globaltimer at each grid barrier of the last solve).
 void perfilPcg(Pcg* p, bool ligar);
 int lerPerfilPcg(Pcg* p, unsigned long long* out, int cap);

@@ -18,12 +18,13 @@
 namespace tq {
 
 // ---------------------------------------------------------------- types and neighbours
-// The preconditioner's level-0 types: bubble air counts as water (js/pressao-cpu.js:305-308).
-__global__ void k_mg_tipo0(const uint8_t* tipo, const uint32_t* rot, uint8_t* t0, int N, int bolhas) {
+// The preconditioner's level-0 types: bubble air counts as water (js/pressao-cpu.js:305-308);
+// with TQ_PRECOND_BLOCK (bloco) it stays air.
+__global__ void k_mg_tipo0(const uint8_t* tipo, const uint32_t* rot, uint8_t* t0, int N, int bolhas, int bloco) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= N) return;
   uint8_t t = tipo[c];
-  if (bolhas && t == AR && rot[c] >= 2) t = AGUA;
+  if (bolhas && !bloco && t == AR && rot[c] >= 2) t = AGUA;
   t0[c] = t;
 }
 
@@ -59,6 +60,30 @@ __global__ void k_viz(const uint8_t* tipo, int nx, int ny, uint8_t* viz) {
   viz[c] = (uint8_t)m;
 }
 
+// TQ_PRECOND_BLOCK's coarse masks: bits 0-3 open where a fine face across the coarse face joins
+// two non-wall fine cells (both coarse cells not wall), bit 4 water.
+__global__ void k_viz_faces(const uint8_t* tf, int fnx, int fny, const uint8_t* tg, int gnx, int gny, uint8_t* viz) {
+  int C = blockIdx.x * blockDim.x + threadIdx.x;
+  if (C >= gnx * gny) return;
+  const int I = C % gnx, J = C / gnx;
+  int m = 0;
+  if (tg[C] != SOLIDO) {
+    auto livre = [&](int i, int j) { return i >= 0 && j >= 0 && i < fnx && j < fny && tf[i + j * fnx] != SOLIDO; };
+    auto horiz = [&](int i0, int i1) {
+      return (livre(i0, 2 * J) && livre(i1, 2 * J)) || (livre(i0, 2 * J + 1) && livre(i1, 2 * J + 1));
+    };
+    auto vert = [&](int j0, int j1) {
+      return (livre(2 * I, j0) && livre(2 * I, j1)) || (livre(2 * I + 1, j0) && livre(2 * I + 1, j1));
+    };
+    if (I > 0 && tg[C - 1] != SOLIDO && horiz(2 * I - 1, 2 * I)) m |= 1;
+    if (I < gnx - 1 && tg[C + 1] != SOLIDO && horiz(2 * I + 1, 2 * I + 2)) m |= 2;
+    if (J > 0 && tg[C - gnx] != SOLIDO && vert(2 * J - 1, 2 * J)) m |= 4;
+    if (J < gny - 1 && tg[C + gnx] != SOLIDO && vert(2 * J + 1, 2 * J + 2)) m |= 8;
+    if (tg[C] == AGUA) m |= 16;
+  }
+  viz[C] = (uint8_t)m;
+}
+
 // ---------------------------------------------------------------- V-cycle kernels
 // suavizar (js/pressao-cpu.js:99-150): each 16x16 block reads the snapshot `src` (18x18 with
 // its one-cell border, zero outside the grid), runs VARREDURAS red-black sweeps inside the
@@ -68,6 +93,7 @@ template <class T>
 __global__ void __launch_bounds__(256) k_suavizar(NivelDev<T> n, int desl, int ordem, const T* __restrict__ src,
                                                   T* __restrict__ dst, const T* __restrict__ b) {
   __shared__ float qs[18 * 18];
+  if (n.parar && *n.parar) return;  // uniform over the CTA
   const int nx = n.nx, ny = n.ny;
   const int ox = (int)blockIdx.x * 16 - desl, oy = (int)blockIdx.y * 16 - desl;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -126,7 +152,7 @@ __device__ inline float residuoFino(const NivelDev<TF>& f, const TF* __restrict_
 template <class TF, class TG>
 __global__ void k_restringir(NivelDev<TF> f, const TF* __restrict__ xf, const TF* __restrict__ bf, NivelDev<TG> g) {
   int C = blockIdx.x * blockDim.x + threadIdx.x;
-  if (C >= g.nx * g.ny) return;
+  if (C >= g.nx * g.ny || (f.parar && *f.parar)) return;
   g.x[C] = guardar<TG>(0.0f);
   if (!(g.viz[C] & 16)) {
     g.b[C] = guardar<TG>(0.0f);
@@ -153,7 +179,7 @@ __device__ inline float pesoBase(int i) { return (i & 1) == 0 ? 0.25f : 0.75f; }
 template <class TG, class TF>
 __global__ void k_prolongar(NivelDev<TG> g, NivelDev<TF> f, TF* __restrict__ xf) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= f.nx * f.ny) return;
+  if (c >= f.nx * f.ny || (f.parar && *f.parar)) return;
   if (!(f.viz[c] & 16)) return;
   int i = c % f.nx, j = c / f.nx;
   int I0 = grossoBase(i), J0 = grossoBase(j);
@@ -177,6 +203,7 @@ __global__ void k_prolongar(NivelDev<TG> g, NivelDev<TF> f, TF* __restrict__ xf)
 // in place on the coarsest level, one CTA; the level lives in shared memory when it fits.
 __global__ void __launch_bounds__(1024) k_grosso(NivelDev<float> n, int emShared) {
   extern __shared__ unsigned char dyn[];
+  if (n.parar && *n.parar) return;  // uniform over the CTA
   const int N = n.nx * n.ny, nx = n.nx;
   float* x = n.x;
   const float* b = n.b;
@@ -241,7 +268,7 @@ __device__ inline float aplicarA(const Dev& d, const uint8_t* vizOp, const float
 }
 
 // r = -div - A q on water cells (js/pressao-cpu.js:331-338); q = 0 elsewhere.
-__global__ void k_pcg_inicio(Dev d, const uint8_t* vizOp, int bolhas) {
+__global__ void k_pcg_inicio(Dev d, const uint8_t* vizOp, int bolhas, double* q64) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.N) return;
   if (d.tipo[c] != AGUA) {
@@ -250,6 +277,7 @@ __global__ void k_pcg_inicio(Dev d, const uint8_t* vizOp, int bolhas) {
     return;
   }
   d.r[c] = -d.div[c] - aplicarA(d, vizOp, d.q, d.ybf, c, bolhas != 0);
+  if (q64) q64[c] = (double)d.q[c];  // tolerance mode: the FP64 iterate
 }
 
 // Active bubbles (montarBolhas, js/pressao-cpu.js:271-288): faces = number of (interior bubble
@@ -289,7 +317,7 @@ __global__ void k_bolhas_inicio(Dev d) {
 constexpr double ESCALA_PCG = 1099511627776.0;  // 2^40
 __global__ void k_bolhas_somar_v(Dev d, const float* v) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.N) return;
+  if (c >= d.N || d.esc->pronto) return;
   const int nx = d.nx;
   int i = c % nx, j = c / nx;
   if (i < 1 || j < 1 || i >= nx - 1 || j >= d.ny - 1) return;
@@ -306,7 +334,7 @@ __global__ void k_bolhas_somar_v(Dev d, const float* v) {
 // modo 1: apb = faces*pb - sum
 __global__ void k_bolhas_linhas(Dev d, int modo) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= MAX_BOLHAS) return;
+  if (b >= MAX_BOLHAS || d.esc->pronto) return;
   if (b < 2 || d.facesB[b] == 0) return;
   double soma = (double)d.accB[b] / ESCALA_PCG;
   if (modo == 0) d.rb[b] = (double)d.rhsBolhaF[b] - (d.facesB[b] * d.yB[b] - soma);
@@ -319,7 +347,7 @@ __global__ void k_bolhas_linhas(Dev d, int modo) {
 template <class T>
 __global__ void k_pre_espalhar(Dev d, NivelDev<T> n0, int bolhas) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.N) return;
+  if (c >= d.N || d.esc->pronto) return;
   float e = (float)d.esc->escalaMG;
   float v = d.r[c];
   if (bolhas && d.tipo[c] == AR) {
@@ -334,7 +362,7 @@ __global__ void k_pre_espalhar(Dev d, NivelDev<T> n0, int bolhas) {
 template <class T>
 __global__ void k_pre_juntar(Dev d, NivelDev<T> n0, int bolhas) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.N) return;
+  if (c >= d.N || d.esc->pronto) return;
   float inv = (float)(1.0 / d.esc->escalaMG);
   float x = carregar(n0.x[c]) * inv;
   if (bolhas && d.tipo[c] == AR) {
@@ -347,22 +375,26 @@ __global__ void k_pre_juntar(Dev d, NivelDev<T> n0, int bolhas) {
   }
   d.z[c] = x;
 }
-__global__ void k_pre_bolhas(Dev d) {
+// The bubbles' z: the gathered mean correction, or with TQ_PRECOND_BLOCK (bloco) a Jacobi step on
+// the bubble's row, r_b / faces_b.
+__global__ void k_pre_bolhas(Dev d, int bloco) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= MAX_BOLHAS) return;
-  d.zb[b] = (b >= 2 && d.facesB[b] > 0) ? (double)d.accB[b] / ESCALA_PCG : 0.0;
+  if (b >= MAX_BOLHAS || d.esc->pronto) return;
+  const bool at = b >= 2 && d.facesB[b] > 0;
+  d.zb[b] = !at ? 0.0 : bloco ? d.rb[b] / (double)d.facesB[b] : (double)d.accB[b] / ESCALA_PCG;
 }
 
 // ap = A p on water cells (js/pressao-cpu.js:367-373).
 __global__ void k_aplicar(Dev d, const uint8_t* vizOp, int bolhas) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.N) return;
+  if (c >= d.N || d.esc->pronto) return;
   d.ap[c] = d.tipo[c] == AGUA ? aplicarA(d, vizOp, d.p, d.pbf, c, bolhas != 0) : 0.0f;
 }
 
 // q += alpha p, r -= alpha Ap on water; bubbles likewise (js/pressao-cpu.js:377-385).
-__global__ void k_atualizar(Dev d) {
+__global__ void k_atualizar(Dev d, double* q64) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.esc->pronto) return;
   double alfa = d.esc->alpha;
   if (c < MAX_BOLHAS && c >= 2 && d.facesB[c] > 0) {
     d.yB[c] += alfa * d.pb[c];
@@ -371,13 +403,110 @@ __global__ void k_atualizar(Dev d) {
   }
   if (c >= d.N || d.tipo[c] != AGUA) return;
   float a = (float)alfa;
-  d.q[c] = d.q[c] + a * d.p[c];
+  if (q64) q64[c] += alfa * (double)d.p[c];
+  else d.q[c] = d.q[c] + a * d.p[c];
   d.r[c] = d.r[c] - a * d.ap[c];
+}
+
+__device__ inline double somaBloco(double v, double* sh);  // block sum (valid in thread 0), below
+
+// Tolerance mode, once the recursive residual met the tolerance (Escalares::verificar): the true
+// residual in FP64 from the FP64 iterate and the bubble pressures.  Water cells: rt = -div - A q
+// into d.ap (free until the next A p) and rt^2 into per-CTA partials; interior air of active
+// bubbles: the sum of q over its water faces into the bubble's fixed-point sum (accB, zeroed
+// before).  k_verdade_fim finishes the norm and decides.
+__global__ void __launch_bounds__(256) k_verdade(Dev d, const uint8_t* vizOp, const double* q64, int bolhas) {
+  __shared__ double sh[32];
+  if (!d.esc->verificar || d.esc->pronto) return;  // uniform over the grid
+  double s = 0;
+  const int nx = d.nx;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.N; c += gridDim.x * blockDim.x) {
+    const uint8_t t = d.tipo[c];
+    if (t == AGUA) {
+      const int vz = vizOp[c];
+      double sv = 0;
+      const int nb[4] = {c - 1, c + 1, c - nx, c + nx};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (!(vz & (1 << q))) continue;
+        const uint8_t tn = d.tipo[nb[q]];
+        if (tn == AGUA) sv += q64[nb[q]];
+        else if (bolhas && tn == AR) {
+          const uint32_t r = d.rotulo[nb[q]];
+          if (r >= 2 && r < (uint32_t)MAX_BOLHAS && d.facesB[r] > 0) sv += d.yB[r];
+        }
+      }
+      const double rt = -(double)d.div[c] - ((double)__popc(vz & 15) * q64[c] - sv);
+      d.ap[c] = (float)rt;
+      s += rt * rt;
+    } else if (bolhas && t == AR) {
+      const int i = c % nx, j = c / nx;
+      if (i < 1 || j < 1 || i >= nx - 1 || j >= d.ny - 1) continue;
+      const uint32_t b = d.rotulo[c];
+      if (b < 2 || b >= (uint32_t)MAX_BOLHAS || d.facesB[b] == 0) continue;
+      double t2 = 0;
+      if (d.tipo[c - 1] == AGUA) t2 += q64[c - 1];
+      if (d.tipo[c + 1] == AGUA) t2 += q64[c + 1];
+      if (d.tipo[c - nx] == AGUA) t2 += q64[c - nx];
+      if (d.tipo[c + nx] == AGUA) t2 += q64[c + nx];
+      if (t2 != 0) somaFixa(&d.accB[b], t2, ESCALA_PCG);
+    }
+  }
+  const double tb = somaBloco(s, sh);
+  if (threadIdx.x == 0) d.parciais[2 * blockIdx.x] = tb;
+}
+// One CTA: the true norm (partials in block order, then the bubble rows rhs - (faces y - sum)),
+// and the decision: converged or at the cap -> pronto; else the bubble rows take their true
+// residual, reiniciar is set (k_substituir copies the water part, BETA restarts the direction).
+__global__ void __launch_bounds__(256) k_verdade_fim(Dev d, int blocosVerdade, int cap, double tol, int bolhas,
+                                                    int meiaPrecisao) {
+  __shared__ double sh[32];
+  __shared__ int substituir;
+  Escalares* e = d.esc;
+  if (!e->verificar || e->pronto) return;
+  double p1 = 0, q1 = 0;
+  for (int k = threadIdx.x; k < blocosVerdade; k += blockDim.x) p1 += d.parciais[2 * k];
+  auto rbv = [&](int b) { return (double)d.rhsBolhaF[b] - (d.facesB[b] * d.yB[b] - (double)d.accB[b] / ESCALA_PCG); };
+  if (bolhas)
+    for (int b = threadIdx.x; b < MAX_BOLHAS; b += blockDim.x)
+      if (b >= 2 && d.facesB[b] > 0) {
+        const double v = rbv(b);
+        q1 += v * v;
+      }
+  const double T1 = somaBloco(p1, sh), B1 = somaBloco(q1, sh);
+  if (threadIdx.x == 0) {
+    const double nv = sqrt(T1 + B1);
+    const bool ok = nv <= tol * e->norma0;
+    e->normaVerd = nv;
+    e->verificar = 0;
+    substituir = 0;
+    if (ok || e->iters >= cap) {
+      e->pronto = 1;
+      e->convergiu = ok ? 1 : 0;
+    } else {
+      e->reiniciar = 1;
+      e->trocas++;
+      e->norma = nv;
+      e->escalaMG = (meiaPrecisao && nv > 0) ? 1.0 / nv : 1.0;
+      substituir = 1;
+    }
+  }
+  __syncthreads();
+  if (substituir && bolhas)
+    for (int b = threadIdx.x; b < MAX_BOLHAS; b += blockDim.x)
+      if (b >= 2 && d.facesB[b] > 0) d.rb[b] = rbv(b);
+}
+// After a replacement: r = the true residual on water cells.
+__global__ void k_substituir(Dev d) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.N || !d.esc->reiniciar || d.esc->pronto) return;
+  if (d.tipo[c] == AGUA) d.r[c] = d.ap[c];
 }
 
 // p = z + beta p on water (0 elsewhere); bubbles likewise (js/pressao-cpu.js:395-396).
 __global__ void k_direcao(Dev d) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.esc->pronto) return;
   double beta = d.esc->beta;
   if (c < MAX_BOLHAS && c >= 2 && d.facesB[c] > 0) {
     d.pb[c] = d.zb[c] + beta * d.pb[c];
@@ -399,14 +528,31 @@ __global__ void k_copiar_pz(Dev d) {
 // zOld = z, zvb = zb (js/pressao-cpu.js:388-389)
 __global__ void k_guardar_z(Dev d) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d.esc->pronto) return;
   if (c < MAX_BOLHAS) d.zvb[c] = d.zb[c];
   if (c < d.N) d.zOld[c] = d.z[c];
 }
 // End of the solve: non-water q = 0; bubbles hand back their pressure (js/pressao-cpu.js:399-400).
-__global__ void k_pcg_fim(Dev d, int bolhas) {
+// Tolerance mode: q = the FP64 iterate rounded; the solve's convergence record (thread 0).
+__global__ void k_pcg_fim(Dev d, int bolhas, const double* q64, double tol) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (bolhas && c >= 2 && c < MAX_BOLHAS && d.facesB[c] > 0) d.yBolhaF[c] = (float)d.yB[c];
-  if (c < d.N && d.tipo[c] != AGUA) d.q[c] = 0.0f;
+  if (c < d.N) {
+    if (d.tipo[c] != AGUA) d.q[c] = 0.0f;
+    else if (q64) d.q[c] = (float)q64[c];
+  }
+  if (c == 0) {
+    Escalares* e = d.esc;
+    if (!q64) {
+      e->normaVerd = -1.0;
+      e->convergiu = 0;
+    }
+    e->solves++;
+    if (q64 && !e->convergiu) e->capados++;
+    e->itersAcum += e->iters;
+    e->trocasAcum += e->trocas;
+    if (q64 && e->norma0 > 0 && e->normaVerd / e->norma0 > e->maxRel) e->maxRel = e->normaVerd / e->norma0;
+  }
 }
 
 // ---------------------------------------------------------------- dot products
@@ -434,9 +580,10 @@ __device__ inline double somaBloco(double v, double* sh) {
 }
 
 __global__ void __launch_bounds__(DOT_T) k_produto(Dev d, int modo, const float* a, const float* b1, const float* b2,
-                                                 int it, double tol, int bolhas, int meiaPrecisao) {
+                                                 int it, double tol, int bolhas, int meiaPrecisao, int cap) {
   __shared__ double sh[32];
   __shared__ bool ultimo;
+  if (modo != NORMA0 && d.esc->pronto) return;  // uniform over the grid
   double s1 = 0, s2 = 0;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.N; c += gridDim.x * blockDim.x) {
     if (d.tipo[c] != AGUA) continue;
@@ -487,7 +634,12 @@ __global__ void __launch_bounds__(DOT_T) k_produto(Dev d, int modo, const float*
         e->norma0 = e->norma = nr;
         e->normas[0] = nr;
         e->iters = 0;
-        e->pronto = tol > 0 && nr <= 0.0;
+        e->pronto = 0;
+        e->verificar = 0;
+        e->reiniciar = 0;
+        e->trocas = 0;
+        e->convergiu = 0;
+        e->normaVerd = -1.0;
         e->escalaMG = (meiaPrecisao && nr > 0) ? 1.0 / nr : 1.0;
         break;
       }
@@ -498,13 +650,17 @@ __global__ void __launch_bounds__(DOT_T) k_produto(Dev d, int modo, const float*
         e->norma = nr;
         if (it + 1 < 1024) e->normas[it + 1] = nr;
         e->iters = it + 1;
-        e->pronto = tol > 0 && nr <= tol * e->norma0;
+        // tolerance mode: the recursive residual met the tolerance (or the cap came): the true
+        // residual decides (k_verdade, k_verdade_fim)
+        e->verificar = tol > 0 && (nr <= tol * e->norma0 || it + 1 >= cap);
         e->escalaMG = (meiaPrecisao && nr > 0) ? 1.0 / nr : 1.0;
         break;
       }
       case BETA: {
         double rzNovo = x1, cruzado = x2;
-        e->beta = fabs(e->rz) < 1e-30 ? 0.0 : fmax(0.0, (rzNovo - cruzado) / e->rz);
+        // after a replacement CG restarts: p = z (js/pressao-cpu.js:363-364's form)
+        e->beta = (e->reiniciar || fabs(e->rz) < 1e-30) ? 0.0 : fmax(0.0, (rzNovo - cruzado) / e->rz);
+        e->reiniciar = 0;
         e->rz = rzNovo;
         break;
       }
@@ -584,6 +740,7 @@ void destruirPcg(Pcg* p) {
     cudaFree(p->tmpL[l]);
   }
   cudaFree(p->vizOp);
+  if (p->q64) cudaFree(p->q64);
   delete p;
 }
 
@@ -598,6 +755,7 @@ static NivelDev<T> nivel(Pcg* p, int l) {
   n.b = (T*)p->bL[l];
   n.x = (T*)p->xL[l];
   n.tmp = (T*)p->tmpL[l];
+  n.parar = p->parar;
   return n;
 }
 
@@ -661,45 +819,64 @@ static void cicloV(Pcg* p, cudaStream_t s) {
   }
 }
 
-// Types and neighbour masks of every level for this solve.
-static void prepararNiveis(Pcg* p, const uint8_t* tipo0, cudaStream_t s) {
+// Types and neighbour masks of every level for this solve (bloco: TQ_PRECOND_BLOCK's coarse
+// masks from the fine faces).
+static void prepararNiveis(Pcg* p, const uint8_t* tipo0, bool bloco, cudaStream_t s) {
   if (tipo0 != p->tipoL[0]) cudaMemcpyAsync(p->tipoL[0], tipo0, p->N, cudaMemcpyDeviceToDevice, s);
   for (int l = 1; l < p->L; l++)
     lanca(k_mg_tipo_grosso, blocos((long)p->nxL[l] * p->nyL[l], 256), 256, 0, s, p->tipoL[l - 1], p->nxL[l - 1],
           p->nyL[l - 1], p->tipoL[l], p->nxL[l], p->nyL[l]);
-  for (int l = 0; l < p->L; l++)
-    lanca(k_viz, blocos((long)p->nxL[l] * p->nyL[l], 256), 256, 0, s, p->tipoL[l], p->nxL[l], p->nyL[l], p->vizL[l]);
+  for (int l = 0; l < p->L; l++) {
+    const int nb = blocos((long)p->nxL[l] * p->nyL[l], 256);
+    if (bloco && l >= 1)
+      lanca(k_viz_faces, nb, 256, 0, s, p->tipoL[l - 1], p->nxL[l - 1], p->nyL[l - 1], p->tipoL[l], p->nxL[l],
+            p->nyL[l], p->vizL[l]);
+    else
+      lanca(k_viz, nb, 256, 0, s, p->tipoL[l], p->nxL[l], p->nyL[l], p->vizL[l]);
+  }
 }
 
-static void precondicionar(Pcg* p, const Dev& d, bool bolhas, cudaStream_t s) {
+static void precondicionar(Pcg* p, const Dev& d, bool bolhas, bool bloco, cudaStream_t s) {
   int nb = blocos(d.N, 256);
+  const bool espalhar = bolhas && !bloco;  // with BLOCK the V-cycle does not see the bubbles
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
-    lanca(k_pre_espalhar<T>, nb, 256, 0, s, d, nivel<T>(p, 0), bolhas ? 1 : 0);
+    lanca(k_pre_espalhar<T>, nb, 256, 0, s, d, nivel<T>(p, 0), espalhar ? 1 : 0);
   });
   cicloV(p, s);
-  if (bolhas) cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
+  if (espalhar) cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
-    lanca(k_pre_juntar<T>, nb, 256, 0, s, d, nivel<T>(p, 0), bolhas ? 1 : 0);
+    lanca(k_pre_juntar<T>, nb, 256, 0, s, d, nivel<T>(p, 0), espalhar ? 1 : 0);
   });
-  if (bolhas) lanca(k_pre_bolhas, blocos(MAX_BOLHAS, 256), 256, 0, s, d);
+  if (bolhas) lanca(k_pre_bolhas, blocos(MAX_BOLHAS, 256), 256, 0, s, d, bloco ? 1 : 0);
 }
 
 static void produto(Pcg* p, const Dev& d, int modo, const float* a, const float* b1, const float* b2, int it,
-                    double tol, bool bolhas, cudaStream_t s) {
+                    double tol, bool bolhas, int cap, cudaStream_t s) {
   lanca(k_produto, DOT_BLOCOS, DOT_T, 0, s, d, modo, a, b1, b2, it, tol, bolhas ? 1 : 0,
-        p->precisao != TQ_PREC_FP32 ? 1 : 0);
+        p->precisao != TQ_PREC_FP32 ? 1 : 0, cap);
 }
 
-int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s) {
-  if (p->motor == TQ_ENGINE_FUSED) return resolverPressaoFundido(p, d, iteracoes, tol, bolhas, s);
+// Iterations the plain engine queues between two reads of the stop flag.  Every kernel of an
+// iteration returns at once after the flag is set, so the result is the same as stopping at the
+// exact iteration, with one host round trip per LOTE_VERIFICACAO iterations instead of one each.
+constexpr int LOTE_VERIFICACAO = 8;
+
+int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, int precond, cudaStream_t s) {
+  if (p->motor == TQ_ENGINE_FUSED) return resolverPressaoFundido(p, d, iteracoes, tol, bolhas, precond, s);
+  const bool bloco = precond == TQ_PRECOND_BLOCK;
   const int nb = blocos(d.N, 256);
   const int nbx = blocos(d.N > MAX_BOLHAS ? d.N : MAX_BOLHAS, 256);
+  double* q64 = nullptr;
+  if (tol > 0) {
+    if (!p->q64 && cudaMalloc(&p->q64, (size_t)d.N * sizeof(double)) != cudaSuccess) return TQ_E_NOMEM;
+    q64 = p->q64;
+  }
   // operator (true types) and preconditioner types
   lanca(k_viz, nb, 256, 0, s, d.tipo, d.nx, d.ny, p->vizOp);
-  lanca(k_mg_tipo0, nb, 256, 0, s, d.tipo, d.rotulo, p->tipoL[0], d.N, bolhas ? 1 : 0);
-  prepararNiveis(p, p->tipoL[0], s);
+  lanca(k_mg_tipo0, nb, 256, 0, s, d.tipo, d.rotulo, p->tipoL[0], d.N, bolhas ? 1 : 0, bloco ? 1 : 0);
+  prepararNiveis(p, p->tipoL[0], bloco, s);
   cudaMemsetAsync(d.facesB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
   cudaMemsetAsync(d.celsB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
   if (bolhas) {
@@ -707,16 +884,17 @@ int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas
     lanca(k_bolhas_celulas, nb, 256, 0, s, d);
   }
   lanca(k_bolhas_inicio, blocos(MAX_BOLHAS, 256), 256, 0, s, d);
-  lanca(k_pcg_inicio, nb, 256, 0, s, d, p->vizOp, bolhas ? 1 : 0);
+  lanca(k_pcg_inicio, nb, 256, 0, s, d, p->vizOp, bolhas ? 1 : 0, q64);
   if (bolhas) {
     cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
     lanca(k_bolhas_somar_v, nb, 256, 0, s, d, d.q);
     lanca(k_bolhas_linhas, blocos(MAX_BOLHAS, 256), 256, 0, s, d, 0);
   }
-  produto(p, d, NORMA0, d.r, d.r, nullptr, 0, tol, bolhas, s);
-  precondicionar(p, d, bolhas, s);
+  produto(p, d, NORMA0, d.r, d.r, nullptr, 0, tol, bolhas, iteracoes, s);
+  p->parar = &d.esc->pronto;  // the V-cycle kernels return once the solve has stopped
+  precondicionar(p, d, bolhas, bloco, s);
   lanca(k_copiar_pz, nbx, 256, 0, s, d);
-  produto(p, d, RZ0, d.r, d.z, nullptr, 0, tol, bolhas, s);
+  produto(p, d, RZ0, d.r, d.z, nullptr, 0, tol, bolhas, iteracoes, s);
   int it = 0;
   for (; it < iteracoes; it++) {
     lanca(k_aplicar, nb, 256, 0, s, d, p->vizOp, bolhas ? 1 : 0);
@@ -725,42 +903,52 @@ int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas
       lanca(k_bolhas_somar_v, nb, 256, 0, s, d, d.p);
       lanca(k_bolhas_linhas, blocos(MAX_BOLHAS, 256), 256, 0, s, d, 1);
     }
-    produto(p, d, PAP, d.p, d.ap, nullptr, it, tol, bolhas, s);
-    lanca(k_atualizar, nbx, 256, 0, s, d);
-    produto(p, d, NORMA, d.r, d.r, nullptr, it, tol, bolhas, s);
+    produto(p, d, PAP, d.p, d.ap, nullptr, it, tol, bolhas, iteracoes, s);
+    lanca(k_atualizar, nbx, 256, 0, s, d, q64);
+    produto(p, d, NORMA, d.r, d.r, nullptr, it, tol, bolhas, iteracoes, s);
+    if (q64) {  // the true residual, when NORMA found the recursive one within the tolerance
+      if (bolhas) cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
+      lanca(k_verdade, DOT_BLOCOS, 256, 0, s, d, p->vizOp, q64, bolhas ? 1 : 0);
+      lanca(k_verdade_fim, 1, 256, 0, s, d, DOT_BLOCOS, iteracoes, tol, bolhas ? 1 : 0,
+            p->precisao != TQ_PREC_FP32 ? 1 : 0);
+      lanca(k_substituir, nb, 256, 0, s, d);
+    }
     if (it == iteracoes - 1) break;
-    if (tol > 0) {
+    if (tol > 0 && it % LOTE_VERIFICACAO == LOTE_VERIFICACAO - 1) {
       int pronto = 0;
       if (cudaMemcpyAsync(&pronto, &d.esc->pronto, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-          cudaStreamSynchronize(s) != cudaSuccess)
+          cudaStreamSynchronize(s) != cudaSuccess) {
+        p->parar = nullptr;
         return TQ_E_CUDA;
+      }
       if (pronto) break;
     }
     lanca(k_guardar_z, nbx, 256, 0, s, d);
-    precondicionar(p, d, bolhas, s);
-    produto(p, d, BETA, d.r, d.z, d.zOld, it, tol, bolhas, s);
+    precondicionar(p, d, bolhas, bloco, s);
+    produto(p, d, BETA, d.r, d.z, d.zOld, it, tol, bolhas, iteracoes, s);
     lanca(k_direcao, nbx, 256, 0, s, d);
   }
-  lanca(k_pcg_fim, nbx, 256, 0, s, d, bolhas ? 1 : 0);
-  // residual history for tq_last_norms
-  int iters = 0;
-  if (cudaMemcpyAsync(&iters, &d.esc->iters, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return TQ_E_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return TQ_E_CUDA;
-  p->iters = iters;
-  p->normas.resize(iters + 1);
-  if (cudaMemcpyAsync(p->normas.data(), d.esc->normas, sizeof(double) * (iters + 1), cudaMemcpyDeviceToHost, s) !=
-      cudaSuccess)
-    return TQ_E_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return TQ_E_CUDA;
+  p->parar = nullptr;
+  lanca(k_pcg_fim, nbx, 256, 0, s, d, bolhas ? 1 : 0, q64, tol);
   return cudaGetLastError() == cudaSuccess ? TQ_OK : TQ_E_CUDA;
 }
 
-int normasPcg(Pcg* p, double* out, int cap) {
-  int n = (int)p->normas.size();
-  for (int k = 0; k < n && k < cap; k++) out[k] = p->normas[k];
+// The residual history of the last solve (Escalares::normas), read from the device.
+int normasPcg(Pcg* p, const Dev& d, double* out, int cap, cudaStream_t s) {
+  (void)p;
+  int iters = 0;
+  if (cudaMemcpyAsync(&iters, &d.esc->iters, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return -1;
+  int n = iters + 1 < 1024 ? iters + 1 : 1024;
+  int k = n < cap ? n : cap;
+  if (k > 0 && (cudaMemcpyAsync(out, d.esc->normas, sizeof(double) * k, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess))
+    return -1;
   return n;
 }
-int itersPcg(Pcg* p) { return p->iters; }
+int erroPcg(Pcg* p, cudaStream_t s) { return erroFundido(p->fundido, s); }
+int motorPcg(Pcg* p) { return p->motor; }
 void perfilPcg(Pcg* p, bool ligar) { perfilFundido(p->fundido, ligar); }
 int lerPerfilPcg(Pcg* p, unsigned long long* out, int cap) { return lerPerfilFundido(p->fundido, out, cap); }
 
@@ -779,7 +967,7 @@ __global__ void k_descarregar_x(NivelDev<T> n0, float* x) {
   x[c] = carregar(n0.x[c]);
 }
 int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cudaStream_t s) {
-  prepararNiveis(p, tipo, s);
+  prepararNiveis(p, tipo, false, s);
   int nb = blocos(p->N, 256);
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;

@@ -100,6 +100,8 @@ struct Fundido {
   void* kern = nullptr;
   unsigned long long* perfil = nullptr;
   bool perfilar = false;
+  double* q64 = nullptr;     // the FP64 iterate of a tolerance-mode solve
+  long long* accV = nullptr; // per-bubble fixed-point sums of the true residual
 };
 
 struct Args {
@@ -132,6 +134,11 @@ struct Args {
   // per level: 1 per 16x16 block whose cells are all wall (out-of-grid cells count as wall), the
   // blocks of shift 0 then those of shift 8; null where the level does not skip wall blocks
   uint8_t* sol[MAX_NIVEIS];
+  int bloco;  // TQ_PRECOND_BLOCK: bubble rows Jacobi, V-cycle on water, coarse masks from faces
+  // tolerance mode: q accumulates in FP64 (q64) and the solve stops on the true residual
+  // ||b - A q64|| (FP64), with residual replacement; null in fixed-count mode
+  double* q64;
+  long long* accV;
 };
 
 // The level table, copied into shared memory at kernel start: every phase reads its level's
@@ -321,6 +328,38 @@ __device__ void somasGlobais(const Args& a, int nAt, F0 f0, F1 f1, double* sh, d
 
 __device__ __forceinline__ bool bolhaAtiva(const Args& a, uint32_t r) {
   return r >= 2 && r < (uint32_t)MAX_BOLHAS && __ldcg(&a.d.facesB[r]) > 0;
+}
+
+// The preconditioned residual z_b of active bubble b: REFERENCE, the mean V-cycle correction
+// over its cells (the gather's fixed-point sum, precondicionar js/pressao-cpu.js:357-361);
+// BLOCK, a Jacobi step on its row, r_b / faces_b (its diagonal).
+__device__ __forceinline__ double zbDe(const Args& a, int b) {
+  return a.bloco ? __ldcg(&a.d.rb[b]) / (double)__ldcg(&a.d.facesB[b]) : (double)__ldcg(&a.accZ[b]) / ESC;
+}
+
+// Free-neighbour bits (0-3: left, right, down, up) of coarse cell (I, J) of level g from the
+// faces of its finer level f (TQ_PRECOND_BLOCK): a coarse face is open when both coarse cells
+// are not wall and a fine face across it (between fine columns 2I+1 and 2I+2 in rows 2J, 2J+1,
+// or the vertical counterpart) joins two non-wall fine cells.  Walls thinner than a coarse cell
+// then still separate the water on either side.
+__device__ __noinline__ int vizinhosPorFaces(const NivelF& f, const NivelF& g, int I, int J) {
+  const int C = I + J * g.nx;
+  if (ldcg8(g.tipo + C) == SOLIDO) return 0;
+  auto livre = [&](int i, int j) {
+    return i >= 0 && j >= 0 && i < f.nx && j < f.ny && ldcg8(f.tipo + i + j * f.nx) != SOLIDO;
+  };
+  auto horiz = [&](int i0, int i1) {
+    return (livre(i0, 2 * J) && livre(i1, 2 * J)) || (livre(i0, 2 * J + 1) && livre(i1, 2 * J + 1));
+  };
+  auto vert = [&](int j0, int j1) {
+    return (livre(2 * I, j0) && livre(2 * I, j1)) || (livre(2 * I + 1, j0) && livre(2 * I + 1, j1));
+  };
+  int m = 0;
+  if (I > 0 && ldcg8(g.tipo + C - 1) != SOLIDO && horiz(2 * I - 1, 2 * I)) m |= 1;
+  if (I < g.nx - 1 && ldcg8(g.tipo + C + 1) != SOLIDO && horiz(2 * I + 1, 2 * I + 2)) m |= 2;
+  if (J > 0 && ldcg8(g.tipo + C - g.nx) != SOLIDO && vert(2 * J - 1, 2 * J)) m |= 4;
+  if (J < g.ny - 1 && ldcg8(g.tipo + C + g.nx) != SOLIDO && vert(2 * J + 1, 2 * J + 2)) m |= 8;
+  return m;
 }
 
 // Per-cell operator descriptor of level 0 (built once per solve): bits 0-3 the left, right,
@@ -1378,7 +1417,7 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
   const int N = d.N, nx = d.nx, ny = d.ny;
   const int gt0 = blockIdx.x * TF + threadIdx.x, GT = gridDim.x * TF;
   auto pbNovoV = [&](int b) {
-    const double zb = (double)__ldcg(&a.accZ[b]) / ESC;
+    const double zb = zbDe(a, b);
     return prim ? zb : zb + beta * __ldcg(&pbVelho[b]);
   };
   double s = 0;
@@ -1446,6 +1485,50 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
   if (threadIdx.x == 0) a.parc[blockIdx.x * NPARC + 0] = tb;
 }
 
+// The true residual of a tolerance-mode solve, in FP64 from the FP64 iterate q64 and the bubble
+// pressures yB: on water cells r = -div - A q (js/pressao-cpu.js:331-338, bubble neighbours
+// through their y), written to d.r in FP32 (the replacement, when it comes to that) and summed
+// squared into channel 0; on the interior air of active bubbles, the sum of q over the bubble's
+// water faces into its fixed-point sum accV (the bubble row, :339-341, is finished after the
+// next barrier).
+__device__ __noinline__ void faseVerdade(const Args& a, double* sh) {
+  const Dev& d = a.d;
+  const int N = d.N, nx = d.nx;
+  const int gt0 = blockIdx.x * TF + threadIdx.x, GT = gridDim.x * TF;
+  double s = 0;
+  for (int c = gt0; c < N; c += GT) {
+    const int mk = __ldcg(a.op + c);
+    if (!(mk & (OP_AGUA | OP_FACE))) continue;
+    const int nb[4] = {c - 1, c + 1, c - nx, c + nx};  // read only where the mask says in grid
+    const unsigned long long rl = a.bolhas ? __ldcg(a.rotB + c) : 0ull;
+    if (mk & OP_AGUA) {
+      double sv = 0;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (mk & (1 << q)) sv += __ldcg(a.q64 + nb[q]);
+        else if (mk & OP_VIZ_BOLHA) {
+          const int r = (int)(rl >> (12 + 12 * q)) & 0xfff;
+          if (r) sv += __ldcg(d.yB + r);
+        }
+      }
+      const double rt = -(double)__ldcg(d.div + c) - ((double)(mk >> 8) * __ldcg(a.q64 + c) - sv);
+      d.r[c] = (float)rt;
+      s += rt * rt;
+    } else {
+      double t = 0;
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (mk & (1 << q)) t += __ldcg(a.q64 + nb[q]);
+      if (t != 0) somaFixa(&a.accV[(int)(rl & 0xfff)], t, ESC);
+    }
+  }
+  const double tb = somaBloco(s, sh);
+  if (threadIdx.x == 0) {
+    a.parc[blockIdx.x * NPARC + 0] = tb;
+    a.parc[blockIdx.x * NPARC + 1] = 0.0;
+  }
+}
+
 // The wall-block flags of the levels that have them (Args::sol), both shifts: one warp per
 // block, 8 cells a lane; a block is wall when every cell of it in the grid is.
 __device__ __noinline__ void marcarParedes(const Args& a) {
@@ -1494,7 +1577,9 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     for (int c = gt0; c < N; c += GT) {
       const int t = d.tipo[c];
       const uint32_t rot = d.rotulo[c];
-      t0[c] = (a.bolhas && t == AR && rot >= 2) ? AGUA : (uint8_t)t;
+      // REFERENCE: enclosed air of a bubble is water to the V-cycle (js/pressao-cpu.js:305-308);
+      // BLOCK: it stays air (free surface), the bubble rows take a Jacobi step instead
+      t0[c] = (a.bolhas && !a.bloco && t == AR && rot >= 2) ? AGUA : (uint8_t)t;
       const int i = c % nx, j = c / nx;
       int m = 0;
       if (i > 0 && d.tipo[c - 1] != SOLIDO) m |= 1;
@@ -1538,16 +1623,21 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       const int i = c % n.nx, j = c / n.nx;
       const uint8_t* tp = n.tipo;
       int m = 0;
-      if (i > 0 && ldcg8(tp + c - 1) != SOLIDO) m |= 1;
-      if (i < n.nx - 1 && ldcg8(tp + c + 1) != SOLIDO) m |= 2;
-      if (j > 0 && ldcg8(tp + c - n.nx) != SOLIDO) m |= 4;
-      if (j < n.ny - 1 && ldcg8(tp + c + n.nx) != SOLIDO) m |= 8;
+      if (l >= 1 && a.bloco) {
+        m = vizinhosPorFaces(s_niv[l - 1], n, i, j);
+      } else {
+        if (i > 0 && ldcg8(tp + c - 1) != SOLIDO) m |= 1;
+        if (i < n.nx - 1 && ldcg8(tp + c + 1) != SOLIDO) m |= 2;
+        if (j > 0 && ldcg8(tp + c - n.nx) != SOLIDO) m |= 4;
+        if (j < n.ny - 1 && ldcg8(tp + c + n.nx) != SOLIDO) m |= 8;
+      }
       if (ldcg8(tp + c) == AGUA) m |= 16;
       if (l == 0) {  // the descriptor's water and bubble-air bits (OP_AGUA, OP_BOLHA) for the
-                     // spread and the gather; every other reader masks bits 0-4
+                     // spread and the gather; every other reader masks bits 0-4.  With BLOCK
+                     // the V-cycle does not see bubbles: no cell spreads or gathers for one.
         const int t = d.tipo[c];
         if (t == AGUA) m |= V0_AGUA;
-        else if (a.bolhas && t == AR && bolhaAtiva(a, d.rotulo[c])) m |= V0_BOLHA;
+        else if (a.bolhas && !a.bloco && t == AR && bolhaAtiva(a, d.rotulo[c])) m |= V0_BOLHA;
       }
       n.viz[c] = (uint8_t)m;
     }
@@ -1632,6 +1722,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
                           [&](uint32_t r) { return (float)__ldcg(d.yB + r); });
       float rv = -d.div[c] - ar;
       d.r[c] = rv;
+      if (a.q64) a.q64[c] = (double)d.q[c];
       s += (double)rv * rv;
     }
     if (a.bolhas)
@@ -1718,11 +1809,13 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     }
   if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, d.z, nullptr}, sh, secaoDensa)) return;
   int cz = 0, cp = 0;  // which of the two z / p buffers holds the latest values
-  auto zbAtual = [&](int b) { return (double)__ldcg(&a.accZ[b]) / ESC; };
+  auto zbAtual = [&](int b) { return zbDe(a, b); };
   somasGlobais(a, nAt, [&](int b) { return __ldcg(&d.rb[b]) * zbAtual(b); }, [](int) { return 0.0; }, sh, somas);
   double rz = somas[0] + somas[2];
   double beta = 0.0;
   bool primeira = true;
+  int itersFeitas = 0, trocas = 0;
+  double normaVerd = -1.0;
 
   for (int it = 0; it < a.iteracoes; it++) {
     float* zc = cz ? a.z2 : d.z;
@@ -1765,11 +1858,13 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       for (int c0 = gt0; c0 < N; c0 += 4 * GT) {  // batches of 4 cells: all loads first
         int m[4];
         float qv[4], pnv[4], rv[4], apv[4];
+        double qd[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
           const int c = c0 + k * GT < N ? c0 + k * GT : 0;
           m[k] = c0 + k * GT < N ? __ldcg(a.op + c) : 0;
-          qv[k] = __ldcg(d.q + c);
+          if (a.q64) qd[k] = __ldcg(a.q64 + c);
+          else qv[k] = __ldcg(d.q + c);
           pnv[k] = __ldcg(pn + c);
           rv[k] = __ldcg(d.r + c);
           apv[k] = __ldcg(d.ap + c);
@@ -1778,7 +1873,8 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
         for (int k = 0; k < 4; k++) {
           if (!(m[k] & OP_AGUA)) continue;
           const int c = c0 + k * GT;
-          d.q[c] = qv[k] + af * pnv[k];
+          if (a.q64) a.q64[c] = qd[k] + alfa * (double)pnv[k];
+          else d.q[c] = qv[k] + af * pnv[k];
           const float r = rv[k] - af * apv[k];
           d.r[c] = r;
           s += (double)r * r;
@@ -1794,7 +1890,10 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
           sb += rbn * rbn;
         }
         s += sb;
-        for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) a.accZ[b] = 0;
+        for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) {
+          a.accZ[b] = 0;
+          if (a.q64) a.accV[b] = 0;
+        }
       }
       double tb = somaBloco(s, sh);
       if (threadIdx.x == 0) a.parc[blockIdx.x * NPARC + 0] = tb;
@@ -1802,8 +1901,34 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     if (!barreira(a, ep)) return;
     // ---- [C] norm, convergence, spread the residual
     somasGlobais(a, 0, [](int) { return 0.0; }, [](int) { return 0.0; }, sh, somas);
-    const double norma = sqrt(somas[0]);
-    const bool fim = it == a.iteracoes - 1 || (a.tol > 0 && norma <= a.tol * norma0);
+    double norma = sqrt(somas[0]);
+    itersFeitas = it + 1;
+    bool fim = it == a.iteracoes - 1 || (a.tol > 0 && norma <= a.tol * norma0);
+    bool reinicio = false;
+    if (fim && a.q64) {
+      // tolerance mode: the true residual of the FP64 iterate decides
+      faseVerdade(a, sh);
+      if (!barreira(a, ep)) return;
+      auto rbVerd = [&](int b) {
+        return (double)d.rhsBolhaF[b] - (__ldcg(&d.facesB[b]) * __ldcg(&d.yB[b]) - (double)__ldcg(&a.accV[b]) / ESC);
+      };
+      somasGlobais(a, nAt, [&](int b) { const double v = rbVerd(b); return v * v; }, [](int) { return 0.0; }, sh, somas);
+      normaVerd = sqrt(somas[0] + somas[2]);
+      if (!(normaVerd <= a.tol * norma0) && it < a.iteracoes - 1) {
+        // replacement: r (water) was rewritten by faseVerdade, the bubble rows follow; CG
+        // restarts from the true residual
+        fim = false;
+        reinicio = true;
+        trocas++;
+        norma = normaVerd;
+        if (blockIdx.x == 0)
+          for (int k = threadIdx.x; k < nAt; k += TF) {
+            const int b = __ldcg(&a.ativos[k]);
+            d.rb[b] = rbVerd(b);
+          }
+        if (!barreira(a, ep)) return;  // rb visible before the spread
+      }
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       if (it + 1 < 1024) d.esc->normas[it + 1] = norma;
       d.esc->iters = it + 1;
@@ -1814,15 +1939,35 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     escala = (a.escalar && norma > 0) ? (float)(1.0 / norma) : 1.0f;
     if (blockIdx.x == 0)
       for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) d.accB[b] = 0;
-    if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, zo, zc}, sh, secaoDensa)) return;
+    if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, zo, reinicio ? nullptr : zc}, sh, secaoDensa))
+      return;
     cz ^= 1;
     cp ^= 1;
-    primeira = false;
+    primeira = reinicio;
+    if (reinicio) {  // r.z of the restart (the first iteration's form)
+      somasGlobais(a, nAt, [&](int b) { return __ldcg(&d.rb[b]) * zbAtual(b); }, [](int) { return 0.0; }, sh, somas);
+      rz = somas[0] + somas[2];
+    }
   }
-  // ---- end: q = 0 off water; bubbles hand back their pressure
+  // ---- end: q = 0 off water (the FP64 iterate rounded on water); bubbles hand back their
+  // pressure; the solve's convergence record
   if (!barreira(a, ep)) return;
-  for (int c = gt0; c < N; c += GT)
+  for (int c = gt0; c < N; c += GT) {
     if (d.tipo[c] != AGUA) d.q[c] = 0.0f;
+    else if (a.q64) d.q[c] = (float)__ldcg(a.q64 + c);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    Escalares* e = d.esc;
+    const bool ok = a.q64 && normaVerd <= a.tol * norma0;
+    e->normaVerd = a.q64 ? normaVerd : -1.0;
+    e->convergiu = ok ? 1 : 0;
+    e->trocas = trocas;
+    e->solves++;
+    if (a.q64 && !ok) e->capados++;
+    e->itersAcum += itersFeitas;
+    e->trocasAcum += trocas;
+    if (a.q64 && norma0 > 0 && normaVerd / norma0 > e->maxRel) e->maxRel = normaVerd / norma0;
+  }
   if (blockIdx.x == 0)
     for (int k = threadIdx.x; k < nAt; k += TF) {
       int b = __ldcg(&a.ativos[k]);
@@ -1890,7 +2035,9 @@ Fundido* criarFundido(Pcg* p) {
          cudaMalloc(&f->nAtivos, sizeof(int)) == cudaSuccess && cudaMalloc(&f->p2, N * 4) == cudaSuccess &&
          cudaMalloc(&f->z2, N * 4) == cudaSuccess && cudaMalloc(&f->xc, nLc * 4) == cudaSuccess &&
          cudaMalloc(&f->bc, nLc * 4) == cudaSuccess && cudaMalloc(&f->op, N * sizeof(uint16_t)) == cudaSuccess &&
-         cudaMalloc(&f->rotB, N * sizeof(unsigned long long)) == cudaSuccess;
+         cudaMalloc(&f->rotB, N * sizeof(unsigned long long)) == cudaSuccess &&
+         cudaMalloc(&f->q64, N * sizeof(double)) == cudaSuccess &&
+         cudaMalloc(&f->accV, MAX_BOLHAS * sizeof(long long)) == cudaSuccess;
     // Wall blocks are skipped on levels of at least two full rounds of the grid's warps (a
     // tank atlas's finest levels): there the flags' one extra load per warp and pass is paid
     // back; a level of one round (the 450k-cell scene's) keeps no flags.
@@ -1943,15 +2090,23 @@ void destruirFundido(Fundido* f) {
   if (!f) return;
   void* ps[] = {f->niveis, f->parc, f->bar, f->erro, f->accZ, f->zb2, f->pb2, f->ativos,
                 f->nAtivos, f->p2, f->z2, f->xc, f->bc, f->perfil, f->op, f->rotB, f->mSecao, f->wSecao, f->wInv, f->nW,
-                f->densoG, f->solidos};
+                f->densoG, f->solidos, f->q64, f->accV};
   for (void* q : ps)
     if (q) cudaFree(q);
   delete f;
 }
 
-int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s) {
+// Queues the solve on `s` and returns without waiting: the iteration count, the residual history
+// and the convergence record stay on the device (Escalares), and a bounded wait that gave up
+// leaves f->erro set for erroFundido to report.  Nothing here waits for the device, so a frame
+// of substeps can be captured in a CUDA graph.
+int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, int precond,
+                           cudaStream_t s) {
   Fundido* f = p->fundido;
   Args a{};
+  a.bloco = precond == TQ_PRECOND_BLOCK ? 1 : 0;
+  a.q64 = tol > 0 ? f->q64 : nullptr;
+  a.accV = f->accV;
   a.d = d;
   a.L = p->L;
   a.Lc = f->Lc;
@@ -1992,7 +2147,8 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   cudaMemsetAsync(d.celsB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
   cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
   cudaMemsetAsync(f->bar, 0, 2 * sizeof(unsigned), s);
-  cudaMemsetAsync(f->erro, 0, sizeof(int), s);
+  // f->erro is not cleared here: a solve that gave up keeps it set until erroFundido reads it,
+  // and every later solve of the frame then stops at its first barrier instead of waiting.
   // The levels that skip wall blocks start the solve with their snapshots and right side at 0,
   // and with level 0 so do both z vectors (a pass never writes anything else off water).
   for (int l = 0; l < f->Lc; l++) {
@@ -2010,19 +2166,21 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   contarLancamento();
   cudaError_t e = cudaLaunchCooperativeKernel(f->kern, dim3(f->G), dim3(TF), args, f->smem, s);
   if (e != cudaSuccess) return TQ_E_CUDA;
-  int h[2] = {0, 0};
-  if (cudaMemcpyAsync(&h[0], f->erro, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaMemcpyAsync(&h[1], &d.esc->iters, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return TQ_E_CUDA;
-  if (h[0]) return TQ_E_TIMEOUT;
-  p->iters = h[1];
-  p->normas.resize(h[1] + 1);
-  if (cudaMemcpyAsync(p->normas.data(), d.esc->normas, sizeof(double) * (h[1] + 1), cudaMemcpyDeviceToHost, s) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return TQ_E_CUDA;
   return TQ_OK;
+}
+
+// TQ_E_TIMEOUT when a solve since the last call gave up on a bounded wait (the flag is cleared),
+// else TQ_OK.  Waits for the stream.
+int erroFundido(Fundido* f, cudaStream_t s) {
+  if (!f) return TQ_OK;
+  int h = 0;
+  if (cudaMemcpyAsync(&h, f->erro, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return TQ_E_CUDA;
+  if (!h) return TQ_OK;
+  if (cudaMemsetAsync(f->erro, 0, sizeof(int), s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+    return TQ_E_CUDA;
+  return TQ_E_TIMEOUT;
 }
 
 }  // namespace tq

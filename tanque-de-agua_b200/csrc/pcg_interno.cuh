@@ -22,8 +22,8 @@ struct Pcg {
   uint8_t* vizL[MAX_NIVEIS];
   void *bL[MAX_NIVEIS], *xL[MAX_NIVEIS], *tmpL[MAX_NIVEIS];  // 4 bytes per element allocated
   uint8_t* vizOp;
-  std::vector<double> normas;
-  int iters = 0;
+  double* q64 = nullptr;  // the plain engine's FP64 iterate (tolerance mode), allocated on first use
+  const int* parar = nullptr;  // the running plain solve's stop flag (NivelDev::parar)
   size_t smemGrosso = 0;
   Fundido* fundido = nullptr;
 };
@@ -31,7 +31,9 @@ struct Pcg {
 // pcg_fundido.cu
 Fundido* criarFundido(Pcg* p);
 void destruirFundido(Fundido* f);
-int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, cudaStream_t s);
+int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, int precond,
+                           cudaStream_t s);
+int erroFundido(Fundido* f, cudaStream_t s);
 void perfilFundido(Fundido* f, bool ligar);
 int lerPerfilFundido(Fundido* f, unsigned long long* out, int cap);
 

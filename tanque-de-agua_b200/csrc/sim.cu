@@ -3,6 +3,7 @@
 // and error reporting.  Every entry point returns a status and never throws.
 #include <array>
 #include <atomic>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -77,7 +78,13 @@ struct tq_sim {
   std::vector<std::array<int, 8>> regSub;
   std::vector<std::array<int, 2>> regAr;
   std::array<int, 8>* atual = nullptr;
-  long long itersTotal = 0;
+  long long itersBase = 0;  // Escalares::itersAcum when timing started
+  // tq_advance_graph: the substeps of a frame captured once and replayed; valid for the same dt
+  // and substep count while the live particle count stays within the captured launch bound
+  cudaGraph_t grafo = nullptr;
+  cudaGraphExec_t grafoExec = nullptr;
+  double grafoDt = 0, grafoG[2] = {0, 0};  // gravity is a kernel argument baked into the graph
+  int grafoSub = 0, grafoN = -1;
 };
 
 namespace {
@@ -173,9 +180,8 @@ int subpasso(tq_sim* s, double dt) {
   lancarClassificar(d, dt, s->o.tau_density, st);                          // #classificar
   if (ar) lancarLadoDireitoBolhas(d, dt, st);                              // #ladoDireitoDasBolhas
   marca(s, 4);
-  int r = resolverPressao(s->pcg, d, s->o.iterations, s->o.tolerance, ar, st);  // #pressao
+  int r = resolverPressao(s->pcg, d, s->o.iterations, s->o.tolerance, ar, s->o.preconditioner, st);  // #pressao
   if (r) return r == TQ_E_CUDA ? falha(r, "pressure solve failed") : r;
-  if (s->timing) s->itersTotal += itersPcg(s->pcg);
   lancarPosPressao(d, dt, ar, st);
   marca(s, 5);
   lancarGradiente(d, st);                                                  // #gradiente
@@ -284,6 +290,8 @@ int tq_create(const tq_options* o, tq_sim** out) {
   if (o->p2g_mode != TQ_P2G_FIXED) return falha(TQ_E_ARG, "the CUDA library implements TQ_P2G_FIXED only");
   if (o->precision < TQ_PREC_FP32 || o->precision > TQ_PREC_BF16) return falha(TQ_E_ARG, "bad precision");
   if (o->engine != TQ_ENGINE_PLAIN && o->engine != TQ_ENGINE_FUSED) return falha(TQ_E_ARG, "bad engine");
+  if (o->preconditioner != TQ_PRECOND_REFERENCE && o->preconditioner != TQ_PRECOND_BLOCK)
+    return falha(TQ_E_ARG, "bad preconditioner");
   int st = iniciarCuda(o->device);
   if (st) return st;
   tq_sim* s = new (std::nothrow) tq_sim();
@@ -360,6 +368,8 @@ int tq_create(const tq_options* o, tq_sim** out) {
 int tq_destroy(tq_sim* s) {
   if (!s) return TQ_OK;
   if (s->s) cudaStreamSynchronize(s->s);
+  if (s->grafoExec) cudaGraphExecDestroy(s->grafoExec);
+  if (s->grafo) cudaGraphDestroy(s->grafo);
   destruirPcg(s->pcg);
   destruirRastreador(s->ar);
   for (void* p : s->alocados) cudaFree(p);
@@ -479,20 +489,28 @@ int tq_reset_air(tq_sim* s) {
   return TQ_OK;
 }
 
+// The end of tq_substep / tq_advance: compaction, launch errors, and a fused solve that gave up
+// on a bounded wait (waits for the stream once).
+static int fimDePasso(tq_sim* s) {
+  compactar(s);
+  CK(cudaGetLastError());
+  int r = erroPcg(s->pcg, s->s);
+  if (r == TQ_E_TIMEOUT) return falha(r, "pressure solve: a grid barrier wait gave up");
+  if (r) return falhaCuda(cudaGetLastError(), "pressure solve");
+  return TQ_OK;
+}
+
 int tq_substep(tq_sim* s, double dt) {
   if (!s) return falha(TQ_E_ARG, "null handle");
   if (!(dt > 0)) return falha(TQ_E_ARG, "dt must be > 0");
   int r = subpasso(s, dt);
   if (r) return r;
-  compactar(s);
-  CK(cudaGetLastError());
-  return TQ_OK;
+  return fimDePasso(s);
 }
 
 int tq_advance(tq_sim* s, double dt, int32_t sub) {
   if (!s) return falha(TQ_E_ARG, "null handle");
   if (!(dt > 0) || sub < 1) return falha(TQ_E_ARG, "need dt > 0 and substeps >= 1");
-  std::vector<double> tempos;
   if (s->o.air) {
     int r = tq_update_air(s);
     if (r) return r;
@@ -502,9 +520,53 @@ int tq_advance(tq_sim* s, double dt, int32_t sub) {
     int r = subpasso(s, d);
     if (r) return r;
   }
-  compactar(s);
-  CK(cudaGetLastError());
-  return TQ_OK;
+  return fimDePasso(s);
+}
+
+int tq_advance_graph(tq_sim* s, double dt, int32_t sub) {
+  if (!s) return falha(TQ_E_ARG, "null handle");
+  if (!(dt > 0) || sub < 1) return falha(TQ_E_ARG, "need dt > 0 and substeps >= 1");
+  if (motorPcg(s->pcg) == TQ_ENGINE_PLAIN && s->o.tolerance > 0)
+    return falha(TQ_E_STATE, "the plain engine reads its stop flag on the host in tolerance mode: not capturable");
+  if (s->o.air) {
+    int r = tq_update_air(s);
+    if (r) return r;
+  }
+  const bool timing = s->timing;
+  if (!s->grafoExec || s->grafoDt != dt || s->grafoSub != sub || s->nHint > s->grafoN ||
+      s->grafoG[0] != s->o.gravity[0] || s->grafoG[1] != s->o.gravity[1]) {
+    if (s->grafoExec) cudaGraphExecDestroy(s->grafoExec);
+    if (s->grafo) cudaGraphDestroy(s->grafo);
+    s->grafoExec = nullptr;
+    s->grafo = nullptr;
+    s->timing = false;  // stage events are not recorded into the graph
+    CK(cudaStreamBeginCapture(s->s, cudaStreamCaptureModeThreadLocal));
+    int r = TQ_OK;
+    for (int k = 0; k < sub && !r; k++) r = subpasso(s, dt / sub);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->s, &g);
+    s->timing = timing;
+    if (r) {
+      if (g) cudaGraphDestroy(g);
+      return r;
+    }
+    if (e != cudaSuccess) return falhaCuda(e, "capturing the frame's substeps");
+    e = cudaGraphInstantiate(&s->grafoExec, g, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      s->grafoExec = nullptr;
+      return falhaCuda(e, "instantiating the frame's graph");
+    }
+    s->grafo = g;
+    s->grafoDt = dt;
+    s->grafoSub = sub;
+    s->grafoN = s->nHint;
+    s->grafoG[0] = s->o.gravity[0];
+    s->grafoG[1] = s->o.gravity[1];
+  }
+  contarLancamento();
+  CK(cudaGraphLaunch(s->grafoExec, s->s));
+  return fimDePasso(s);
 }
 
 int tq_count(tq_sim* s, int32_t* n) {
@@ -667,7 +729,31 @@ int tq_get_scalar(tq_sim* s, int32_t w, double* out) {
     case TQ_SCALAR_LAUNCHES: *out = (double)g_lancamentos.load(); return TQ_OK;
     case TQ_SCALAR_PRIMEIRA: *out = primeiraRastreador(s->ar); return TQ_OK;
     case TQ_SCALAR_TIPOS_PRONTOS: *out = s->tiposProntos ? 1 : 0; return TQ_OK;
-    case TQ_SCALAR_PCG_ITERS: *out = itersPcg(s->pcg); return TQ_OK;
+    case TQ_SCALAR_PCG_ITERS: {
+      int v = 0;
+      int st = baixar(s, &v, &s->d.esc->iters, sizeof v);
+      if (st) return st;
+      *out = v;
+      return TQ_OK;
+    }
+    case TQ_SCALAR_PCG_TRUE_RES: return baixar(s, out, &s->d.esc->normaVerd, sizeof(double));
+    case TQ_SCALAR_PCG_CONVERGED:
+    case TQ_SCALAR_SOLVES:
+    case TQ_SCALAR_SOLVES_CAPPED:
+    case TQ_SCALAR_SOLVE_ITERS:
+    case TQ_SCALAR_SOLVE_MAX_REL:
+    case TQ_SCALAR_SOLVE_REPLACEMENTS: {
+      Escalares e;
+      int st = baixar(s, &e, s->d.esc, offsetof(Escalares, normas));
+      if (st) return st;
+      *out = w == TQ_SCALAR_PCG_CONVERGED  ? (double)e.convergiu
+             : w == TQ_SCALAR_SOLVES       ? (double)e.solves
+             : w == TQ_SCALAR_SOLVES_CAPPED ? (double)e.capados
+             : w == TQ_SCALAR_SOLVE_ITERS  ? (double)e.itersAcum
+             : w == TQ_SCALAR_SOLVE_MAX_REL ? e.maxRel
+                                            : (double)e.trocasAcum;
+      return TQ_OK;
+    }
     case TQ_SCALAR_GRAVITY_X: *out = s->o.gravity[0]; return TQ_OK;
     case TQ_SCALAR_GRAVITY_Y: *out = s->o.gravity[1]; return TQ_OK;
     case TQ_SCALAR_PCG_RES0:
@@ -689,6 +775,14 @@ int tq_set_scalar(tq_sim* s, int32_t w, double v) {
     case TQ_SCALAR_TIPOS_PRONTOS: s->tiposProntos = v != 0; return TQ_OK;
     case TQ_SCALAR_GRAVITY_X: s->o.gravity[0] = v; return TQ_OK;
     case TQ_SCALAR_GRAVITY_Y: s->o.gravity[1] = v; return TQ_OK;
+    case TQ_SCALAR_SOLVES: {  // 0 resets the accumulated solve statistics
+      if (v != 0) return falha(TQ_E_ARG, "TQ_SCALAR_SOLVES can only be reset to 0");
+      Escalares* e = s->d.esc;
+      CK(cudaMemsetAsync(&e->solves, 0, sizeof e->solves + sizeof e->capados + sizeof e->itersAcum +
+                                            sizeof e->trocasAcum + sizeof e->maxRel, s->s));
+      CK(cudaStreamSynchronize(s->s));
+      return TQ_OK;
+    }
     case TQ_SCALAR_VMAX: {
       unsigned long long b;
       std::memcpy(&b, &v, 8);
@@ -703,7 +797,8 @@ int tq_set_scalar(tq_sim* s, int32_t w, double v) {
 int tq_last_norms(tq_sim* s, double* out, int32_t cap, int32_t* n) {
   if (!s) return falha(TQ_E_ARG, "null handle");
   std::vector<double> tmp(1024);
-  int k = normasPcg(s->pcg, tmp.data(), 1024);
+  int k = normasPcg(s->pcg, s->d, tmp.data(), 1024, s->s);
+  if (k < 0) return falhaCuda(cudaGetLastError(), "reading the residual history");
   if (n) *n = k;
   if (out)
     for (int i = 0; i < k && i < cap; i++) out[i] = tmp[i];
@@ -731,7 +826,9 @@ int tq_set_timing(tq_sim* s, int32_t on) {
   s->regSub.clear();
   s->regAr.clear();
   s->atual = nullptr;
-  s->itersTotal = 0;
+  long long base = 0;
+  CK(cudaMemcpy(&base, &s->d.esc->itersAcum, sizeof base, cudaMemcpyDeviceToHost));
+  s->itersBase = base;
   return TQ_OK;
 }
 
@@ -756,7 +853,9 @@ int tq_get_timing(tq_sim* s, double* ms, int32_t cap, int32_t* n) {
     }
     for (auto& r : s->regAr) v[7] += dur(r[0], r[1]);
     v[8] = completos;
-    v[9] = (double)s->itersTotal;
+    long long acum = 0;
+    CK(cudaMemcpy(&acum, &s->d.esc->itersAcum, sizeof acum, cudaMemcpyDeviceToHost));
+    v[9] = (double)(acum - s->itersBase);
     v[10] = (double)s->regAr.size();
     cudaGetLastError();
   }
@@ -779,8 +878,8 @@ int tq_get_phase_trace(tq_sim* s, uint64_t* out, int32_t cap, int32_t* n) {
 
 // ---------------------------------------------------------------- standalone solver
 int tq_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float* div, float* q, int32_t iterations,
-                      double tolerance, const tq_bubbles* b, int32_t precision, int32_t engine, double* norms,
-                      int32_t norms_cap, int32_t* n_norms) {
+                      double tolerance, const tq_bubbles* b, int32_t precision, int32_t engine, int32_t precond,
+                      double* norms, int32_t norms_cap, int32_t* n_norms, tq_solve_info* info) {
   if (nx < 3 || ny < 3 || !tipo || !div || !q || iterations < 1 || iterations > 1000)
     return falha(TQ_E_ARG, "bad arguments");
   if (b && (!b->rotulo || !b->rhs || !b->y)) return falha(TQ_E_ARG, "bad bubbles");
@@ -791,6 +890,7 @@ int tq_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float* 
   o.capacity = 1;
   o.iterations = iterations;
   o.tolerance = tolerance;
+  o.preconditioner = precond;
   tq_sim* s = nullptr;
   int st = tq_create(&o, &s);
   if (st) return st;
@@ -810,18 +910,33 @@ int tq_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float* 
         cudaMemcpyAsync(d.yBolhaF, b->y, MAX_BOLHAS * 4, cudaMemcpyHostToDevice, s->s) != cudaSuccess)
       return fim(falha(TQ_E_CUDA, "upload failed"));
   }
-  st = resolverPressao(s->pcg, d, iterations, tolerance, b != nullptr, s->s);
+  st = resolverPressao(s->pcg, d, iterations, tolerance, b != nullptr, precond, s->s);
   if (st) return fim(st == TQ_E_CUDA ? falha(st, "pressure solve failed") : st);
+  st = erroPcg(s->pcg, s->s);
+  if (st) return fim(st == TQ_E_TIMEOUT ? falha(st, "pressure solve: a grid barrier wait gave up") : st);
   if (cudaMemcpyAsync(q, d.q, N * 4, cudaMemcpyDeviceToHost, s->s) != cudaSuccess)
     return fim(falha(TQ_E_CUDA, "download failed"));
   if (b && cudaMemcpyAsync(b->y, d.yBolhaF, MAX_BOLHAS * 4, cudaMemcpyDeviceToHost, s->s) != cudaSuccess)
     return fim(falha(TQ_E_CUDA, "download failed"));
   if (cudaStreamSynchronize(s->s) != cudaSuccess) return fim(falha(TQ_E_CUDA, "solve failed"));
   std::vector<double> tmp(1024);
-  int k = normasPcg(s->pcg, tmp.data(), 1024);
+  int k = normasPcg(s->pcg, s->d, tmp.data(), 1024, s->s);
+  if (k < 0) return fim(falha(TQ_E_CUDA, "reading the residual history"));
   if (n_norms) *n_norms = k;
   if (norms)
     for (int i = 0; i < k && i < norms_cap; i++) norms[i] = tmp[i];
+  if (info) {
+    Escalares e;
+    if (cudaMemcpy(&e, s->d.esc, offsetof(Escalares, normas), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fim(falha(TQ_E_CUDA, "reading the solve record"));
+    info->iterations = e.iters;
+    info->converged = e.convergiu;
+    info->replacements = e.trocas;
+    info->pad = 0;
+    info->residual0 = e.norma0;
+    info->residual = e.norma;
+    info->true_residual = e.normaVerd;
+  }
   return fim(TQ_OK);
 }
 

@@ -25,6 +25,7 @@ TQ_E_STATE = -7
 TQ_PREC_FP32, TQ_PREC_FP16, TQ_PREC_BF16 = 0, 1, 2
 TQ_ENGINE_PLAIN, TQ_ENGINE_FUSED = 0, 1
 TQ_P2G_FLOAT, TQ_P2G_FIXED = 0, 1
+TQ_PRECOND_REFERENCE, TQ_PRECOND_BLOCK = 0, 1
 
 # enum tq_field (include/tanque.h) -> (numpy dtype, size in units of N / nu / nv / 4096 / sdf)
 CAMPOS_ENUM = {
@@ -38,6 +39,9 @@ TQ_SCALAR_VMAX, TQ_SCALAR_PRIMEIRA, TQ_SCALAR_TIPOS_PRONTOS = 0, 1, 2
 TQ_SCALAR_PCG_ITERS, TQ_SCALAR_PCG_RES0, TQ_SCALAR_PCG_RES = 3, 4, 5
 TQ_SCALAR_LAUNCHES = 6
 TQ_SCALAR_GRAVITY_X, TQ_SCALAR_GRAVITY_Y = 7, 8
+TQ_SCALAR_PCG_TRUE_RES, TQ_SCALAR_PCG_CONVERGED = 9, 10
+TQ_SCALAR_SOLVES, TQ_SCALAR_SOLVES_CAPPED, TQ_SCALAR_SOLVE_ITERS = 11, 12, 13
+TQ_SCALAR_SOLVE_MAX_REL, TQ_SCALAR_SOLVE_REPLACEMENTS = 14, 15
 
 
 class TqOptions(C.Structure):
@@ -46,7 +50,7 @@ class TqOptions(C.Structure):
         ("iterations", C.c_int32), ("air", C.c_int32), ("tau_density", C.c_double),
         ("surface_tension", C.c_double), ("tolerance", C.c_double), ("precision", C.c_int32),
         ("engine", C.c_int32), ("p2g_mode", C.c_int32), ("capacity", C.c_int32),
-        ("device", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("device", C.c_int32), ("preconditioner", C.c_int32), ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -59,6 +63,13 @@ class TqTool(C.Structure):
 
 class TqBubbles(C.Structure):
     _fields_ = [("rotulo", C.c_void_p), ("rhs", C.c_void_p), ("y", C.c_void_p)]
+
+
+class TqSolveInfo(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32), ("converged", C.c_int32), ("replacements", C.c_int32), ("pad", C.c_int32),
+        ("residual0", C.c_double), ("residual", C.c_double), ("true_residual", C.c_double),
+    ]
 
 
 class ErroTanque(RuntimeError):
@@ -94,11 +105,12 @@ ASSINATURAS = {
     "get_scalar": (C.c_int, [_P, _I, C.POINTER(_D)]),
     "set_scalar": (C.c_int, [_P, _I, _D]),
     "last_norms": (C.c_int, [_P, C.POINTER(_D), _I, C.POINTER(_I)]),
-    "solve_pressure": (C.c_int, [_I, _I, _P, _P, _P, _I, _D, C.POINTER(TqBubbles), _I, _I,
-                                 C.POINTER(_D), _I, C.POINTER(_I)]),
+    "solve_pressure": (C.c_int, [_I, _I, _P, _P, _P, _I, _D, C.POINTER(TqBubbles), _I, _I, _I,
+                                 C.POINTER(_D), _I, C.POINTER(_I), C.POINTER(TqSolveInfo)]),
     "vcycle": (C.c_int, [_I, _I, _P, _P, _P, _I]),
 }
 SO_PRODUTO = {
+    "advance_graph": (C.c_int, [_P, _D, _I]),
     "sync": (C.c_int, [_P]),
     "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "set_timing": (C.c_int, [_P, _I]),
@@ -180,6 +192,7 @@ def opcoes_padrao(nx: int, ny: int, h: float, **kw) -> TqOptions:
     o.p2g_mode = TQ_P2G_FIXED
     o.capacity = 0
     o.device = 0
+    o.preconditioner = TQ_PRECOND_REFERENCE
     for k, v in kw.items():
         if k == "gravity":
             o.gravity[0], o.gravity[1] = v

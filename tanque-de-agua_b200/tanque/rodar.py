@@ -2,7 +2,7 @@
 times of the last frame or, with --phases, the fused solver's per-phase times of one substep.
 
     python -m tanque.rodar [--scene ultra|atlas] [--frames F] [--substeps S] [--precision 0|1|2]
-                           [--engine 0|1] [--tolerance T] [--phases]
+                           [--engine 0|1] [--precond 0|1] [--tolerance T] [--phases]
 
 `ultra` is the 450k-cell scene of the throughput benchmark; `atlas` is the largest atlas of
 the 256-tank batch (tanque.lote).  Frames are 1/60 s split into S substeps (default: 14 for
@@ -60,6 +60,7 @@ def main(argv=None):
     ap.add_argument("--substeps", type=int, default=0, help="0: 14 (ultra) or the capillary limit (atlas)")
     ap.add_argument("--precision", type=int, default=1, help="0 FP32, 1 FP16, 2 BF16 V-cycle storage")
     ap.add_argument("--engine", type=int, default=1, help="0 plain, 1 fused")
+    ap.add_argument("--precond", type=int, default=1, help="0 reference, 1 block preconditioner")
     ap.add_argument("--tolerance", type=float, default=1e-6)
     ap.add_argument("--phases", action="store_true", help="per-phase times of one more substep (fused engine)")
     args = ap.parse_args(argv)
@@ -72,15 +73,19 @@ def main(argv=None):
         at = montar_atlas(Cena, [t[k] for k in agrupar(t)[0]], h)
         cena, agua = at["cena"], at["particulas"]
         sub = args.substeps or math.ceil((1 / 60) / passo_maximo(h, cena.ny * h) - 1e-9)
-    sim = SimulacaoGPU(cena, {"tolerance": args.tolerance, "iterations": 200, "precision": args.precision,
-                              "engine": args.engine})
+    sim = SimulacaoGPU(cena, {"tolerance": args.tolerance, "iterations": 1000, "precision": args.precision,
+                              "engine": args.engine, "preconditioner": args.precond})
     sim.adicionar(agua, False)
     for q in range(args.frames):
         if q == args.frames - 1:
             sim.tempos(True)
         sim.avancar(1 / 60, sub)
     out = {"scene": args.scene, "grid": [cena.nx, cena.ny], "particles": sim.n, "frames": args.frames,
-           "substeps": sub, "last_frame_ms": sim.tempos()}
+           "substeps": sub, "last_frame_ms": sim.tempos(),
+           "solves": {"n": sim.escalar(_abi.TQ_SCALAR_SOLVES), "capped": sim.escalar(_abi.TQ_SCALAR_SOLVES_CAPPED),
+                      "iters": sim.escalar(_abi.TQ_SCALAR_SOLVE_ITERS),
+                      "max_true_rel": sim.escalar(_abi.TQ_SCALAR_SOLVE_MAX_REL),
+                      "replacements": sim.escalar(_abi.TQ_SCALAR_SOLVE_REPLACEMENTS)}}
     if args.phases:
         lig = _abi.carregar()
         lig.lib.tq_get_phase_trace.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.c_int32, C.POINTER(C.c_int32)]
@@ -94,7 +99,9 @@ def main(argv=None):
         d = np.diff(np.array(buf[:n.value], dtype=np.int64)) / 1000.0
         Lc = secao(niveis(cena.nx, cena.ny))
         per = 2 + 5 * Lc + 1
-        fim = len(d) - 3  # the last iteration runs DA and B only, then the closing barrier
+        # the last iteration runs DA and B only, then (tolerance mode) the true residual, then
+        # the closing barrier
+        fim = len(d) - (4 if args.tolerance > 0 else 3)
         ini = fim - (it - 1) * per
         if it > 1 and ini >= 0:
             med = np.median(d[ini:fim].reshape(it - 1, per), axis=0)

@@ -114,6 +114,11 @@ class Simulacao:
         self._lig("advance", self._h, float(dt), int(subpassos))
         self._andou = True
 
+    def avancarGrafo(self, dt: float, subpassos: int = 1):
+        """avancar with the substeps replayed from a CUDA graph (tq_advance_graph): same bits."""
+        self._lig("advance_graph", self._h, float(dt), int(subpassos))
+        self._andou = True
+
     def atualizarAr(self):
         self._lig("update_air", self._h)
 
@@ -277,10 +282,11 @@ class SimulacaoGPU(Simulacao):
 
 
 def resolver_pressao(tipo, div, q, iteracoes=ITERACOES_PCG, tolerancia=0.0, bolhas=None, precisao=0, motor=0,
-                     ligacao: _abi.Ligacao | None = None):
+                     precond=0, info: dict | None = None, ligacao: _abi.Ligacao | None = None):
     """resolverPCG (js/pressao-cpu.js:296-402) through tq_solve_pressure; q is updated in place.
 
     bolhas: optional dict(rotulo=uint32[N], rhs=float32[4096], y=float32[4096]); y is updated.
+    precond: TQ_PRECOND_*.  info: optional dict, filled with tq_solve_info's fields.
     Returns the residual-norm history."""
     lig = ligacao or _abi.carregar()
     ny, nx = tipo.shape
@@ -299,8 +305,11 @@ def resolver_pressao(tipo, div, q, iteracoes=ITERACOES_PCG, tolerancia=0.0, bolh
             C.byref(b) if b is not None else None]
     if lig.prefixo == "tq_":
         args += [precisao, motor]
-    args += [normas, 1024, C.byref(nn)]
+    inf = _abi.TqSolveInfo()
+    args += [precond, normas, 1024, C.byref(nn), C.byref(inf)]
     lig("solve_pressure", *args)
+    if info is not None:
+        info.update({k: getattr(inf, k) for k, _ in _abi.TqSolveInfo._fields_ if k != "pad"})
     return np.array(normas[: nn.value])
 
 

@@ -20,8 +20,8 @@ _P, _I, _D = C.c_void_p, C.c_int32, C.c_double
 ASSINATURAS_ORACULO = dict(_abi.ASSINATURAS)
 ASSINATURAS_ORACULO.update({
     "create_fp64": (C.c_int, [C.POINTER(_abi.TqOptions), C.POINTER(_P)]),
-    "solve_pressure": (C.c_int, [_I, _I, _P, _P, _P, _I, _D, C.POINTER(_abi.TqBubbles), C.POINTER(_D), _I,
-                                 C.POINTER(_I)]),
+    "solve_pressure": (C.c_int, [_I, _I, _P, _P, _P, _I, _D, C.POINTER(_abi.TqBubbles), _I, C.POINTER(_D), _I,
+                                 C.POINTER(_I), C.POINTER(_abi.TqSolveInfo)]),
     "vcycle": (C.c_int, [_I, _I, _P, _P, _P]),
     "scene_new": (_P, [_I, _I, _D]),
     "scene_free": (None, [_P]),
@@ -128,9 +128,10 @@ def mancha_oraculo(particulas, nx, ny, h, largura, altura):
     return out.reshape(5, altura, largura)
 
 
-def resolver_pressao_oraculo(tipo, div, q, iteracoes=3, tolerancia=0.0, bolhas=None):
+def resolver_pressao_oraculo(tipo, div, q, iteracoes=3, tolerancia=0.0, bolhas=None, precond=0, info=None):
     from tanque.simulacao import resolver_pressao
-    return resolver_pressao(tipo, div, q, iteracoes, tolerancia, bolhas, ligacao=carregar_oraculo())
+    return resolver_pressao(tipo, div, q, iteracoes, tolerancia, bolhas, precond=precond, info=info,
+                            ligacao=carregar_oraculo())
 
 
 def ciclo_v_oraculo(tipo, b):

@@ -38,6 +38,8 @@ def test_layout_das_estruturas():
     assert _abi.TqOptions.h.offset == 8
     assert _abi.TqOptions.gravity.offset == 16
     assert _abi.TqOptions.tolerance.offset == 56
+    assert _abi.TqOptions.preconditioner.offset == 84
+    assert C.sizeof(_abi.TqSolveInfo) == 40
     assert C.sizeof(_abi.TqTool) == 72
     assert C.sizeof(_abi.TqBubbles) == 24
 
