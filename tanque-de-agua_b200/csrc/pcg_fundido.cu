@@ -414,7 +414,9 @@ struct Reuniao {
 // A half-sweep reads no value that it writes.
 // Every snapshot holds x = 0 on cells that are not water (the passes store 0 there, the frame
 // outside the grid is 0), so a wall neighbour adds +0 and the sum needs no mask; only 1/k and
-// whether the cell changes come from the mask.
+// whether the cell changes come from the mask.  The exception is TQ_PRECOND_BLOCK's coarse
+// levels, whose masks close faces between two water cells across a thin wall: with `masc` the
+// neighbours the mask leaves out are dropped from the sum (masc is uniform over the grid).
 struct Moldura {
   float esq[4], dir[4];  // frame left / right of the lane's rows (k = 0 / k = 7)
   float bai[2], cim[2];  // frame below / above the lane's columns (g = 0 / g = 3), by column
@@ -422,7 +424,7 @@ struct Moldura {
 
 template <int COR>
 __device__ __forceinline__ void meiaReg(float (&x)[2][4], const float (&bq)[2][4], const float (&iq)[2][4],
-                                        const float (&at)[2][4], const Moldura& f) {
+                                        const float (&at)[2][4], const Moldura& f, const int (&v)[2][4], bool masc) {
   const int lane = threadIdx.x & 31, g = lane >> 3, k = lane & 7;
   float H[4];
 #pragma unroll
@@ -434,10 +436,17 @@ __device__ __forceinline__ void meiaReg(float (&x)[2][4], const float (&bq)[2][4
   for (int m = 0; m < 4; m++) {
     const int jc = (COR + 1 + m) & 1;  // the column of colour COR in row m
     const float y = x[1 - COR][m];
-    const float esq = jc ? y : (k == 0 ? f.esq[m] : H[m]);
-    const float dir = jc ? (k == 7 ? f.dir[m] : H[m]) : y;
-    const float baixo = m >= 1 ? x[1 - COR][m >= 1 ? m - 1 : 0] : (g >= 1 ? D : f.bai[jc]);
-    const float cima = m <= 2 ? x[1 - COR][m <= 2 ? m + 1 : 3] : (g <= 2 ? U : f.cim[jc]);
+    float esq = jc ? y : (k == 0 ? f.esq[m] : H[m]);
+    float dir = jc ? (k == 7 ? f.dir[m] : H[m]) : y;
+    float baixo = m >= 1 ? x[1 - COR][m >= 1 ? m - 1 : 0] : (g >= 1 ? D : f.bai[jc]);
+    float cima = m <= 2 ? x[1 - COR][m <= 2 ? m + 1 : 3] : (g <= 2 ? U : f.cim[jc]);
+    if (masc) {
+      const int mk = v[COR][m];
+      esq = (mk & 1) ? esq : 0.0f;
+      dir = (mk & 2) ? dir : 0.0f;
+      baixo = (mk & 4) ? baixo : 0.0f;
+      cima = (mk & 8) ? cima : 0.0f;
+    }
     const float sm = ((esq + dir) + baixo) + cima;
     const float q = x[COR][m];
     const float dlt = (sm + bq[COR][m]) * iq[COR][m] - q;
@@ -448,7 +457,7 @@ __device__ __forceinline__ void meiaReg(float (&x)[2][4], const float (&bq)[2][4
 // The VARREDURAS red-black sweeps (js/pressao-cpu.js:114-137) of the warp's block in registers;
 // v = neighbour mask | 16 water | 128 in grid, bq = right side; ordem 0 sweeps colour 0 first.
 __device__ __forceinline__ void varrerReg(float (&x)[2][4], const int (&v)[2][4], const float (&bq)[2][4],
-                                         const Moldura& f, int ordem) {
+                                         const Moldura& f, int ordem, bool masc) {
   float iq[2][4], at[2][4];
 #pragma unroll
   for (int c = 0; c < 2; c++)
@@ -461,8 +470,8 @@ __device__ __forceinline__ void varrerReg(float (&x)[2][4], const int (&v)[2][4]
   // rolled loop: the pass code stays small in the instruction cache, which each phase enters cold
 #pragma unroll 1
   for (int h = 0; h < 2 * VARREDURAS; h++) {
-    if (((h & 1) ^ ordem) == 0) meiaReg<0>(x, bq, iq, at, f);
-    else meiaReg<1>(x, bq, iq, at, f);
+    if (((h & 1) ^ ordem) == 0) meiaReg<0>(x, bq, iq, at, f, v, masc);
+    else meiaReg<1>(x, bq, iq, at, f, v, masc);
   }
 }
 
@@ -638,7 +647,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   for (int cr = 0; cr < 2; cr++)
 #pragma unroll
     for (int m = 0; m < 4; m++) mexe |= (v[cr][m] & 16) && (v[cr][m] & 15);
-  if (__any_sync(0xffffffffu, mexe)) varrerReg(x, v, bq, f, ordem);
+  if (__any_sync(0xffffffffu, mexe)) varrerReg(x, v, bq, f, ordem, a.bloco != 0);
   if (MODO == M_JUNTAR) {
     const float inv = 1.0f / ru.escala;
     float rv[2][4], zv[2][4];
@@ -860,14 +869,18 @@ __device__ __forceinline__ void faseRestringirR(const Args& a, int l, float* are
     {
       // residuals of the fine cells: every shared load of the lane's cells goes out before the
       // first store.  x is 0 off water and outside the grid, so the neighbour sum needs no
-      // mask; the residual is 0 off water.
+      // mask (but TQ_PRECOND_BLOCK's coarse masks can close a face between two water cells);
+      // the residual is 0 off water.
+      const bool masc = a.bloco != 0;
       float rv[KB];
 #pragma unroll
       for (int k = 0; k < KB; k++) {
         const int s = lane + 32 * k < RBn ? lane + 32 * k : 0;
         const float* xc = xs + (s / 66 + 1) * 68 + s % 66 + 1;
         const int vz = vs[s];
-        const float t = ((xc[-1] + xc[1]) + xc[-68]) + xc[68];
+        const float t = masc ? ((((vz & 1) ? xc[-1] : 0.0f) + ((vz & 2) ? xc[1] : 0.0f)) + ((vz & 4) ? xc[-68] : 0.0f)) +
+                                   ((vz & 8) ? xc[68] : 0.0f)
+                             : ((xc[-1] + xc[1]) + xc[-68]) + xc[68];
         rv[k] = (vz & 16) ? bs[s] - ((float)__popc(vz & 15) * xc[0] - t) : 0.0f;
       }
 #pragma unroll
@@ -915,7 +928,7 @@ struct NivelS {
 // One smoother pass over a level held in shared memory: the level's 16x16 blocks are taken in
 // turn by the CTA's warps, each sweeping its block in registers (varrerReg) from the snapshot
 // `src` and writing `dst`.
-__device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int ordem, int src, int dst) {
+__device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int ordem, int src, int dst, bool masc) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, gl = lane >> 3, k = lane & 7;
   const int nx = n.nx, ny = n.ny;
   const int nbx = (nx + desl + 15) >> 4, nby = (ny + desl + 15) >> 4;
@@ -952,7 +965,7 @@ __device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int
       f.bai[j] = okB ? F[src + gx + (oy - 1) * nx] : 0.0f;
       f.cim[j] = okT ? F[src + gx + (oy + 16) * nx] : 0.0f;
     }
-    varrerReg(x, v, bq, f, ordem);
+    varrerReg(x, v, bq, f, ordem, masc);
 #pragma unroll
     for (int cr = 0; cr < 2; cr++)
 #pragma unroll
@@ -1132,9 +1145,9 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
   for (int l = a.Lc; l < a.L - 1; l++) {
     const NivelS f = s[l];
     const NivelS g = s[l + 1];
-    passoS(F, U, f, 0, 0, f.xa, f.xb);
+    passoS(F, U, f, 0, 0, f.xa, f.xb, a.bloco != 0);
     marcaSecao(a, marcar);
-    passoS(F, U, f, 8, 0, f.xb, f.xa);
+    passoS(F, U, f, 8, 0, f.xb, f.xa, a.bloco != 0);
     marcaSecao(a, marcar);
     // restringir: residuals of the fine level into its free x buffer, then the 4x4 gathers.
     // Out-of-range and dry neighbours enter with weight or value 0, which adds +0 to a sum.
@@ -1317,9 +1330,9 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
     }
     __syncthreads();
     marcaSecao(a, marcar);
-    passoS(F, U, f, 8, 1, f.xa, f.xb);
+    passoS(F, U, f, 8, 1, f.xa, f.xb, a.bloco != 0);
     marcaSecao(a, marcar);
-    passoS(F, U, f, 0, 1, f.xb, f.xa);
+    passoS(F, U, f, 0, 1, f.xb, f.xa, a.bloco != 0);
     marcaSecao(a, marcar);
   }
   const NivelS t = s[a.Lc];

@@ -59,6 +59,56 @@ def test_tolerancia_verdadeira(lib_gpu, nome, precond, prec, motor):
     assert len(n_g) <= len(n_o) + folga
 
 
+def labirinto_sintetico(nx=210, ny=150, seed=7):
+    """A pressure problem with walls 2 cells thick (thinner than a cell from the third level
+    down, where the block preconditioner's face masks close faces between water cells) and
+    enclosed air pockets with labels >= 2."""
+    from tanque.constantes import AGUA, AR, SOLIDO
+    rng = np.random.default_rng(seed)
+    tipo = np.full((ny, nx), AGUA, np.uint8)
+    tipo[int(0.8 * ny):, :] = AR
+    for x0 in range(12, nx - 6, 14):  # vertical walls with a gap alternating bottom / top
+        tipo[2:ny - 2, x0:x0 + 2] = SOLIDO
+        g = 4 if (x0 // 14) % 2 else int(0.8 * ny) - 10
+        tipo[g:g + 6, x0:x0 + 2] = AGUA if g < int(0.8 * ny) else AR
+    tipo[:2, :] = tipo[-2:, :] = SOLIDO
+    tipo[:, :2] = tipo[:, -2:] = SOLIDO
+    rot = np.zeros((ny, nx), np.uint32)
+    rot[tipo == AR] = 1
+    jj, ii = np.mgrid[0:ny, 0:nx]
+    for k, (cx, cy, r) in enumerate([(30, 40, 5), (75, 60, 7), (130, 30, 4), (180, 80, 6)]):
+        bolha = ((ii - cx) ** 2 + (jj - cy) ** 2 < r * r) & (tipo == AGUA)
+        tipo[bolha] = AR
+        rot[bolha] = 2 + k
+    div = rng.standard_normal((ny, nx)).astype(np.float32)
+    div[tipo != AGUA] = 0
+    rhs = np.zeros(4096, np.float32)
+    rhs[2:6] = rng.standard_normal(4).astype(np.float32)
+    return tipo, div, dict(rotulo=rot.ravel(), rhs=rhs, y=np.zeros(4096, np.float32))
+
+
+@pytest.mark.parametrize("motor", MOTORES)
+@pytest.mark.parametrize("prec", PRECS)
+def test_bloco_paredes_finas(lib_gpu, prec, motor):
+    """The block preconditioner's coarse masks on thin walls: the GPU solve matches the oracle's
+    (q, y) and needs about as many iterations (a smoother that summed across a closed face
+    would diverge or crawl)."""
+    tipo, div, bol = labirinto_sintetico()
+    q_o = np.zeros(tipo.size, np.float32)
+    q_g = q_o.copy()
+    b_o = {k: v.copy() for k, v in bol.items()}
+    b_g = {k: v.copy() for k, v in bol.items()}
+    i_o, i_g = {}, {}
+    resolver_pressao_oraculo(tipo, div, q_o, 600, 1e-6, b_o, precond=_abi.TQ_PRECOND_BLOCK, info=i_o)
+    resolver_pressao(tipo, div, q_g, 600, 1e-6, b_g, precisao=prec, motor=motor, precond=_abi.TQ_PRECOND_BLOCK,
+                     info=i_g)
+    assert i_o["converged"] == 1 and i_g["converged"] == 1
+    assert erro_relativo(q_g, q_o) < 1e-4
+    assert erro_relativo(b_g["y"][2:6], b_o["y"][2:6]) < 1e-3
+    folga = 3 if prec == _abi.TQ_PREC_FP32 else 0.25 * i_o["iterations"]
+    assert i_g["iterations"] <= i_o["iterations"] + folga
+
+
 @pytest.mark.parametrize("motor", MOTORES)
 def test_bloco_converge_mais_depressa(lib_gpu, motor):
     """On a scene with trapped air the block preconditioner needs fewer iterations."""
