@@ -308,7 +308,8 @@ typedef struct tq_solve_info {
  * stops when the TRUE residual ||b - A q||, recomputed in FP64 from the FP64 iterate and the
  * bubble pressures, is <= tolerance * ||r0||, or at `iterations` (the cap).  The true residual
  * is recomputed whenever the recursive FP32 one meets the tolerance; if the true one does
- * not, it replaces the recursive one and CG restarts from it (residual replacement).
+ * not, it replaces the recursive one and CG goes on with the same search direction (residual
+ * replacement).
  * q is returned rounded to FP32, so b - A q of the returned float q carries their rounding
  * (about 1e-7 of |A| |q| per cell) on top of the reported true residual.
  * norms receives the recursive residual history (initial, then one per iteration).

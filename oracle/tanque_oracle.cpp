@@ -495,7 +495,8 @@ struct InfoPCG {
 // counterpart in the reference) keeps q in double during the solve and stops when the TRUE
 // residual ||b - A q|| (double, from the double iterate and the bubbles' y) is <= tol*||r0||,
 // or at the cap.  The true residual is recomputed when the recursive one meets the tolerance;
-// when the true one does not, it replaces the recursive one and CG restarts from it.
+// when the true one does not, it replaces the recursive one and the iteration goes on with the
+// same search direction (a residual replacement without restart).
 // precond = TQ_PRECOND_BLOCK replaces precondicionar (:352-361) by the block-diagonal form:
 // bubble rows z_b = r_b / faces_b, the V-cycle on the water alone (enclosed air stays air) with
 // coarse neighbour masks from the fine faces (vizinhosPorFaces).
@@ -697,13 +698,9 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
         inf.convergiu = rv <= tol * normas[0] ? 1 : 0;
         break;
       }
+      // the true residual replaces r and rb; the search direction carries on (no restart)
       residuoVerdadeiro(true);
       inf.trocas++;
-      precondicionar(z, zb);  // restart: p = z
-      p = z;
-      for (uint32_t b : ativos) pb.set(b, zb.get(b));
-      rz = produto(r, z, tipo) + produtoB(rb, zb);
-      continue;
     }
     if (it == iteracoes - 1) break;
     zVelho = z;

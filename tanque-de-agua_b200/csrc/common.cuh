@@ -62,7 +62,7 @@ struct Escalares {
   int pronto;                 // the running solve met its tolerance
   int erro;                   // device-side error flag (bounded waits, capacity)
   int verificar;              // plain engine, tolerance mode: a true-residual check is due
-  int reiniciar;              // plain engine: the true residual replaced r; CG restarts
+  int reiniciar;              // plain engine: the true residual is to replace r (k_substituir)
   int aceitas;                // particles accepted by the last add
   int pendentes;              // label-propagation work list length
   int pad;

@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(256) k_verdade(Dev d, const uint8_t* vizOp, co
 }
 // One CTA: the true norm (partials in block order, then the bubble rows rhs - (faces y - sum)),
 // and the decision: converged or at the cap -> pronto; else the bubble rows take their true
-// residual, reiniciar is set (k_substituir copies the water part, BETA restarts the direction).
+// residual, reiniciar is set (k_substituir copies the water part into r).
 __global__ void __launch_bounds__(256) k_verdade_fim(Dev d, int blocosVerdade, int cap, double tol, int bolhas,
                                                     int meiaPrecisao) {
   __shared__ double sh[32];
@@ -658,8 +658,8 @@ __global__ void __launch_bounds__(DOT_T) k_produto(Dev d, int modo, const float*
       }
       case BETA: {
         double rzNovo = x1, cruzado = x2;
-        // after a replacement CG restarts: p = z (js/pressao-cpu.js:363-364's form)
-        e->beta = (e->reiniciar || fabs(e->rz) < 1e-30) ? 0.0 : fmax(0.0, (rzNovo - cruzado) / e->rz);
+        // (after a residual replacement the direction carries on: no restart)
+        e->beta = fabs(e->rz) < 1e-30 ? 0.0 : fmax(0.0, (rzNovo - cruzado) / e->rz);
         e->reiniciar = 0;
         e->rz = rzNovo;
         break;

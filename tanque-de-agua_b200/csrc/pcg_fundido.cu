@@ -1917,7 +1917,6 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     double norma = sqrt(somas[0]);
     itersFeitas = it + 1;
     bool fim = it == a.iteracoes - 1 || (a.tol > 0 && norma <= a.tol * norma0);
-    bool reinicio = false;
     if (fim && a.q64) {
       // tolerance mode: the true residual of the FP64 iterate decides
       faseVerdade(a, sh);
@@ -1928,10 +1927,9 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       somasGlobais(a, nAt, [&](int b) { const double v = rbVerd(b); return v * v; }, [](int) { return 0.0; }, sh, somas);
       normaVerd = sqrt(somas[0] + somas[2]);
       if (!(normaVerd <= a.tol * norma0) && it < a.iteracoes - 1) {
-        // replacement: r (water) was rewritten by faseVerdade, the bubble rows follow; CG
-        // restarts from the true residual
+        // replacement: r (water) was rewritten by faseVerdade, the bubble rows follow; the
+        // iteration goes on with the same search direction
         fim = false;
-        reinicio = true;
         trocas++;
         norma = normaVerd;
         if (blockIdx.x == 0)
@@ -1952,15 +1950,10 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     escala = (a.escalar && norma > 0) ? (float)(1.0 / norma) : 1.0f;
     if (blockIdx.x == 0)
       for (int b = threadIdx.x; b < MAX_BOLHAS; b += TF) d.accB[b] = 0;
-    if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, zo, reinicio ? nullptr : zc}, sh, secaoDensa))
-      return;
+    if (!cicloV<T>(a, ep, areas, dyn, tabS, &tileOff, Reuniao{escala, zo, zc}, sh, secaoDensa)) return;
     cz ^= 1;
     cp ^= 1;
-    primeira = reinicio;
-    if (reinicio) {  // r.z of the restart (the first iteration's form)
-      somasGlobais(a, nAt, [&](int b) { return __ldcg(&d.rb[b]) * zbAtual(b); }, [](int) { return 0.0; }, sh, somas);
-      rz = somas[0] + somas[2];
-    }
+    primeira = false;
   }
   // ---- end: q = 0 off water (the FP64 iterate rounded on water); bubbles hand back their
   // pressure; the solve's convergence record
