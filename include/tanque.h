@@ -307,9 +307,11 @@ typedef struct tq_solve_info {
  * tolerance > 0 (no counterpart in the reference) accumulates q in FP64 during the solve and
  * stops when the TRUE residual ||b - A q||, recomputed in FP64 from the FP64 iterate and the
  * bubble pressures, is <= tolerance * ||r0||, or at `iterations` (the cap).  The true residual
- * is recomputed whenever the recursive FP32 one meets the tolerance; if the true one does
- * not, it replaces the recursive one and CG goes on with the same search direction (residual
- * replacement).
+ * is recomputed whenever the recursive FP32 one meets the tolerance, and each time the
+ * recursive one has fallen by 1e-3 since the last recomputation; unless the solve ends there,
+ * the true residual replaces the recursive one and CG goes on with the same search direction
+ * (residual replacement), which keeps the FP32 rounding of the recursive residual far below
+ * the tolerance.
  * q is returned rounded to FP32, so b - A q of the returned float q carries their rounding
  * (about 1e-7 of |A| |q| per cell) on top of the reported true residual.
  * norms receives the recursive residual history (initial, then one per iteration).

@@ -485,6 +485,12 @@ void vizinhosPorFaces(const Nivel<S>& f, Nivel<S>& g) {
     }
 }
 
+// Tolerance mode replaces the recursive residual by the true one each time the recursive one has
+// fallen by this factor since the last replacement (or since r0): the FP32 rounding the
+// recursive residual gathers (about 1e-7 of the residual it started from, per iteration) is
+// then far below the tolerance by the end of the solve.
+constexpr double FATOR_TROCA = 1e-3;
+
 // What a solve reports beside q (tq_solve_info).
 struct InfoPCG {
   int iters = 0, convergiu = 0, trocas = 0;
@@ -494,9 +500,10 @@ struct InfoPCG {
 // resolverPCG, js/pressao-cpu.js:296-402.  tol = 0 is the reference's fixed count.  tol > 0 (no
 // counterpart in the reference) keeps q in double during the solve and stops when the TRUE
 // residual ||b - A q|| (double, from the double iterate and the bubbles' y) is <= tol*||r0||,
-// or at the cap.  The true residual is recomputed when the recursive one meets the tolerance;
-// when the true one does not, it replaces the recursive one and the iteration goes on with the
-// same search direction (a residual replacement without restart).
+// or at the cap.  The true residual is recomputed when the recursive one meets the tolerance, and
+// each time the recursive one has fallen by FATOR_TROCA since the last replacement; unless the
+// solve ends there, it replaces the recursive one and the iteration goes on with the same
+// search direction (a residual replacement without restart).
 // precond = TQ_PRECOND_BLOCK replaces precondicionar (:352-361) by the block-diagonal form:
 // bubble rows z_b = r_b / faces_b, the V-cycle on the water alone (enclosed air stays air) with
 // coarse neighbour masks from the fine faces (vizinhosPorFaces).
@@ -663,6 +670,7 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
   };
   InfoPCG inf;
   inf.r0 = normas[0];
+  double proxTroca = normas[0] * FATOR_TROCA;  // the next residual replacement's threshold
   precondicionar(z, zb);
   p = z;
   for (uint32_t b : ativos) pb.set(b, zb.get(b));
@@ -689,18 +697,19 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
     }
     normas.push_back(norma());
     inf.iters = it + 1;
-    if (verdade && (normas.back() <= tol * normas[0] || it == iteracoes - 1)) {
+    if (verdade && (normas.back() <= tol * normas[0] || normas.back() <= proxTroca || it == iteracoes - 1)) {
       const bool ultima = it == iteracoes - 1;
-      // the true residual; when it misses the tolerance before the cap it replaces r, rb
+      // the true residual: below the tolerance or at the cap the solve ends; otherwise it
+      // replaces r and rb and the search direction carries on (no restart)
       const double rv = residuoVerdadeiro(false);
       inf.rv = rv;
       if (rv <= tol * normas[0] || ultima) {
         inf.convergiu = rv <= tol * normas[0] ? 1 : 0;
         break;
       }
-      // the true residual replaces r and rb; the search direction carries on (no restart)
       residuoVerdadeiro(true);
       inf.trocas++;
+      proxTroca = rv * FATOR_TROCA;
     }
     if (it == iteracoes - 1) break;
     zVelho = z;

@@ -63,6 +63,7 @@ struct Escalares {
   int erro;                   // device-side error flag (bounded waits, capacity)
   int verificar;              // plain engine, tolerance mode: a true-residual check is due
   int reiniciar;              // plain engine: the true residual is to replace r (k_substituir)
+  double proxTroca;           // plain engine: the recursive norm that triggers the next replacement
   int aceitas;                // particles accepted by the last add
   int pendentes;              // label-propagation work list length
   int pad;

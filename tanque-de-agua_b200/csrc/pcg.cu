@@ -410,6 +410,10 @@ __global__ void k_atualizar(Dev d, double* q64) {
 
 __device__ inline double somaBloco(double v, double* sh);  // block sum (valid in thread 0), below
 
+// Tolerance mode replaces the recursive FP32 residual by the true one each time the recursive one
+// has fallen by this factor since the last replacement (as the fused engine and the oracle do).
+constexpr double FATOR_TROCA = 1e-3;
+
 // Tolerance mode, once the recursive residual met the tolerance (Escalares::verificar): the true
 // residual in FP64 from the FP64 iterate and the bubble pressures.  Water cells: rt = -div - A q
 // into d.ap (free until the next A p) and rt^2 into per-CTA partials; interior air of active
@@ -486,6 +490,7 @@ __global__ void __launch_bounds__(256) k_verdade_fim(Dev d, int blocosVerdade, i
     } else {
       e->reiniciar = 1;
       e->trocas++;
+      e->proxTroca = nv * FATOR_TROCA;
       e->norma = nv;
       e->escalaMG = (meiaPrecisao && nv > 0) ? 1.0 / nv : 1.0;
       substituir = 1;
@@ -640,6 +645,7 @@ __global__ void __launch_bounds__(DOT_T) k_produto(Dev d, int modo, const float*
         e->trocas = 0;
         e->convergiu = 0;
         e->normaVerd = -1.0;
+        e->proxTroca = nr * FATOR_TROCA;
         e->escalaMG = (meiaPrecisao && nr > 0) ? 1.0 / nr : 1.0;
         break;
       }
@@ -650,9 +656,10 @@ __global__ void __launch_bounds__(DOT_T) k_produto(Dev d, int modo, const float*
         e->norma = nr;
         if (it + 1 < 1024) e->normas[it + 1] = nr;
         e->iters = it + 1;
-        // tolerance mode: the recursive residual met the tolerance (or the cap came): the true
-        // residual decides (k_verdade, k_verdade_fim)
-        e->verificar = tol > 0 && (nr <= tol * e->norma0 || it + 1 >= cap);
+        // tolerance mode: the recursive residual met the tolerance, or fell by FATOR_TROCA since
+        // the last replacement, or the cap came: the true residual decides (k_verdade,
+        // k_verdade_fim)
+        e->verificar = tol > 0 && (nr <= tol * e->norma0 || nr <= e->proxTroca || it + 1 >= cap);
         e->escalaMG = (meiaPrecisao && nr > 0) ? 1.0 / nr : 1.0;
         break;
       }

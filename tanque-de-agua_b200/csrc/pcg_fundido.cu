@@ -54,6 +54,10 @@ constexpr int SECAO_DENSA_MIN_ITERS = 30;
 // The coarsest level's sweeps run on one warp up to this many cells, on every warp of CTA 0 above.
 constexpr int GROSSO_UM_WARP = 1024;
 constexpr int NPARC = 4;                           // partial slots per CTA
+// Tolerance mode replaces the recursive FP32 residual by the true one (FP64) each time the
+// recursive one has fallen by this factor since the last replacement: the rounding it gathers,
+// about 1e-7 of the residual it started from per iteration, then stays far below the tolerance.
+constexpr double FATOR_TROCA = 1e-3;
 constexpr int PERFIL_MAX = 1 << 16;                // phase-trace capacity
 constexpr int PERFIL_SECAO = 1 << 14;              // coarse-section stamps (after the phase trace)
 // per-warp shared-memory areas (floats)
@@ -1829,6 +1833,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
   bool primeira = true;
   int itersFeitas = 0, trocas = 0;
   double normaVerd = -1.0;
+  double proxTroca = norma0 * FATOR_TROCA;  // the next residual replacement's threshold
 
   for (int it = 0; it < a.iteracoes; it++) {
     float* zc = cz ? a.z2 : d.z;
@@ -1917,8 +1922,9 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     double norma = sqrt(somas[0]);
     itersFeitas = it + 1;
     bool fim = it == a.iteracoes - 1 || (a.tol > 0 && norma <= a.tol * norma0);
-    if (fim && a.q64) {
-      // tolerance mode: the true residual of the FP64 iterate decides
+    if (a.q64 && (fim || norma <= proxTroca)) {
+      // tolerance mode: the true residual of the FP64 iterate decides, and replaces the
+      // recursive one unless the solve ends here
       faseVerdade(a, sh);
       if (!barreira(a, ep)) return;
       auto rbVerd = [&](int b) {
@@ -1926,11 +1932,12 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       };
       somasGlobais(a, nAt, [&](int b) { const double v = rbVerd(b); return v * v; }, [](int) { return 0.0; }, sh, somas);
       normaVerd = sqrt(somas[0] + somas[2]);
-      if (!(normaVerd <= a.tol * norma0) && it < a.iteracoes - 1) {
+      fim = normaVerd <= a.tol * norma0 || it == a.iteracoes - 1;
+      if (!fim) {
         // replacement: r (water) was rewritten by faseVerdade, the bubble rows follow; the
         // iteration goes on with the same search direction
-        fim = false;
         trocas++;
+        proxTroca = normaVerd * FATOR_TROCA;
         norma = normaVerd;
         if (blockIdx.x == 0)
           for (int k = threadIdx.x; k < nAt; k += TF) {
