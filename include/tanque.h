@@ -344,7 +344,12 @@ int tq_vcycle(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float
  * streams, or two host threads) race on it and corrupt each other's results, so keep the
  * calls on one device in one stream, or wait for one before issuing the next.
  * The first call on each device does a one-time set-up (it looks up the scratch's device
- * address); a caller that captures streams makes that first call before capturing. */
+ * address); a caller that captures streams makes that first call before capturing.  The
+ * address belongs to the device's current context: after cudaDeviceReset (or a primary
+ * context released and made again) the next call sees the new context and looks the address
+ * up again, which is again a set-up call.  Grids above 2^20 cells a side or 2^28 cells are
+ * refused with TQ_E_CAPACITY before any size arithmetic.  A CUDA error left pending by earlier
+ * work on the calling thread is reported (and cleared) as TQ_E_CUDA without launching. */
 int tq_vcycle_noalloc(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float* x,
                       int32_t precision, void* stream);
 

@@ -1029,20 +1029,50 @@ size_t bytesScratchVCiclo(int nx, int ny) {
   return total;
 }
 
-// Device address of the scratch on the current device, looked up once per device.
+// Device address of the scratch on the current device.  The address is looked up with
+// cudaGetSymbolAddress once per device and context: the cache holds, per device ordinal, the
+// context the address belongs to, and a different current context (the device was reset, or the
+// primary context was released and created again, which loads the module anew) looks it up
+// again instead of handing out a stale address.  The current context comes from the driver's
+// cuCtxGetCurrent, reached through cudaGetDriverEntryPoint (no link to libcuda).
+namespace {
+using CtxGetCurrent = int (*)(void**);
+CtxGetCurrent ctxGetCurrent() {
+  static CtxGetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      f = nullptr;
+    }
+    return (CtxGetCurrent)f;
+  }();
+  return fn;
+}
+}  // namespace
+
 int enderecoScratchVCiclo(void** out) {
   static std::mutex mtx;
   static void* base[64] = {};
+  static void* ctxDe[64] = {};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return TQ_E_NODEV;
   std::lock_guard<std::mutex> g(mtx);
-  if (!base[dev]) {
+  void* ctx = nullptr;
+  CtxGetCurrent f = ctxGetCurrent();
+  if (!f) return TQ_E_CUDA;
+  if (!base[dev] || f(&ctx) != 0 || !ctx || ctx != ctxDe[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_scratchVCiclo) != cudaSuccess || !p) {
       cudaGetLastError();
+      base[dev] = nullptr;
       return TQ_E_CUDA;
     }
+    // the lookup makes the runtime's primary context current if none was: read it after
+    if (f(&ctx) != 0 || !ctx) return TQ_E_CUDA;
     base[dev] = p;
+    ctxDe[dev] = ctx;
   }
   *out = base[dev];
   return TQ_OK;

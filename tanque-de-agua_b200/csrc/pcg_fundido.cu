@@ -106,6 +106,13 @@ struct Fundido {
   bool perfilar = false;
   double* q64 = nullptr;     // the FP64 iterate of a tolerance-mode solve
   long long* accV = nullptr; // per-bubble fixed-point sums of the true residual
+  // Bounded-wait test hooks, read from the environment when the solver is created:
+  // TQ_BARRIER_WAIT_CYCLES sets the grid barrier's limit (SM clock cycles); TQ_BARRIER_HOLD_CTA
+  // and TQ_BARRIER_HOLD_CYCLES make that CTA wait that many cycles before it arrives at the
+  // first barrier of the NEXT solve only (one-shot), so the other CTAs' waits run out.
+  long long limite = LIMITE_CICLOS;
+  int segurarCta = -1;
+  long long segurarCiclos = 0;
 };
 
 struct Args {
@@ -138,6 +145,9 @@ struct Args {
   // per level: 1 per 16x16 block whose cells are all wall (out-of-grid cells count as wall), the
   // blocks of shift 0 then those of shift 8; null where the level does not skip wall blocks
   uint8_t* sol[MAX_NIVEIS];
+  long long limite;          // grid barrier wait limit (cycles)
+  int segurarCta;            // test hook: this CTA arrives late at the first barrier (-1: none)
+  long long segurarCiclos;   // ... after waiting this many cycles (bounded)
   int bloco;  // TQ_PRECOND_BLOCK: bubble rows Jacobi, V-cycle on water, coarse masks from faces
   // tolerance mode: q accumulates in FP64 (q64) and the solve stops on the true residual
   // ||b - A q64|| (FP64), with residual replacement; null in fixed-count mode
@@ -215,6 +225,10 @@ __device__ bool barreira(const Args& a, unsigned& epoca) {
   __shared__ int falhou;
   __syncthreads();
   if (threadIdx.x == 0) {
+    if (epoca == 0 && (int)blockIdx.x == a.segurarCta) {  // test hook: a late arrival, bounded
+      const long long t = clock64();
+      while (clock64() - t < a.segurarCiclos) __nanosleep(1000);
+    }
     epoca++;
     const unsigned alvo = epoca * gridDim.x;
     somarLiberar(a.bar, 1u);
@@ -227,7 +241,7 @@ __device__ bool barreira(const Args& a, unsigned& epoca) {
           f = 1;
           break;
         }
-        if (clock64() - t0 > LIMITE_CICLOS) {
+        if (clock64() - t0 > a.limite) {
           atomicExch(a.erro, 1);
           f = 1;
           break;
@@ -2058,6 +2072,15 @@ Fundido* criarFundido(Pcg* p) {
     // threshold in blocks; the tests use 1 to skip on every grid level and 0x7fffffff for none.
     long long limiar = 2LL * WARPS * f->G;
     if (const char* e = getenv("TQ_WALL_SKIP_MIN_BLOCKS")) limiar = atoll(e);
+    if (const char* e = getenv("TQ_BARRIER_WAIT_CYCLES")) {
+      const long long v = atoll(e);
+      if (v > 0 && v <= LIMITE_CICLOS) f->limite = v;
+    }
+    if (const char* e = getenv("TQ_BARRIER_HOLD_CTA")) f->segurarCta = atoi(e);
+    if (const char* e = getenv("TQ_BARRIER_HOLD_CYCLES")) {
+      const long long v = atoll(e);
+      f->segurarCiclos = v > 0 && v <= 4 * LIMITE_CICLOS ? v : 0;
+    }
     size_t nFlags = 0;
     for (int l = 0; l < Lc; l++) {
       f->comParedes[l] = blocosNivel(p->nxL[l], p->nyL[l], 0) >= limiar;
@@ -2118,6 +2141,10 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   Fundido* f = p->fundido;
   Args a{};
   a.bloco = precond == TQ_PRECOND_BLOCK ? 1 : 0;
+  a.limite = f->limite;
+  a.segurarCta = f->segurarCta;
+  a.segurarCiclos = f->segurarCiclos;
+  f->segurarCta = -1;  // the hold is one-shot
   a.q64 = tol > 0 ? f->q64 : nullptr;
   a.accV = f->accV;
   a.d = d;

@@ -974,6 +974,9 @@ int tq_vcycle_noalloc(int32_t nx, int32_t ny, const uint8_t* tipo, const float* 
                       void* stream) {
   if (nx < 3 || ny < 3 || !tipo || !b || !x) return falha(TQ_E_ARG, "tq_vcycle_noalloc: bad arguments");
   if (precision < TQ_PREC_FP32 || precision > TQ_PREC_BF16) return falha(TQ_E_ARG, "tq_vcycle_noalloc: bad precision");
+  // sizes far beyond any scratch are refused before the level arithmetic sees them
+  if (nx > (1 << 20) || ny > (1 << 20) || (long long)nx * ny > (1LL << 28))
+    return falha(TQ_E_CAPACITY, "tq_vcycle_noalloc: grid larger than 2^20 cells a side or 2^28 cells");
   const size_t preciso = bytesScratchVCiclo(nx, ny);
   if (preciso > BYTES_SCRATCH_VCICLO) {
     std::snprintf(g_erro, sizeof g_erro,
@@ -986,6 +989,14 @@ int tq_vcycle_noalloc(int32_t nx, int32_t ny, const uint8_t* tipo, const float* 
   int st = enderecoScratchVCiclo(&scratch);
   if (st == TQ_E_NODEV) return falha(st, "tq_vcycle_noalloc: no current CUDA device");
   if (st) return falha(st, "tq_vcycle_noalloc: cudaGetSymbolAddress of the scratch failed");
+  // an error left by earlier, unrelated work on this thread is reported as such (and cleared),
+  // not as a failure of this call's launches
+  cudaError_t antes = cudaGetLastError();
+  if (antes != cudaSuccess) {
+    std::snprintf(g_erro, sizeof g_erro, "tq_vcycle_noalloc: a CUDA error was pending before the call: %s",
+                  cudaGetErrorString(antes));
+    return TQ_E_CUDA;
+  }
   st = cicloVSemAlocar(scratch, nx, ny, tipo, b, x, precision, (cudaStream_t)stream);
   if (st) return falha(st, "tq_vcycle_noalloc: V-cycle launch failed");
   return TQ_OK;

@@ -46,6 +46,9 @@ def test_grade_grande_demais_recusada():
     assert st == _abi.TQ_E_CAPACITY
     msg = lib.tq_last_error().decode()
     assert "bytes" in msg and str(BYTES_SCRATCH) in msg
+    # sizes whose level arithmetic would overflow int are refused before it runs
+    for nx, ny in [(2**31 - 1, 16), (16, 2**31 - 1), (1 << 21, 4), (1 << 15, 1 << 15)]:
+        assert f(nx, ny, 1, 1, 1, _abi.TQ_PREC_FP32, None) == _abi.TQ_E_CAPACITY, (nx, ny)
     assert f(2, 2, 1, 1, 1, _abi.TQ_PREC_FP32, None) == _abi.TQ_E_ARG
     assert f(40, 30, 1, 1, 1, 7, None) == _abi.TQ_E_ARG
 
