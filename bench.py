@@ -55,7 +55,7 @@ BYTES_ITER = {"fp32": 156.0, "fp16": 120.0, "bf16": 120.0}
 BYTES_SETUP = {"fp32": 110.0, "fp16": 85.0, "bf16": 85.0}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fused FP16 solve of this
 # scene, from one ncu capture of the kernel: the solve's working set stays in L2.
-TRAFEGO_SOLVE_BYTES = 14_248_704
+TRAFEGO_SOLVE_BYTES = 90_651_136
 
 
 def picos():

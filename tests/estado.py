@@ -79,3 +79,37 @@ def comparar_passo(o, g, quadro, tol_campos=1e-3, tol_pos=1e-5):
     pg, po = g.p.reshape(-1, CAMPOS), o.p.reshape(-1, CAMPOS)
     assert pg.shape == po.shape, quadro
     assert float(np.max(np.abs(pg[:, :2].astype(np.float64) - po[:, :2]))) < tol_pos, quadro
+
+
+def divergencia(sim) -> np.ndarray:
+    """Discrete divergence of the MAC velocities on water cells (per unit cell width), 0 elsewhere:
+    u[i+1,j] - u[i,j] + v[i,j+1] - v[i,j] (js/fisica-cpu.js:456-470's form without the density
+    term)."""
+    nx, ny = sim.nx, sim.ny
+    u = sim.campo("u").astype(np.float64).reshape(ny, nx + 1)
+    v = sim.campo("v").astype(np.float64).reshape(ny + 1, nx)
+    d = (u[:, 1:] - u[:, :-1]) + (v[1:, :] - v[:-1, :])
+    d[sim.campo("tipo").reshape(ny, nx) != 1] = 0.0
+    return d
+
+
+def volume_na_grade(sim) -> float:
+    """Water volume on the grid: the sum over cells of the fraction min(1, rho / 4)
+    (js/fisica-cpu.js:309) times h^2."""
+    return float(np.sum(np.minimum(1.0, sim.campo("densidade").astype(np.float64) / 4.0))) * sim.h * sim.h
+
+
+def nivel_medio(sim) -> tuple[float, float]:
+    """The reference's volume check (testes/fisica.test.js:96-116): the mean over the columns away
+    from the walls of the highest particle's height, above the frame, and the level the water's
+    area would fill."""
+    from tanque.constantes import MOLDURA
+    h, nx = sim.h, sim.nx
+    p = sim.p.reshape(-1, CAMPOS)
+    topo = np.zeros(nx, np.float32)
+    i = np.floor(p[:, 0].astype(np.float64) / h).astype(np.int64)
+    ok = (i >= 0) & (i < nx)
+    np.maximum.at(topo, i[ok], p[ok, 1])
+    m = MOLDURA * h
+    cols = topo[MOLDURA + 3: nx - MOLDURA - 3].astype(np.float64)
+    return float(cols.mean()) - m, sim.area() / (nx * h - 2 * m)

@@ -45,3 +45,31 @@ def test_subpasso_ultra(lib_gpu, precond):
     for s in (o, g):
         assert s.escalar(_abi.TQ_SCALAR_PCG_CONVERGED) == 1
         assert s.escalar(_abi.TQ_SCALAR_PCG_TRUE_RES) <= 1e-6 * s.escalar(_abi.TQ_SCALAR_PCG_RES0)
+
+
+def test_erro_ultra_contra_fp64(lib_gpu, capsys):
+    """One substep of the bench scene in the mixed configuration against the FP64 oracle (double
+    storage everywhere) from the same state: the errors of FP32 arithmetic and FP16 V-cycle
+    storage once both solves meet the true 1e-6.  Bound: 1e-3 relative on q, u, v and the
+    divergence; bubble volumes exact."""
+    from estado import divergencia
+    opc = {"tolerance": 1e-6, "iterations": 1000, "preconditioner": _abi.TQ_PRECOND_BLOCK}
+    cena_g, _, agua, torneira = cena_ultra(Cena)
+    cena_o, _, _, _ = cena_ultra(CenaOraculo)
+    g = SimulacaoGPU(cena_g, dict(opc, engine=_abi.TQ_ENGINE_FUSED, precision=_abi.TQ_PREC_FP16))
+    g.adicionar(agua, False)
+    g.adicionar(jato_torneira(torneira, 0, 1 / 60), True)
+    g.avancar(1 / 60, SUB)
+    o = SimulacaoOraculo(cena_o, dict(opc, p2g_mode=_abi.TQ_P2G_FIXED), fp64=True)
+    copiar_estado(g, o)
+    o.definirCampo("yBolha", g.campo("yBolha"))
+    for s in (o, g):
+        s.subpasso(1 / 60 / SUB)
+    erros = {c: erro_relativo(g.campo(c), o.campo(c)) for c in ["q", "u", "v"]}
+    erros["div"] = erro_relativo(divergencia(g), divergencia(o))
+    vb_g, vb_o = g.campo("volumeBolha"), o.campo("volumeBolha")
+    ativas = np.nonzero(vb_o)[0]
+    with capsys.disabled():
+        print("\n840x536 mixed vs FP64 oracle: " + ", ".join(f"{k} {v:.2e}" for k, v in erros.items()))
+    assert np.array_equal(vb_g[ativas], vb_o[ativas])
+    assert max(erros.values()) <= 1e-3, erros
