@@ -353,6 +353,48 @@ int tq_vcycle(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float
 int tq_vcycle_noalloc(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float* x,
                       int32_t precision, void* stream);
 
+/* ---------------------------------------------------------------- adjoint of the step */
+/* No counterpart in the reference (it has no gradients).  A differentiable simulation: the
+ * substep of SimulacaoCPU.subpasso (js/fisica-cpu.js:176-189) with air tracking off, surface
+ * tension 0 and the density correction off — P2G (APIC), gravity and wall faces, cell flags, the
+ * pressure projection (resolverPCG's system solved to a relative 1e-12), gradient, extrapolation,
+ * G2P with micro-steps and wall collisions — run forward and backward in FP64 on the GPU.  The
+ * discrete structure (cell flags, valid masks, micro-step counts, speed clamps, collision branches,
+ * kills, the faucet's insert filter) is the forward run's, held fixed in the backward run: the
+ * gradient is that of the smooth map the forward run sits on.
+ *
+ * Loss: sum over cells of (min(1, rho/4) - target)^2, rho the bilinear particle density at the
+ * cell centres after the last step (#paraGrade's densidade, js/fisica-cpu.js:244-254).
+ * Controls: the initial particle velocities (2 per particle) and the faucet velocity theta (2
+ * scalars), the velocity of the particles the faucet emits at the start of every step at the
+ * given positions (they pass adicionar's wall filter, js/fisica-cpu.js:100).
+ * The forward run keeps the state every `checkpoint_every` steps; the backward run recomputes
+ * each segment from its checkpoint and goes back through it (the torch.autograd.Function
+ * contract: forward saves what backward needs). */
+typedef struct tq_adj_scene {
+  int32_t nx, ny;
+  double h, dt;
+  int32_t steps;
+  int32_t checkpoint_every;     /* steps between checkpoints; 0: 10 */
+  double gravity[2];
+  const float* sdf;             /* wall SDF, (2 nx) x (2 ny), as tq_set_walls */
+  const float* positions;       /* 2 per initial particle (x, y) in metres */
+  const float* affine;          /* 4 per initial particle (cux cuy cvx cvy), or NULL for 0 */
+  const float* faucet_positions;/* steps x faucet_per_step x 2 */
+  const float* target;          /* nx * ny target water fraction */
+  int32_t n_particles;
+  int32_t faucet_per_step;
+} tq_adj_scene;
+
+typedef struct tq_adj tq_adj;
+int tq_adj_create(const tq_adj_scene* scene, int32_t device, tq_adj** out);
+int tq_adj_destroy(tq_adj* a);
+/* The forward run: v0 = 2 per initial particle, theta = 2; *loss receives the loss. */
+int tq_adj_forward(tq_adj* a, const float* v0, const double* theta, double* loss);
+/* The backward run of the last forward run: dL/dv0 (2 per initial particle, FP32) and dL/dtheta
+ * (2), scaled by `grad_loss` (the incoming gradient of the loss). */
+int tq_adj_backward(tq_adj* a, double grad_loss, float* dv0, double* dtheta);
+
 /* ---------------------------------------------------------------- errors */
 const char* tq_status_string(int status);
 /* Last error message of the calling thread (CUDA error text or argument problem). */

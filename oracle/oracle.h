@@ -71,6 +71,16 @@ int tqo_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float*
                        tq_solve_info* info);
 int tqo_vcycle(int32_t nx, int32_t ny, const uint8_t* tipo, const float* b, float* x);
 
+/* ---- the FP64 CPU adjoint (adjunto_oracle.cpp), the checker of tq_adj_*.  record = 1 records
+ * the discrete structure of the run; record = 0 reuses the last recorded one (frozen), so central
+ * finite differences see the same smooth map as the adjoint.  Velocities in double. */
+typedef struct tqo_adj tqo_adj;
+int tqo_adj_create(const tq_adj_scene* scene, tqo_adj** out);
+int tqo_adj_destroy(tqo_adj* a);
+int tqo_adj_forward(tqo_adj* a, const double* v0, const double* theta, int32_t record, double* loss);
+int tqo_adj_backward(tqo_adj* a, double* dv0, double* dtheta);
+int tqo_adj_count(tqo_adj* a, int32_t* n);
+
 const char* tqo_last_error(void);
 
 #ifdef __cplusplus

@@ -732,6 +732,23 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
   return normas;
 }
 
+}  // namespace
+
+// A q = b on the water cells of `tipo` with resolverPCG's operator, in double storage, to a
+// relative residual of 1e-13 (the reference preconditioner, at most 2000 iterations): the exact
+// pressure solve of the FP64 adjoint checker (adjunto_oracle.cpp).
+void resolverExatoFP64(int nx, int ny, const uint8_t* tipo, const double* b, double* q) {
+  Niveis<double> L;
+  montarNiveis(L, nx, ny);
+  const size_t N = (size_t)nx * ny;
+  std::vector<double> div(N);
+  for (size_t c = 0; c < N; c++) div[c] = -b[c];  // resolverPCG solves A q = -div
+  std::fill(q, q + N, 0.0);
+  resolverPCG<double>(L, tipo, div.data(), q, 2000, nullptr, 1e-13);
+}
+
+namespace {
+
 // ------------------------------------------------------------- js/ar.js:22-159
 template <class S>
 struct Rastreador {

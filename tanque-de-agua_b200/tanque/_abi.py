@@ -65,6 +65,15 @@ class TqBubbles(C.Structure):
     _fields_ = [("rotulo", C.c_void_p), ("rhs", C.c_void_p), ("y", C.c_void_p)]
 
 
+class TqAdjScene(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("h", C.c_double), ("dt", C.c_double), ("steps", C.c_int32),
+        ("checkpoint_every", C.c_int32), ("gravity", C.c_double * 2), ("sdf", C.c_void_p), ("positions", C.c_void_p),
+        ("affine", C.c_void_p), ("faucet_positions", C.c_void_p), ("target", C.c_void_p), ("n_particles", C.c_int32),
+        ("faucet_per_step", C.c_int32),
+    ]
+
+
 class TqSolveInfo(C.Structure):
     _fields_ = [
         ("iterations", C.c_int32), ("converged", C.c_int32), ("replacements", C.c_int32), ("pad", C.c_int32),
@@ -111,6 +120,10 @@ ASSINATURAS = {
 }
 SO_PRODUTO = {
     "advance_graph": (C.c_int, [_P, _D, _I]),
+    "adj_create": (C.c_int, [C.POINTER(TqAdjScene), _I, C.POINTER(_P)]),
+    "adj_destroy": (C.c_int, [_P]),
+    "adj_forward": (C.c_int, [_P, _P, C.POINTER(_D), C.POINTER(_D)]),
+    "adj_backward": (C.c_int, [_P, _D, _P, C.POINTER(_D)]),
     "sync": (C.c_int, [_P]),
     "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "set_timing": (C.c_int, [_P, _I]),
@@ -199,3 +212,21 @@ def opcoes_padrao(nx: int, ny: int, h: float, **kw) -> TqOptions:
         else:
             setattr(o, k, v)
     return o
+
+
+def cena_adjunto_c(cena: dict):
+    """tq_adj_scene of a tanque.cenarios.cena_adjunto dict; returns (arrays to keep alive, struct)."""
+    import numpy as np
+    arr = {k: np.ascontiguousarray(cena[k], dtype=np.float32) for k in ("sdf", "positions", "faucet_positions", "target")}
+    sc = TqAdjScene()
+    sc.nx, sc.ny, sc.h, sc.dt = cena["nx"], cena["ny"], cena["h"], cena["dt"]
+    sc.steps, sc.checkpoint_every = cena["steps"], cena.get("checkpoint_every", 10)
+    sc.gravity[0], sc.gravity[1] = cena.get("gravity", (0.0, -9.81))
+    sc.sdf = arr["sdf"].ctypes.data
+    sc.positions = arr["positions"].ctypes.data if arr["positions"].size else None
+    sc.affine = None
+    sc.faucet_positions = arr["faucet_positions"].ctypes.data if arr["faucet_positions"].size else None
+    sc.target = arr["target"].ctypes.data
+    sc.n_particles = arr["positions"].shape[0]
+    sc.faucet_per_step = arr["faucet_positions"].shape[1] if arr["faucet_positions"].ndim == 3 else 0
+    return arr, sc

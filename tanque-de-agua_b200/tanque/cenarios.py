@@ -334,3 +334,36 @@ def cena_ar_preso(Cena, nx: int = 480, ny: int = 270, h: float = 0.0022):
         by = m + r + al() * (0.25 * H - r)
         fora &= (x - bx) ** 2 + (y - by) ** 2 >= r * r
     return cena, agua[fora].ravel()
+
+
+def cena_adjunto(nx: int = 256, ny: int = 160, h: float = 0.004, passos: int = 60, dt: float = 1 / 240,
+                 jato: int = 6, seed: int = 5) -> dict:
+    """The differentiable scene of the adjoint (tq_adj_*): an empty tank (the frame of
+    MOLDURA cells), a block of water seeded 2 x 2 per cell (semearRetangulo, js/fisica-cpu.js:705-727)
+    with seeded initial velocities, a faucet near the top left that emits at every step a slab of
+    `jato` cells by one cell, 4 particles a cell on a jittered 2 x 2 lattice (the jet density of
+    js/principal.js:301-321, whose slab per frame is the jet's length over the frame; a jet of
+    about 1 m/s moves about a cell a step here), and a seeded target blob of water fraction.
+    Returns arrays: sdf (2ny, 2nx), positions (n, 2), v0 (n, 2), faucet_positions
+    (passos, 4 jato, 2), target (ny, nx), theta0 (2,)."""
+    from .cena import Cena
+    cena = Cena(nx, ny, h)
+    m = MOLDURA * h
+    W, H = nx * h, ny * h
+    al = semente(seed)
+    bloco = semear_retangulo(m, m, m + 0.3 * W, m + 0.35 * H, h, (0, 0, 0), al).reshape(-1, CAMPOS)
+    pos = bloco[:, :2].astype(np.float32)
+    v0 = np.stack([[(al() - 0.5) * 0.4, (al() - 0.5) * 0.4] for _ in range(len(pos))]).astype(np.float32)
+    x0, y0 = m + 0.10 * W, H - m - 0.18 * H
+    fp = np.zeros((passos, 4 * jato, 2), np.float32)
+    for s_ in range(passos):
+        for k in range(jato):
+            for q in range(4):
+                fp[s_, 4 * k + q] = (x0 + (k + (q & 1) * 0.5 + 0.25 + (al() - 0.5) * 0.25) * h,
+                                     y0 + ((q >> 1) * 0.5 + 0.25 + (al() - 0.5) * 0.25) * h)
+    jj, ii = np.mgrid[0:ny, 0:nx]
+    tx, ty, tr = (0.35 + 0.3 * al()) * nx, (0.1 + 0.2 * al()) * ny, (0.08 + 0.05 * al()) * nx
+    alvo = np.clip(1.2 - np.hypot(ii + 0.5 - tx, jj + 0.5 - ty) / tr, 0, 1).astype(np.float32)
+    return {"nx": nx, "ny": ny, "h": h, "dt": dt, "steps": passos, "checkpoint_every": 10,
+            "sdf": np.asarray(cena.sdf, np.float32).reshape(2 * ny, 2 * nx), "positions": pos, "v0": v0,
+            "faucet_positions": fp, "target": alvo, "theta0": np.array([0.9, -0.4])}

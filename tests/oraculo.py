@@ -34,6 +34,11 @@ ASSINATURAS_ORACULO.update({
     "passo_maximo": (_D, [_D, _D, _D, _I, _D]),
     "semear_retangulo": (_I, [_D, _D, _D, _D, _D, C.POINTER(_D), C.POINTER(C.c_uint32), _P, _I]),
     "splat": (None, [_P, _I, _I, _I, _D, _I, _I, _P]),
+    "adj_create": (C.c_int, [C.POINTER(_abi.TqAdjScene), C.POINTER(_P)]),
+    "adj_destroy": (C.c_int, [_P]),
+    "adj_forward": (C.c_int, [_P, _P, _P, _I, C.POINTER(_D)]),
+    "adj_backward": (C.c_int, [_P, _P, _P]),
+    "adj_count": (C.c_int, [_P, C.POINTER(_I)]),
 })
 
 
@@ -137,3 +142,34 @@ def resolver_pressao_oraculo(tipo, div, q, iteracoes=3, tolerancia=0.0, bolhas=N
 def ciclo_v_oraculo(tipo, b):
     from tanque.simulacao import ciclo_v
     return ciclo_v(tipo, b, ligacao=carregar_oraculo())
+
+
+class AdjuntoOraculo:
+    """The FP64 CPU adjoint (oracle/adjunto_oracle.cpp) of a tanque.cenarios.cena_adjunto scene."""
+
+    def __init__(self, cena: dict):
+        self.lig = carregar_oraculo()
+        self._mantem, sc = _abi.cena_adjunto_c(cena)
+        h = C.c_void_p()
+        self.lig("adj_create", C.byref(sc), C.byref(h))
+        self._h = h
+        self.n0 = cena["positions"].shape[0]
+
+    def __del__(self):
+        try:
+            self.lig("adj_destroy", self._h)
+        except Exception:
+            pass
+
+    def forward(self, v0, theta, gravar=True) -> float:
+        v = np.ascontiguousarray(v0, dtype=np.float64).ravel()
+        t = np.ascontiguousarray(theta, dtype=np.float64)
+        perda = C.c_double()
+        self.lig("adj_forward", self._h, v.ctypes.data, t.ctypes.data, 1 if gravar else 0, C.byref(perda))
+        return perda.value
+
+    def backward(self):
+        gv = np.zeros(2 * self.n0, np.float64)
+        gt = np.zeros(2, np.float64)
+        self.lig("adj_backward", self._h, gv.ctypes.data, gt.ctypes.data)
+        return gv.reshape(-1, 2), gt
