@@ -506,6 +506,83 @@ def executar_lote(args, rank, mundo, dist):
     }
 
 
+# ------------------------------------------------------------------ the adjoint (256 x 160, 60 steps)
+METRIC_ADJ = "adjoint gradient evaluations/s @256x160, 60 steps (forward + backward, 32 candidate controls)"
+
+
+def executar_adjunto(args, rank, mundo, dist):
+    """--workload adjunto: the adjoint scene (tanque.cenarios.cena_adjunto: 256 x 160, h = 4 mm,
+    60 steps of 1/240 s, a dam-break block and a faucet, loss = L2 distance of the final water
+    fraction to a seeded target blob); a step is one gradient evaluation (forward with checkpoints
+    every 10 steps, backward with recomputation) of each of 32 candidate controls (initial
+    velocities and faucet velocity perturbed from a seed), the 32 handles driven by host threads
+    so their solves overlap on the GPU.  value = gradient evaluations per second."""
+    import concurrent.futures as cf
+
+    import torch
+    from tanque.adjunto import AdjuntoGPU
+    from tanque.cenarios import cena_adjunto
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    cena = cena_adjunto()
+    K = 32
+    rng = np.random.default_rng(7 + rank)
+    controles = [(cena["v0"] + rng.normal(0, 0.05, cena["v0"].shape).astype(np.float32),
+                  cena["theta0"] + rng.normal(0, 0.1, 2)) for _ in range(K)]
+    alcas = [AdjuntoGPU(cena, dev) for _ in range(K)]
+
+    def um(k):
+        a = alcas[k]
+        v, th = controles[k]
+        t0 = time.perf_counter()
+        L = a.frente(v, th)
+        t1 = time.perf_counter()
+        gv, gt = a.tras(1.0)
+        t2 = time.perf_counter()
+        return L, gt, t1 - t0, t2 - t1
+
+    pool = cf.ThreadPoolExecutor(max_workers=K)
+    for _ in range(args.warmup):
+        list(pool.map(um, range(K)))
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ini = torch.cuda.Event(enable_timing=True)
+    fim = torch.cuda.Event(enable_timing=True)
+    l0 = None
+    from tanque import SimulacaoGPU
+    l0 = SimulacaoGPU.lancamentos()
+    ini.record()
+    t0 = time.perf_counter()
+    res = []
+    for _ in range(args.steps):
+        res = list(pool.map(um, range(K)))
+    t = time.perf_counter() - t0
+    fim.record()
+    torch.cuda.synchronize()
+    lanc = SimulacaoGPU.lancamentos() - l0
+    ms = tempos_max_ranks([t * 1000.0], dist, "cuda")[0]
+    pool.shutdown()
+    for a in alcas:
+        a.fechar()
+    if rank != 0:
+        return None
+    valor = mundo * K * args.steps / (ms / 1000.0)
+    return {
+        "metric": METRIC_ADJ, "value": round(valor, 3), "unit": "gradients/s", "n_gpus": mundo, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "adjoint: 256x160 h=4mm, 60 steps of 1/240 s, dam-break block + faucet, "
+                               "L2 water-fraction loss to a seeded blob; 32 candidate controls per step",
+                   "particles": int(cena["positions"].shape[0]), "checkpoint_every": 10,
+                   "controls": K, "timing": "host wall clock over the threads (each call waits for its stream)"},
+        "per_control_ms": {"forward": round(1000 * float(np.mean([r[2] for r in res])), 2),
+                           "backward": round(1000 * float(np.mean([r[3] for r in res])), 2)},
+        "gpu_launches": int(lanc),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -515,8 +592,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-oracle timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", dest="fused", action="store_false", help="mixed config on the plain engine")
-    ap.add_argument("--workload", default="ultra", choices=["ultra", "lote"],
-                    help="ultra: the 450k-cell scene (default); lote: the 256-tank batch")
+    ap.add_argument("--workload", default="ultra", choices=["ultra", "lote", "adjunto"],
+                    help="ultra: the 450k-cell scene (default); lote: the 256-tank batch; adjunto: the adjoint")
     args = ap.parse_args()
 
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
@@ -549,6 +626,37 @@ def main():
         }
         print(json.dumps(linha))
         return
+    if args.impl == "reference" and args.workload == "adjunto":
+        if rank != 0:
+            return
+        # the reference has no adjoint: the CPU arm is the oracle's FP64 adjoint (the checker),
+        # one gradient evaluation of the scene's control per step
+        sys.path.insert(0, os.path.join(RAIZ, "tests"))
+        from oraculo import AdjuntoOraculo
+        from tanque.cenarios import cena_adjunto
+        cena = cena_adjunto()
+        a = AdjuntoOraculo(cena)
+        v0 = cena["v0"].astype(np.float64)
+        t0 = time.perf_counter()
+        feitos = 0
+        while feitos < max(1, args.steps):
+            a.forward(v0, cena["theta0"], True)
+            a.backward()
+            feitos += 1
+            if time.perf_counter() - t0 > args.cpu_budget:
+                break
+        v = feitos / (time.perf_counter() - t0)
+        print(json.dumps({
+            "metric": METRIC_ADJ, "impl": "reference", "value": round(v, 4), "unit": "gradients/s",
+            "n_gpus": args.gpus, "steps": feitos, "warmup": 0, "ms_per_step": round(1000 / v, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "adjoint scene as ours; one step = one gradient evaluation of one control"},
+            "cpu_baseline": {"value": round(v, 4), "unit": "gradients/s", "cores": 1, "kind": "port",
+                             "sample": f"{feitos} forward + backward runs of the FP64 CPU adjoint (the oracle's "
+                                       "checker; the reference has no adjoint), single thread"},
+            "e2e": {"value": round(v, 4), "unit": "gradients/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
     if args.impl == "reference":
         if rank != 0:
             return
@@ -574,7 +682,8 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    linha = (executar_lote if args.workload == "lote" else executar_gpu)(args, rank, mundo, dist)
+    corre = {"lote": executar_lote, "adjunto": executar_adjunto}.get(args.workload, executar_gpu)
+    linha = corre(args, rank, mundo, dist)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
