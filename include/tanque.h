@@ -150,6 +150,24 @@ int tq_splat(tq_sim* s, int32_t w, int32_t h, float* out);
 int tq_add_particles(tq_sim* s, const float* list, int32_t n, int32_t check_full,
                      int32_t* accepted);
 
+/* The faucet: emitirTorneira (js/principal.js:301-321) on the device.  Emits, through
+ * adicionar(lista, true)'s filter (walls, full cells), min(40000, round(2 r max(0.7, |v|) dt /
+ * h^2 * 4)) particles in a disk of radius r around (x, y) at velocity (vx, vy) with the given dye;
+ * the LCG of testes/apoio.js:4-9 seeded with `seed` stands in for Math.random (particle k takes
+ * draws 2k+1, 2k+2: angle u1 * 2 pi, radius sqrt(u2) r), so the list equals the one the same LCG
+ * makes on the host.  The caller computes the jet's velocity (the reference derives it from the
+ * pointer). *accepted receives the count kept; beyond capacity: TQ_E_CAPACITY, nothing added. */
+typedef struct tq_faucet {
+  double x, y;        /* jet centre (m) */
+  double radius;      /* jet radius (m) */
+  double vx, vy;      /* jet velocity (m/s) */
+  double dt;          /* the time the emission covers (s) */
+  double absorb[3];   /* dye of the emitted water */
+  uint32_t seed;
+  int32_t pad;
+} tq_faucet;
+int tq_emit_faucet(tq_sim* s, const tq_faucet* faucet, int32_t* accepted);
+
 /* MotorCPU.limparAgua without the air reset: sim.n = 0, contagemCelula.fill(0)
  * (js/motor.js:95). */
 int tq_clear_particles(tq_sim* s);

@@ -14,6 +14,9 @@ void lancarAdicionar(const Dev& d, const float* lista, int total, int checar, in
 void lancarEmpacotar(const Dev& d, float* out, int n, cudaStream_t s);
 void lancarDesempacotar(const Dev& d, const float* in, int n, unsigned long long idBase, cudaStream_t s);
 void lancarFerramenta(const Dev& d, int nHint, const tq_tool& f, cudaStream_t s);
+// emitirTorneira's particle list (12 floats each) into a device buffer
+void lancarTorneira(float* lista, int n, uint32_t semente, double cx, double cy, double raio, float vx, float vy,
+                    const float absorb[3], cudaStream_t s);
 
 // grade.cu
 void lancarSolidos(const Dev& d, cudaStream_t s);

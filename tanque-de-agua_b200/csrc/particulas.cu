@@ -459,7 +459,51 @@ __global__ void k_ferramenta(Dev d, tq_tool f) {
   }
 }
 
+// ---------------------------------------------------------------- faucet
+// emitirTorneira (js/principal.js:301-321) on the device, with the LCG of testes/apoio.js:4-9 in
+// place of Math.random: particle k takes the generator's draws 2k+1 and 2k+2 from the seed, reached
+// by jumping the LCG ahead (s -> A s + C composed with itself by squaring), so every thread makes
+// its particle independently and the list equals the one a host loop makes.  In a disk of the
+// jet's radius around (cx, cy): angle a = u1 * pi * 2, radius sqrt(u2) * raio, in the reference's
+// double arithmetic, stored as float; velocity and dye as given, foam and affine terms 0.
+__device__ __forceinline__ uint32_t lcgSalto(uint32_t s, uint32_t k) {
+  uint32_t A = 1664525u, C = 1013904223u, a = 1u, c = 0u;
+  while (k) {
+    if (k & 1u) {
+      a *= A;
+      c = c * A + C;
+    }
+    C = (A + 1u) * C;
+    A *= A;
+    k >>= 1;
+  }
+  return a * s + c;
+}
+__global__ void k_torneira(float* lista, int n, uint32_t semente, double cx, double cy, double raio, float vx, float vy,
+                           float a0, float a1, float a2) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t s1 = lcgSalto(semente, 2u * (uint32_t)k + 1u);
+  const uint32_t s2 = s1 * 1664525u + 1013904223u;
+  const double u1 = s1 / 4294967296.0, u2 = s2 / 4294967296.0;
+  const double a = u1 * 3.141592653589793 * 2, r = sqrt(u2) * raio;
+  float* o = lista + (size_t)k * CAMPOS;
+  o[0] = (float)(cx + cos(a) * r);
+  o[1] = (float)(cy + sin(a) * r);
+  o[2] = vx;
+  o[3] = vy;
+  o[4] = o[5] = o[6] = o[7] = o[8] = 0.0f;
+  o[9] = a0;
+  o[10] = a1;
+  o[11] = a2;
+}
+
 // ---------------------------------------------------------------- host launchers
+void lancarTorneira(float* lista, int n, uint32_t semente, double cx, double cy, double raio, float vx, float vy,
+                    const float absorb[3], cudaStream_t s) {
+  if (n > 0) lanca(k_torneira, blocos(n, 256), 256, 0, s, lista, n, semente, cx, cy, raio, vx, vy, absorb[0], absorb[1],
+                   absorb[2]);
+}
 // ---------------------------------------------------------------- headless splat
 // WGSL_MANCHA (js/gpu/render.js:11-43) without a graphics pipeline: every live particle adds,
 // at each pixel centre of a w x h target covering the tank (row 0 at the top, as the render

@@ -448,6 +448,36 @@ int tq_add_particles(tq_sim* s, const float* list, int32_t n, int32_t check, int
   return TQ_OK;
 }
 
+int tq_emit_faucet(tq_sim* s, const tq_faucet* f, int32_t* accepted) {
+  if (!s || !f) return falha(TQ_E_ARG, "null argument");
+  if (accepted) *accepted = 0;
+  if (!std::isfinite(f->x) || !std::isfinite(f->y) || !(f->radius >= 0) || !std::isfinite(f->vx) ||
+      !std::isfinite(f->vy) || !(f->dt >= 0) || !std::isfinite(f->radius) || !std::isfinite(f->dt))
+    return falha(TQ_E_ARG, "non-finite or negative faucet parameters");
+  // n = min(40000, Math.round((vazao * dt) / h^2 * PARTICULAS_POR_CELULA)), vazao = 2 r max(0.7, |v|)
+  const double h = s->o.h;
+  const double vazao = 2 * f->radius * std::fmax(0.7, std::hypot(f->vx, f->vy));
+  const double nr = std::floor((vazao * f->dt) / (h * h) * PARTICULAS_POR_CELULA + 0.5);
+  const int n = (int)std::fmin(40000.0, nr);
+  if (n <= 0) return TQ_OK;
+  int atual = 0;
+  int st = lerContagem(s, &atual);
+  if (st) return st;
+  if ((long long)atual + n > s->d.cap) return falha(TQ_E_CAPACITY, "particle capacity exceeded");
+  st = garantirStaging(s, (size_t)n * CAMPOS);
+  if (st) return st;
+  const float ab[3] = {(float)f->absorb[0], (float)f->absorb[1], (float)f->absorb[2]};
+  lancarTorneira(s->staging, n, f->seed, f->x, f->y, f->radius, (float)f->vx, (float)f->vy, ab, s->s);
+  lancarAdicionar(s->d, s->staging, n, 1, s->cont, s->offs, s->proximoId, s->s);  // motor.adicionar(lista, true)
+  int a = 0;
+  CK(cudaMemcpyAsync(&a, &s->d.esc->aceitas, sizeof(int), cudaMemcpyDeviceToHost, s->s));
+  CK(cudaStreamSynchronize(s->s));
+  s->proximoId += (unsigned long long)a;
+  s->nHint = atual + a;
+  if (accepted) *accepted = a;
+  return TQ_OK;
+}
+
 int tq_clear_particles(tq_sim* s) {
   if (!s) return falha(TQ_E_ARG, "null handle");
   CK(cudaMemsetAsync(&s->d.esc->n, 0, sizeof(int), s->s));

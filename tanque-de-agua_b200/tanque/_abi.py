@@ -65,6 +65,13 @@ class TqBubbles(C.Structure):
     _fields_ = [("rotulo", C.c_void_p), ("rhs", C.c_void_p), ("y", C.c_void_p)]
 
 
+class TqFaucet(C.Structure):
+    _fields_ = [
+        ("x", C.c_double), ("y", C.c_double), ("radius", C.c_double), ("vx", C.c_double), ("vy", C.c_double),
+        ("dt", C.c_double), ("absorb", C.c_double * 3), ("seed", C.c_uint32), ("pad", C.c_int32),
+    ]
+
+
 class TqAdjScene(C.Structure):
     _fields_ = [
         ("nx", C.c_int32), ("ny", C.c_int32), ("h", C.c_double), ("dt", C.c_double), ("steps", C.c_int32),
@@ -120,6 +127,7 @@ ASSINATURAS = {
 }
 SO_PRODUTO = {
     "advance_graph": (C.c_int, [_P, _D, _I]),
+    "emit_faucet": (C.c_int, [_P, C.POINTER(TqFaucet), C.POINTER(_I)]),
     "adj_create": (C.c_int, [C.POINTER(TqAdjScene), _I, C.POINTER(_P)]),
     "adj_destroy": (C.c_int, [_P]),
     "adj_forward": (C.c_int, [_P, _P, C.POINTER(_D), C.POINTER(_D)]),

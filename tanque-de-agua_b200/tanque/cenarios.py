@@ -287,7 +287,7 @@ def jato_torneira(torneira: dict, quadro: int, dt: float) -> np.ndarray:
     r0 = torneira["raio"]
     vx, vy = torneira["vx"], torneira["vy"]
     vazao = 2 * r0 * max(0.7, math.hypot(vx, vy))
-    n = min(40000, round((vazao * dt) / (h * h) * 4))
+    n = min(40000, math.floor((vazao * dt) / (h * h) * 4 + 0.5))  # Math.round
     al = semente(1000 + quadro)
     lista = np.zeros((n, CAMPOS), dtype=np.float32)
     for k in range(n):

@@ -228,6 +228,19 @@ class SimulacaoGPU(Simulacao):
     def sincronizar(self):
         self._lig("sync", self._h)
 
+    def emitirTorneira(self, torneira: dict, dt: float, semente: int, absorcao=(0.0, 0.0, 0.0)) -> int:
+        """emitirTorneira (js/principal.js:301-321) on the device (tq_emit_faucet): the jet of
+        `torneira` (x, y, raio, vx, vy) for `dt` seconds, the LCG seeded with `semente` in place
+        of Math.random, through adicionar(lista, true).  Returns the particles kept."""
+        f = _abi.TqFaucet()
+        f.x, f.y, f.radius = torneira["x"], torneira["y"], torneira["raio"]
+        f.vx, f.vy, f.dt = torneira["vx"], torneira["vy"], float(dt)
+        f.absorb[0], f.absorb[1], f.absorb[2] = absorcao
+        f.seed = int(semente) & 0xFFFFFFFF
+        aceitas = C.c_int32(0)
+        self._lig("emit_faucet", self._h, C.byref(f), C.byref(aceitas))
+        return aceitas.value
+
     def tracarParede(self, x0, y0, x1, y1, raio, apagar: bool = False):
         """Cena.tracar (js/cena.js:43-72) + atualizarParedes on the device mask (tq_trace_wall).
         The handle's mask then differs from self.cena's until the scene draws the same segment."""

@@ -40,6 +40,9 @@ def test_layout_das_estruturas():
     assert _abi.TqOptions.tolerance.offset == 56
     assert _abi.TqOptions.preconditioner.offset == 84
     assert C.sizeof(_abi.TqSolveInfo) == 40
+    assert C.sizeof(_abi.TqFaucet) == 80
+    assert C.sizeof(_abi.TqAdjScene) == 96
+    assert _abi.TqAdjScene.n_particles.offset == 88
     assert C.sizeof(_abi.TqTool) == 72
     assert C.sizeof(_abi.TqBubbles) == 24
 

@@ -103,3 +103,25 @@ def test_barreira_desiste_e_o_proximo_solve_e_normal(lib_gpu, monkeypatch):
     for campo in ["q", "u", "v"]:
         assert erro_relativo(g.campo(campo), o.campo(campo)) <= 1e-4, campo
     assert g.escalar(_abi.TQ_SCALAR_PCG_CONVERGED) == 1
+
+
+def test_torneira_no_dispositivo(lib_gpu):
+    """tq_emit_faucet (emitirTorneira on the device) against the host generator's list through
+    tq_add_particles(check_full=1), from the same state: the same count kept and the same
+    particles.  Positions to 1e-6 m (the device's cos/sin may round the last double bit
+    differently from the host's before the float store); velocity and dye bit-exact."""
+    from tanque.cenarios import jato_torneira
+    o, g = par("barragem")
+    mesmo_estado(o, g)
+    g2 = SimulacaoGPU(g.cena, {})
+    copiar_estado(o, g2)
+    torneira = dict(x=0.3, y=0.32, raio=0.03, vx=0.4, vy=-1.1, h=g.h)
+    for quadro in range(3):
+        lista = jato_torneira(torneira, quadro, 1 / 60)
+        a_host = g.adicionar(lista, True)
+        a_disp = g2.emitirTorneira(torneira, 1 / 60, 1000 + quadro)
+        assert a_disp == a_host and a_host > 0
+        p1, p2 = g.p.reshape(-1, CAMPOS), g2.p.reshape(-1, CAMPOS)
+        assert p1.shape == p2.shape
+        assert float(np.max(np.abs(p1[:, :2].astype(np.float64) - p2[:, :2]))) <= 1e-6
+        assert np.array_equal(bits(p1[:, 2:]), bits(p2[:, 2:]))
