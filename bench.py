@@ -14,11 +14,12 @@ Every pressure solve stops on the TRUE residual ||b - A q|| <= 1e-6 ||r0|| (FP64
 FP64), with an iteration cap of 1000; each arm reports the fraction of its solves that converged
 and the largest true relative residual.  `value` is the mixed-precision configuration (fused
 engine, FP16 V-cycle storage, block preconditioner, frames replayed from a CUDA graph) timed on
-the device, the faucet's particles added from pinned host memory each frame; `fp32_fused` is the
+the device, the faucet's particles made on the device each frame (tq_emit_faucet); `fp32_fused` is the
 same engine with FP32 storage; `fp32_plain` is the one-launch-per-step FP32 engine with the
 reference's preconditioner (the reference's algorithm on the GPU); `e2e` is the mixed
 configuration through the C-ABI with host buffers (faucet particles in, every particle out, each
-frame).  --impl reference times the CPU oracle (the reference engine's algorithm restated in C++,
+frame; the device-timed arms make the same jet on the device, tq_emit_faucet).  --impl reference
+times the CPU oracle (the reference engine's algorithm restated in C++,
 single-threaded as the reference is) on the same scene.
 With --gpus N > 1 each rank (relaunched under torch.distributed.run when WORLD_SIZE is unset)
 advances its own replica (a tank does not shard).
@@ -262,7 +263,10 @@ def executar_gpu(args, rank, mundo, dist):
         cap = s.opcoes.capacity or math.ceil(NX * NY * 4.6)
         saida = torch.empty(cap * 12, dtype=torch.float32, pin_memory=True).numpy() if e2e else None
         for q in range(args.warmup):
-            s.adicionar(jatos[q], True)
+            if e2e:
+                s.adicionar(jatos[q], True)
+            else:
+                s.emitirTorneira(torneira, DT_QUADRO, 1000 + q)
             avancar(DT_QUADRO, SUB)
         s.sincronizar()
         barreira()
@@ -281,7 +285,11 @@ def executar_gpu(args, rank, mundo, dist):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(ext)
             ent = jatos[args.warmup + q]
-            s.adicionar(ent, True)
+            if e2e:  # the drop-in path: the host's jet list crosses to the device
+                s.adicionar(ent, True)
+                h2d += ent.nbytes
+            else:  # inputs resident: the same jet made on the device (tq_emit_faucet)
+                s.emitirTorneira(torneira, DT_QUADRO, 1000 + args.warmup + q)
             avancar(DT_QUADRO, SUB)
             if e2e:
                 n = C.c_int32(0)
@@ -289,7 +297,6 @@ def executar_gpu(args, rank, mundo, dist):
                 d2h += n.value * 48
             e1.record(ext)
             eventos.append((e0, e1))
-            h2d += ent.nbytes
         s.sincronizar()
         torch.cuda.synchronize()
         if rel:

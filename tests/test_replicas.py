@@ -54,3 +54,22 @@ def test_uma_replica_sem_process_group():
     import bench
     assert list(bench.tempos_max_ranks([1.0, 2.0], None, "cpu")) == [1.0, 2.0]
     assert bench.vazao_replicas(1, 6, 14, 1000.0) == pytest.approx(84.0)
+
+
+def test_bench_lanca_um_rank_por_gpu():
+    """`bench.py --gpus 2` outside torchrun relaunches itself under torch.distributed.run with 2
+    ranks (127.0.0.1); here the CPU reference arm of the adjoint workload, which rank 0 alone runs
+    and prints (the other rank exits 0 without work)."""
+    import json
+    import subprocess
+    env = dict(os.environ)
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    r = subprocess.run([sys.executable, os.path.join(RAIZ, "bench.py"), "--gpus", "2", "--impl", "reference",
+                        "--workload", "adjunto", "--steps", "1", "--cpu-budget", "0.1"],
+                       capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    linhas = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(linhas) == 1  # one line, from rank 0
+    d = json.loads(linhas[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2
