@@ -421,6 +421,7 @@ def executar_lote(args, rank, mundo, dist):
         barreira()
         for s in lote.sims:
             s.tempos(True)
+            s.definirEscalar(_abi.TQ_SCALAR_SOLVES, 0)
         l0 = SimulacaoGPU.lancamentos()
         rel = Relogios(dev) if com_relogio else None
         if rel:
@@ -454,8 +455,18 @@ def executar_lote(args, rank, mundo, dist):
         lanc = SimulacaoGPU.lancamentos() - l0
         ms = sum(a.elapsed_time(b) for a, b in eventos)
         etapas = [s.tempos() for s in lote.sims]
+        # each tank's own true residual at the last solve (registered tanks: fused engine), and
+        # the atlases' solve records
+        piores = []
+        for s in lote.sims:
+            r = s.residuosTanques()
+            if len(r):
+                agua = r[:, 0] > 0
+                piores.append(float(np.max(r[agua, 1] / r[agua, 0])) if agua.any() else 0.0)
+        solves = [estatisticas_solve(s) for s in lote.sims]
         celulas = [at["cena"].nx * at["cena"].ny for at in lote.atlas]
         res = dict(ms=ms, lancamentos=lanc, particulas=lote.n, etapas=etapas, celulas=celulas,
+                   max_rel_tanque=max(piores) if piores else None, solves=solves,
                    atlas=[[at["cena"].nx, at["cena"].ny] for at in lote.atlas], relogios=rel.resumo() if rel else None,
                    d2h=d2h / max(args.steps, 1))
         lote.fechar()
@@ -495,14 +506,20 @@ def executar_lote(args, rank, mundo, dist):
                         f"water 20-70 %, 4 ppc; one step = 1 relabel + {sub} substeps of {DT_QUADRO / sub * 1000:.3f} ms "
                         "for every tank",
             "tank_cells": sum(t["nx"] * t["ny"] for t in todos), "atlases_rank0": misto["atlas"],
+            "atlas_padding_frac_rank0": round(1 - sum(t["nx"] * t["ny"] for t in meus) / sum(misto["celulas"]), 4),
             "atlas_cells_rank0": sum(misto["celulas"]), "particles_rank0": misto["particulas"], "tolerance": TOL,
             "mixed_precision": "fp16 V-cycle storage", "mixed_engine": "fused",
             "l2": "flushed (256 MB write) between timed steps", "parallelism": f"tanks split over {mundo} GPU(s) by cells",
         },
         "fp32_plain": {"value": round(valor_plano, 1), "unit": "tank-substeps/s", "mgpcg_gbs": round(r_p["gbs"], 1),
-                       "pcg_iters_per_atlas_substep": round(r_p["iters"], 2)},
+                       "pcg_iters_per_atlas_substep": round(r_p["iters"], 2),
+                       "stop": "the atlas's true residual as a whole (the plain engine has no per-tank test)",
+                       "solves_per_atlas": plano["solves"]},
         "mixed": {"mgpcg_gbs": round(r_m["gbs"], 1), "pcg_iters_per_atlas_substep": round(r_m["iters"], 2),
-                  "speedup_vs_fp32_plain": round(valor / valor_plano, 3)},
+                  "speedup_vs_fp32_plain": round(valor / valor_plano, 3),
+                  "stop": "every tank's own true residual <= 1e-6 of its own r0 (tq_set_tanks)",
+                  "max_tank_true_rel_residual_last_solve": misto["max_rel_tanque"],
+                  "solves_per_atlas": misto["solves"]},
         "roofline": {"kernel": "MGPCG pressure solve", "bound": "hbm", "achieved": round(r_m["gbs"], 1),
                      "peak": hbm, "peak_source": origem_pico, "unit": "GB/s", "frac": round(r_m["gbs"] / hbm, 4),
                      "traffic": None},

@@ -168,6 +168,18 @@ typedef struct tq_faucet {
 } tq_faucet;
 int tq_emit_faucet(tq_sim* s, const tq_faucet* faucet, int32_t* accepted);
 
+/* Tanks of an atlas (no counterpart in the reference, which steps one tank): n rectangles of
+ * cells, 4 int32 each (x0, y0, width, height), side by side in disjoint column ranges, walls
+ * between them.  The tanks' systems are independent blocks of the atlas's pressure system; in
+ * tolerance mode the solve then stops only when EVERY tank's own true residual is within the
+ * tolerance of ITS OWN initial residual (bubble rows counted with the tank holding the bubble),
+ * not the atlas's as a whole.  FUSED engine only (TQ_E_STATE otherwise); at most 4096 tanks;
+ * n = 0 returns to the whole-grid test. */
+int tq_set_tanks(tq_sim* s, int32_t n, const int32_t* rects);
+/* After a solve with tanks: 2 doubles per tank, ||r0_t|| and the true ||r_t|| at the solve's end
+ * (*n receives the tank count). */
+int tq_get_tank_residuals(tq_sim* s, double* out, int32_t cap, int32_t* n);
+
 /* MotorCPU.limparAgua without the air reset: sim.n = 0, contagemCelula.fill(0)
  * (js/motor.js:95). */
 int tq_clear_particles(tq_sim* s);

@@ -18,6 +18,7 @@ constexpr double GRAVIDADE = 9.81;
 constexpr double DENSIDADE_AGUA = 1000;
 constexpr double TENSAO_SUPERFICIAL = 0.0728;
 constexpr int MAX_BOLHAS = 4096;
+constexpr int MAX_TANQUES = 4096;  // tanks of one atlas (tq_set_tanks)
 constexpr double VOLTA_VOLUME_BOLHA = 0.05;
 constexpr double PRESSAO_BOLHA_MAX = 20000;
 constexpr double PARTICULAS_POR_CELULA = 4;
@@ -130,7 +131,21 @@ struct Dev {
   // reductions
   double* parciais;
   Escalares* esc;
+  // tanks of an atlas (tq_set_tanks): a cell (i, j) belongs to tank colTanque[i] when
+  // y0T[t] <= j < y1T[t]; per tank the squared norms of the initial and the true residual
+  int nTanques;
+  int *colTanque, *y0T, *y1T;
+  double *r0T, *rvT;
+  int* tanqueBolha;  // per bubble label: its tank (-1: none)
 };
+
+// The tank of cell c, or -1 (no tanks, or a cell outside every tank).
+__device__ inline int tanqueDe(const Dev& d, int c) {
+  if (!d.nTanques) return -1;
+  const int i = c % d.nx, j = c / d.nx;
+  const int t = d.colTanque[i];
+  return (t >= 0 && j >= d.y0T[t] && j < d.y1T[t]) ? t : -1;
+}
 
 // ------------------------------------------------------------ helpers
 __host__ __device__ inline int clampi(int v, int a, int b) { return v < a ? a : v > b ? b : v; }

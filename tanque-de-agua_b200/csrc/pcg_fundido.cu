@@ -1516,6 +1516,59 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
   if (threadIdx.x == 0) a.parc[blockIdx.x * NPARC + 0] = tb;
 }
 
+// Per-tank sums of v^2 over the water cells of each tank of an atlas (tq_set_tanks) into destino:
+// a warp-uniform loop over 32-cell segments; a segment inside one tank is reduced by shuffles and
+// added with one FP64 atomic, a segment across tanks adds lane by lane.  Summation order varies
+// with the schedule (FP64 rounding, far below the tolerance); every CTA later reads the same sums.
+__device__ __noinline__ void somarPorTanque(const Args& a, const float* v, double* destino) {
+  const Dev& d = a.d;
+  const int N = d.N, GT = gridDim.x * TF, lane = threadIdx.x & 31;
+  for (int c0 = blockIdx.x * TF + (threadIdx.x & ~31); c0 < N; c0 += GT) {
+    const int c = c0 + lane;
+    int t = -1;
+    double x = 0.0;
+    if (c < N && d.tipo[c] == AGUA) {
+      t = tanqueDe(d, c);
+      if (t >= 0) {
+        x = (double)__ldcg(v + c);
+        x *= x;
+      }
+    }
+    const int t0 = __shfl_sync(0xffffffffu, t, 0);
+    if (__all_sync(0xffffffffu, t == t0)) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0 && t0 >= 0 && x != 0.0) atomicAdd(destino + t0, x);
+    } else if (t >= 0 && x != 0.0) {
+      atomicAdd(destino + t, x);
+    }
+  }
+}
+
+// Every tank's true residual within the tolerance of its own initial one: ||r_t||^2 = the water
+// sums (d.rvT) plus the squared true rows of the tank's bubbles, against tol^2 ||r0_t||^2.  Thread
+// t takes tanks t, t + TF, ..., adding its bubbles in the active list's order, so every CTA
+// reaches the same answer from the same global values (the barrier before made them visible).
+// CTA 0 leaves the totals in d.rvT for tq_get_tank_residuals.
+template <class FB>
+__device__ bool tanquesConvergiram(const Args& a, int nAt, FB rbVerd) {
+  const Dev& d = a.d;
+  bool ok = true;
+  for (int t = threadIdx.x; t < d.nTanques; t += TF) {
+    double s = __ldcg(d.rvT + t);
+    for (int k = 0; k < nAt; k++) {
+      const int b = __ldcg(&a.ativos[k]);
+      if (__ldcg(d.tanqueBolha + b) != t) continue;
+      const double v = rbVerd(b);
+      s += v * v;
+    }
+    const double r0 = __ldcg(d.r0T + t);
+    ok = ok && s <= a.tol * a.tol * r0;
+    if (blockIdx.x == 0) d.rvT[t] = s;
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
 // The true residual of a tolerance-mode solve, in FP64 from the FP64 iterate q64 and the bubble
 // pressures yB: on water cells r = -div - A q (js/pressao-cpu.js:331-338, bubble neighbours
 // through their y), written to d.r in FP32 (the replacement, when it comes to that) and summed
@@ -1558,6 +1611,7 @@ __device__ __noinline__ void faseVerdade(const Args& a, double* sh) {
     a.parc[blockIdx.x * NPARC + 0] = tb;
     a.parc[blockIdx.x * NPARC + 1] = 0.0;
   }
+  if (d.nTanques) somarPorTanque(a, d.r, d.rvT);  // d.r holds the true residual now (FP32)
 }
 
 // The wall-block flags of the levels that have them (Args::sol), both shifts: one warp per
@@ -1694,6 +1748,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       if (i >= 1 && j >= 1 && i < nx - 1 && j < ny - 1) m |= OP_FACE;
     }
     a.op[c] = (uint16_t)(m | (livres << 8));
+    if (d.nTanques && (m & OP_FACE)) d.tanqueBolha[d.rotulo[c] & 0xfffu] = tanqueDe(d, c);  // same for all its cells
     unsigned long long rl = 0;
     if (a.bolhas && (m & (OP_BOLHA | OP_VIZ_BOLHA))) {
       if (m & OP_BOLHA) rl = d.rotulo[c] & 0xfffu;
@@ -1800,6 +1855,9 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     if (threadIdx.x == 0) *a.nWp = base;
   }
   if (!barreira(a, ep)) return;
+  // each tank's ||r0||^2, water rows (r is complete since the barrier; read at the checks, many
+  // barriers later)
+  if (d.nTanques && a.q64) somarPorTanque(a, d.r, d.r0T);
   // rb = rhs - (faces*y - sum) (js/pressao-cpu.js:339-341); norm0
   auto rbInicial = [&](int b) {
     return (double)d.rhsBolhaF[b] - (__ldcg(&d.facesB[b]) * __ldcg(&d.yB[b]) - (double)__ldcg(&d.accB[b]) / ESC);
@@ -1810,6 +1868,10 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     for (int k = threadIdx.x; k < nAt; k += TF) {
       int b = __ldcg(&a.ativos[k]);
       d.rb[b] = rbInicial(b);
+      if (d.nTanques && a.q64) {  // the bubble rows of each tank's ||r0||^2
+        const int t = __ldcg(d.tanqueBolha + b);
+        if (t >= 0) atomicAdd(d.r0T + t, d.rb[b] * d.rb[b]);
+      }
     }
     if (threadIdx.x == 0) {
       d.esc->norma0 = d.esc->norma = norma0;
@@ -1846,6 +1908,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
   double beta = 0.0;
   bool primeira = true;
   int itersFeitas = 0, trocas = 0;
+  bool convergiu = false;
   double normaVerd = -1.0;
   double proxTroca = norma0 * FATOR_TROCA;  // the next residual replacement's threshold
 
@@ -1926,6 +1989,8 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
           a.accZ[b] = 0;
           if (a.q64) a.accV[b] = 0;
         }
+        if (a.q64)
+          for (int t = threadIdx.x; t < d.nTanques; t += TF) d.rvT[t] = 0.0;
       }
       double tb = somaBloco(s, sh);
       if (threadIdx.x == 0) a.parc[blockIdx.x * NPARC + 0] = tb;
@@ -1946,7 +2011,9 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
       };
       somasGlobais(a, nAt, [&](int b) { const double v = rbVerd(b); return v * v; }, [](int) { return 0.0; }, sh, somas);
       normaVerd = sqrt(somas[0] + somas[2]);
-      fim = normaVerd <= a.tol * norma0 || it == a.iteracoes - 1;
+      // with tanks, each tank's own residual decides; without, the whole grid's
+      convergiu = d.nTanques ? tanquesConvergiram(a, nAt, rbVerd) : normaVerd <= a.tol * norma0;
+      fim = convergiu || it == a.iteracoes - 1;
       if (!fim) {
         // replacement: r (water) was rewritten by faseVerdade, the bubble rows follow; the
         // iteration goes on with the same search direction
@@ -1985,7 +2052,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     Escalares* e = d.esc;
-    const bool ok = a.q64 && normaVerd <= a.tol * norma0;
+    const bool ok = a.q64 && convergiu;
     e->normaVerd = a.q64 ? normaVerd : -1.0;
     e->convergiu = ok ? 1 : 0;
     e->trocas = trocas;
@@ -2186,6 +2253,7 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   cudaMemsetAsync(d.facesB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
   cudaMemsetAsync(d.celsB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
   cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
+  if (d.nTanques && tol > 0) cudaMemsetAsync(d.r0T, 0, (size_t)d.nTanques * sizeof(double), s);
   cudaMemsetAsync(f->bar, 0, 2 * sizeof(unsigned), s);
   // f->erro is not cleared here: a solve that gave up keeps it set until erroFundido reads it,
   // and every later solve of the frame then stops at its first barrier instead of waiting.

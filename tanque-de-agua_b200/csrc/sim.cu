@@ -448,6 +448,57 @@ int tq_add_particles(tq_sim* s, const float* list, int32_t n, int32_t check, int
   return TQ_OK;
 }
 
+int tq_set_tanks(tq_sim* s, int32_t n, const int32_t* rects) {
+  if (!s || n < 0 || (n > 0 && !rects)) return falha(TQ_E_ARG, "bad tank list");
+  if (n > MAX_TANQUES) return falha(TQ_E_CAPACITY, "more tanks than an atlas may hold (4096)");
+  if (n > 0 && motorPcg(s->pcg) != TQ_ENGINE_FUSED)
+    return falha(TQ_E_STATE, "per-tank convergence needs the fused engine");
+  std::vector<int> col(s->nx, -1), y0(n > 0 ? n : 1), y1(n > 0 ? n : 1);
+  for (int t = 0; t < n; t++) {
+    const int x0 = rects[4 * t], yy = rects[4 * t + 1], w = rects[4 * t + 2], hh = rects[4 * t + 3];
+    if (x0 < 0 || yy < 0 || w < 1 || hh < 1 || x0 + w > s->nx || yy + hh > s->ny)
+      return falha(TQ_E_ARG, "tank rectangle outside the grid");
+    for (int i = x0; i < x0 + w; i++) {
+      if (col[i] >= 0) return falha(TQ_E_ARG, "tanks must occupy disjoint column ranges");
+      col[i] = t;
+    }
+    y0[t] = yy;
+    y1[t] = yy + hh;
+  }
+  Dev& d = s->d;
+  if (!d.colTanque) {
+    if (!aloca(s, &d.colTanque, s->nx) || !aloca(s, &d.y0T, MAX_TANQUES) || !aloca(s, &d.y1T, MAX_TANQUES) ||
+        !aloca(s, &d.r0T, MAX_TANQUES) || !aloca(s, &d.rvT, MAX_TANQUES) || !aloca(s, &d.tanqueBolha, MAX_BOLHAS))
+      return falha(TQ_E_NOMEM, "device allocation failed");
+  }
+  CK(cudaMemcpyAsync(d.colTanque, col.data(), sizeof(int) * s->nx, cudaMemcpyHostToDevice, s->s));
+  if (n > 0) {
+    CK(cudaMemcpyAsync(d.y0T, y0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s->s));
+    CK(cudaMemcpyAsync(d.y1T, y1.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s->s));
+    CK(cudaMemsetAsync(d.r0T, 0, sizeof(double) * n, s->s));
+    CK(cudaMemsetAsync(d.rvT, 0, sizeof(double) * n, s->s));
+  }
+  CK(cudaStreamSynchronize(s->s));
+  d.nTanques = n;
+  return TQ_OK;
+}
+
+int tq_get_tank_residuals(tq_sim* s, double* out, int32_t cap, int32_t* n) {
+  if (!s) return falha(TQ_E_ARG, "null handle");
+  const int nt = s->d.nTanques;
+  if (n) *n = nt;
+  if (!out || nt == 0) return TQ_OK;
+  std::vector<double> r0(nt), rv(nt);
+  CK(cudaMemcpyAsync(r0.data(), s->d.r0T, sizeof(double) * nt, cudaMemcpyDeviceToHost, s->s));
+  CK(cudaMemcpyAsync(rv.data(), s->d.rvT, sizeof(double) * nt, cudaMemcpyDeviceToHost, s->s));
+  CK(cudaStreamSynchronize(s->s));
+  for (int t = 0; t < nt && 2 * t + 1 < cap; t++) {
+    out[2 * t] = std::sqrt(r0[t]);
+    out[2 * t + 1] = std::sqrt(rv[t]);
+  }
+  return TQ_OK;
+}
+
 int tq_emit_faucet(tq_sim* s, const tq_faucet* f, int32_t* accepted) {
   if (!s || !f) return falha(TQ_E_ARG, "null argument");
   if (accepted) *accepted = 0;

@@ -128,6 +128,8 @@ ASSINATURAS = {
 SO_PRODUTO = {
     "advance_graph": (C.c_int, [_P, _D, _I]),
     "emit_faucet": (C.c_int, [_P, C.POINTER(TqFaucet), C.POINTER(_I)]),
+    "set_tanks": (C.c_int, [_P, _I, _P]),
+    "get_tank_residuals": (C.c_int, [_P, C.POINTER(_D), _I, C.POINTER(_I)]),
     "adj_create": (C.c_int, [C.POINTER(TqAdjScene), _I, C.POINTER(_P)]),
     "adj_destroy": (C.c_int, [_P]),
     "adj_forward": (C.c_int, [_P, _P, C.POINTER(_D), C.POINTER(_D)]),

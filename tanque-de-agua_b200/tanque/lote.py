@@ -34,6 +34,7 @@ import math
 
 import numpy as np
 
+from . import _abi
 from .cenarios import raio_de_parede, semear_retangulo_rapido, semente
 from .constantes import CAMPOS, MOLDURA, SDF_MAX
 
@@ -161,6 +162,13 @@ class Lote:
             at = montar_atlas(Cena, [tanques[k] for k in g], h, margem)
             sim = fabrica(at["cena"], dict(opcoes or {}))
             sim.adicionar(at["particulas"], False)
+            # every tank's own convergence (tq_set_tanks) where the engine offers it: the fused
+            # engine in tolerance mode
+            o = dict(opcoes or {})
+            if (hasattr(sim, "definirTanques") and o.get("tolerance", 0) > 0
+                    and o.get("engine", _abi.TQ_ENGINE_PLAIN) == _abi.TQ_ENGINE_FUSED):
+                sim.definirTanques([(x0, y0, tanques[k]["nx"], tanques[k]["ny"])
+                                    for x0, y0, k in zip(at["x0"], at["y0"], g)])
             self.atlas.append(at)
             self.sims.append(sim)
             for i, k in enumerate(g):

@@ -228,6 +228,21 @@ class SimulacaoGPU(Simulacao):
     def sincronizar(self):
         self._lig("sync", self._h)
 
+    def definirTanques(self, retangulos):
+        """The tanks of an atlas (tq_set_tanks): (x0, y0, largura, altura) in cells each, in
+        disjoint column ranges.  In tolerance mode every tank's own true residual must then meet
+        the tolerance of its own initial residual.  Fused engine only."""
+        r = np.ascontiguousarray(np.asarray(retangulos, dtype=np.int32).reshape(-1, 4))
+        self._lig("set_tanks", self._h, len(r), r.ctypes.data if len(r) else None)
+
+    def residuosTanques(self) -> np.ndarray:
+        """(tanks, 2): ||r0|| and the true ||r|| of each tank at the last solve's end."""
+        n = C.c_int32(0)
+        self._lig("get_tank_residuals", self._h, None, 0, C.byref(n))
+        buf = (C.c_double * (2 * max(n.value, 1)))()
+        self._lig("get_tank_residuals", self._h, buf, 2 * n.value, C.byref(n))
+        return np.array(buf[: 2 * n.value]).reshape(-1, 2)
+
     def emitirTorneira(self, torneira: dict, dt: float, semente: int, absorcao=(0.0, 0.0, 0.0)) -> int:
         """emitirTorneira (js/principal.js:301-321) on the device (tq_emit_faucet): the jet of
         `torneira` (x, y, raio, vx, vy) for `dt` seconds, the LCG seeded with `semente` in place

@@ -101,3 +101,25 @@ def test_lote_no_gpu(lib_gpu):
         assert np.all(np.isfinite(q[:, :4]))
         assert np.all(q[:, 0] > 0) and np.all(q[:, 0] < t[k]["nx"] * H)
     lote.fechar()
+
+
+@pytest.mark.parametrize("precond", [_abi.TQ_PRECOND_REFERENCE, _abi.TQ_PRECOND_BLOCK], ids=["referencia", "bloco"])
+def test_cada_tanque_converge_sozinho(lib_gpu, precond):
+    """With the atlas's tanks registered (tq_set_tanks, done by Lote for the fused engine in
+    tolerance mode) every solve stops only when each tank's true residual is within 1e-6 of
+    its own initial residual: checked on every tank after every substep of two frames."""
+    t = _tanques()
+    opc = dict(SOLVE, iterations=1000, precision=_abi.TQ_PREC_FP16, engine=_abi.TQ_ENGINE_FUSED,
+               preconditioner=precond)
+    lote = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, t, H, opc, limite_grosso=300)
+    for _ in range(2):
+        for s in lote.sims:
+            s.atualizarAr()
+            for _ in range(3):
+                s.subpasso(1 / 240)
+                r = s.residuosTanques()
+                assert len(r) > 0
+                agua = r[:, 0] > 0
+                assert np.all(r[agua, 1] <= 1e-6 * r[agua, 0]), r[agua]
+                assert s.escalar(_abi.TQ_SCALAR_PCG_CONVERGED) == 1
+    lote.fechar()
