@@ -486,10 +486,16 @@ __global__ void k_adj_somar(const double* parc, int m, double* out) {
 }
 
 // ---------------------------------------------------------------- CG kernels
+// The CG's scalars live on the device (esc): [0] ||b||^2, [1] alpha, [2] beta, [3] r.z, [4] the
+// latest dot, [5] a second dot, [6] the stop flag (as a double: 0 running, 1 stopped).  Every
+// update kernel returns at once after the flag is set, so the host reads it every few
+// iterations only and the result is that of stopping at the exact iteration.
+enum { E_B2 = 0, E_AL = 1, E_BE = 2, E_RZ = 3, E_D1 = 4, E_D2 = 5, E_PARA = 6 };
+
 // A v on water cells (js/pressao-cpu.js:84-93, true types; air is 0)
-__global__ void k_adj_aplicar(Dispositivo D, const uint8_t* tipo, const double* v, double* out) {
+__global__ void k_adj_aplicar(Dispositivo D, const uint8_t* tipo, const double* v, double* out, const double* esc) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= D.N) return;
+  if (c >= D.N || (esc && esc[E_PARA] != 0)) return;
   if (tipo[c] != AGUA) { out[c] = 0; return; }
   const int nx = D.nx, ny = D.ny, i = c % nx, j = c / nx;
   int k = 0;
@@ -504,34 +510,66 @@ __global__ void k_adj_aplicar(Dispositivo D, const uint8_t* tipo, const double* 
   }
   out[c] = k * v[c] - s;
 }
-__global__ void k_adj_axpy2(int n, const uint8_t* tipo, const double* al, double* q, const double* p, double* r,
+__global__ void k_adj_axpy2(int n, const uint8_t* tipo, const double* esc, double* q, const double* p, double* r,
                             const double* ap) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n || tipo[c] != AGUA) return;
-  const double a = *al;
+  if (c >= n || tipo[c] != AGUA || esc[E_PARA] != 0) return;
+  const double a = esc[E_AL];
   q[c] += a * p[c];
   r[c] -= a * ap[c];
 }
-__global__ void k_adj_direcao(int n, const uint8_t* tipo, const double* be, const double* z, double* p) {
+__global__ void k_adj_direcao(int n, const uint8_t* tipo, const double* esc, const double* z, double* p) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  p[c] = tipo[c] == AGUA ? z[c] + *be * p[c] : 0.0;
+  if (c >= n || esc[E_PARA] != 0) return;
+  p[c] = tipo[c] == AGUA ? z[c] + esc[E_BE] * p[c] : 0.0;
 }
-__global__ void k_adj_para_float(int n, const uint8_t* tipo, const double* r, double escala, float* b) {
+// z from the FP32 V-cycle: r scaled to unit norm (esc[E_D1] = ||r||^2) before, back after
+__global__ void k_adj_para_float(int n, const uint8_t* tipo, const double* r, const double* esc, int qual, float* b) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
-  b[c] = tipo[c] == AGUA ? (float)(r[c] * escala) : 0.0f;
+  const double nr = sqrt(esc[qual]);
+  b[c] = tipo[c] == AGUA ? (float)(r[c] * (nr > 0 ? 1.0 / nr : 1.0)) : 0.0f;
 }
-__global__ void k_adj_de_float(int n, const uint8_t* tipo, const float* x, double escala, double* z) {
+__global__ void k_adj_de_float(int n, const uint8_t* tipo, const float* x, const double* esc, int qual, double* z) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  z[c] = tipo[c] == AGUA ? (double)x[c] * escala : 0.0;
+  if (c >= n || esc[E_PARA] != 0) return;
+  const double nr = sqrt(esc[qual]);
+  z[c] = tipo[c] == AGUA ? (double)x[c] * (nr > 0 ? nr : 1.0) : 0.0;
 }
 __global__ void k_adj_mascarar(int n, const uint8_t* tipo, const double* b, double* r, double* q) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   r[c] = tipo[c] == AGUA ? b[c] : 0.0;
   q[c] = 0.0;
+}
+__global__ void k_adj_copiar_se(double* dst, const double* src, size_t n, const double* esc) {
+  if (esc[E_PARA] != 0) return;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    dst[k] = src[k];
+}
+// the scalar steps of one CG iteration (one thread): modo 0 start (||b||^2 in E_D1 -> E_B2, the
+// flag cleared, rz from E_D2); 1 alpha = rz / p.Ap (E_D1); 2 the stop test on r.r (E_D1);
+// 3 Polak-Ribiere beta from r.z (E_D1) and r.zOld (E_D2)
+__global__ void k_adj_escalares(double* esc, int modo, double tol2) {
+  if (modo == 0) {
+    esc[E_B2] = esc[E_D1];
+    esc[E_PARA] = esc[E_B2] == 0 ? 1.0 : 0.0;
+    return;
+  }
+  if (esc[E_PARA] != 0) return;
+  if (modo == 1) {
+    const double pap = esc[E_D1];
+    if (pap == 0) esc[E_PARA] = 1.0;
+    else esc[E_AL] = esc[E_RZ] / pap;
+  } else if (modo == 2) {
+    if (esc[E_D1] <= tol2 * esc[E_B2]) esc[E_PARA] = 1.0;
+  } else if (modo == 3) {
+    const double rzn = esc[E_D1], cruz = esc[E_D2];
+    esc[E_BE] = fmax(0.0, (rzn - cruz) / esc[E_RZ]);
+    esc[E_RZ] = rzn;
+  } else if (modo == 4) {
+    esc[E_RZ] = esc[E_D1];
+  }
 }
 
 // ---------------------------------------------------------------- backward kernels
@@ -765,10 +803,6 @@ __global__ void k_adj_p2g_T(Dispositivo D, Fita f, int cap, const double* Ub, co
 __global__ void k_adj_zerar(double* a, size_t n) {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) a[k] = 0;
 }
-__global__ void k_adj_copiar(double* dst, const double* src, size_t n) {
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-    dst[k] = src[k];
-}
 __global__ void k_adj_saida_v(Estado B, int n, double escala, float* dv) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -825,7 +859,7 @@ struct tq_adj {
   double *bufB, *bufBin;  // 8 x cap
   double *ugb, *vgb, *ugb2, *vgb2, *qb, *lam, *Ub, *UWb, *Vb, *VWb;
   // CG
-  double *r, *z, *zv, *p, *ap, *parc, *esc;  // esc: [0] dot, [1] alpha, [2] beta
+  double *r, *z, *zv, *p, *ap, *parc, *esc;  // esc: the CG's scalars (E_*) and a host-read slot
   float *bf, *xf;
   double gth[2] = {0, 0};
 };
@@ -852,59 +886,79 @@ Estado estado(double* buf, int cap) {
 int gridDe(long n) { return (int)((n + TB - 1) / TB); }
 
 double somaHost(tq_adj* a, const double* x, const double* y, int n) {
+  // slot 7 of esc: apart from the CG's scalars
   contarLancamento();
   k_adj_produto<<<SOMA_CTAS, TB, 0, a->s>>>(x, y, n, a->parc);
   contarLancamento();
-  k_adj_somar<<<1, TB, 0, a->s>>>(a->parc, SOMA_CTAS, a->esc);
+  k_adj_somar<<<1, TB, 0, a->s>>>(a->parc, SOMA_CTAS, a->esc + 7);
   double v = 0;
-  cudaMemcpyAsync(&v, a->esc, sizeof v, cudaMemcpyDeviceToHost, a->s);
+  cudaMemcpyAsync(&v, a->esc + 7, sizeof v, cudaMemcpyDeviceToHost, a->s);
   cudaStreamSynchronize(a->s);
   return v;
 }
 
-// A x = b on the water cells of `tipo` (device), x in a->q: CG in FP64 preconditioned by the FP32
-// V-cycle, Polak-Ribiere beta, to ||r|| <= 1e-12 ||b||.  Returns TQ_OK or an error.
+// a . b (b null: sum of a) into esc[slot] on the device (deterministic two-pass sum)
+void somaDisp(tq_adj* a, const double* x, const double* y, int n, double* destino) {
+  contarLancamento();
+  k_adj_produto<<<SOMA_CTAS, TB, 0, a->s>>>(x, y, n, a->parc);
+  contarLancamento();
+  k_adj_somar<<<1, TB, 0, a->s>>>(a->parc, SOMA_CTAS, destino);
+}
+
+// A x = b on the water cells of `tipo` (device): CG in FP64 preconditioned by the FP32 V-cycle,
+// Polak-Ribiere beta, to ||r|| <= 1e-12 ||b||.  The scalars stay on the device; the host reads
+// the stop flag every VERIFICAR iterations.  Returns TQ_OK or an error.
+constexpr int VERIFICAR = 8;
 int resolver(tq_adj* a, const uint8_t* tipo, const double* bdev, double* x) {
   const int N = a->N;
   const int g = gridDe(N);
-  contarLancamento();
-  k_adj_mascarar<<<g, TB, 0, a->s>>>(N, tipo, bdev, a->r, x);
-  const double nb2 = somaHost(a, a->r, a->r, N);
-  if (nb2 == 0) return TQ_OK;
-  auto precond = [&](double nr) {  // z = M r (the V-cycle on r scaled to unit norm)
-    const double es = nr > 0 ? 1.0 / nr : 1.0;
+  cudaStream_t st = a->s;
+  double* esc = a->esc;
+  auto escalares = [&](int modo) {
     contarLancamento();
-    k_adj_para_float<<<g, TB, 0, a->s>>>(N, tipo, a->r, es, a->bf);
-    int st = cicloVDispositivo(a->pcg, tipo, a->bf, a->xf, a->s);
-    contarLancamento();
-    k_adj_de_float<<<g, TB, 0, a->s>>>(N, tipo, a->xf, 1.0 / es, a->z);
-    return st;
+    k_adj_escalares<<<1, 1, 0, st>>>(esc, modo, TOL_SOLVE * TOL_SOLVE);
   };
-  double nr = std::sqrt(nb2);
-  if (precond(nr)) return TQ_E_CUDA;
+  auto precond = [&](int qual) {  // z = M r (the V-cycle on r scaled to unit norm; ||r||^2 in esc[qual])
+    contarLancamento();
+    k_adj_para_float<<<g, TB, 0, st>>>(N, tipo, a->r, esc, qual, a->bf);
+    int e = cicloVDispositivo(a->pcg, tipo, a->bf, a->xf, st);
+    contarLancamento();
+    k_adj_de_float<<<g, TB, 0, st>>>(N, tipo, a->xf, esc, qual, a->z);
+    return e;
+  };
   contarLancamento();
-  k_adj_copiar<<<g, TB, 0, a->s>>>(a->p, a->z, N);
-  double rz = somaHost(a, a->r, a->z, N);
+  k_adj_mascarar<<<g, TB, 0, st>>>(N, tipo, bdev, a->r, x);
+  somaDisp(a, a->r, a->r, N, esc + E_D1);
+  escalares(0);  // ||b||^2, flag
+  if (precond(E_B2)) return TQ_E_CUDA;
+  contarLancamento();
+  k_adj_copiar_se<<<g, TB, 0, st>>>(a->p, a->z, N, esc);
+  somaDisp(a, a->r, a->z, N, esc + E_D1);
+  escalares(4);  // rz
   for (int it = 0; it < 2000; it++) {
     contarLancamento();
-    k_adj_aplicar<<<g, TB, 0, a->s>>>(a->D, tipo, a->p, a->ap);
-    const double pap = somaHost(a, a->p, a->ap, N);
-    if (pap == 0) break;
-    const double al = rz / pap;
-    cudaMemcpyAsync(a->esc + 1, &al, sizeof al, cudaMemcpyHostToDevice, a->s);
+    k_adj_aplicar<<<g, TB, 0, st>>>(a->D, tipo, a->p, a->ap, esc);
+    somaDisp(a, a->p, a->ap, N, esc + E_D1);
+    escalares(1);  // alpha
     contarLancamento();
-    k_adj_axpy2<<<g, TB, 0, a->s>>>(N, tipo, a->esc + 1, x, a->p, a->r, a->ap);
-    const double rr = somaHost(a, a->r, a->r, N);
-    if (rr <= TOL_SOLVE * TOL_SOLVE * nb2) return TQ_OK;
+    k_adj_axpy2<<<g, TB, 0, st>>>(N, tipo, esc, x, a->p, a->r, a->ap);
+    somaDisp(a, a->r, a->r, N, esc + E_D1);
+    escalares(2);  // stop test
     contarLancamento();
-    k_adj_copiar<<<g, TB, 0, a->s>>>(a->zv, a->z, N);
-    if (precond(std::sqrt(rr))) return TQ_E_CUDA;
-    const double rzn = somaHost(a, a->r, a->z, N), cruz = somaHost(a, a->r, a->zv, N);
-    const double be = std::fmax(0.0, (rzn - cruz) / rz);
-    rz = rzn;
-    cudaMemcpyAsync(a->esc + 2, &be, sizeof be, cudaMemcpyHostToDevice, a->s);
+    k_adj_copiar_se<<<g, TB, 0, st>>>(a->zv, a->z, N, esc);
+    if (precond(E_D1)) return TQ_E_CUDA;
+    somaDisp(a, a->r, a->z, N, esc + E_D1);
+    somaDisp(a, a->r, a->zv, N, esc + E_D2);
+    escalares(3);  // beta
     contarLancamento();
-    k_adj_direcao<<<g, TB, 0, a->s>>>(N, tipo, a->esc + 2, a->z, a->p);
+    k_adj_direcao<<<g, TB, 0, st>>>(N, tipo, esc, a->z, a->p);
+    if (it % VERIFICAR == VERIFICAR - 1) {
+      double para = 0;
+      if (cudaMemcpyAsync(&para, esc + E_PARA, sizeof para, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess)
+        return TQ_E_CUDA;
+      if (para != 0) return TQ_OK;
+    }
   }
   std::snprintf(g_erroAdj, sizeof g_erroAdj, "adjoint pressure solve did not reach 1e-12 in 2000 iterations");
   return TQ_E_TIMEOUT;
@@ -1042,7 +1096,7 @@ int tq_adj_create(const tq_adj_scene* d, int32_t device, tq_adj** out) {
        alocar(a, &a->ugb2, nu) && alocar(a, &a->vgb2, nv) && alocar(a, &a->qb, N) && alocar(a, &a->lam, N) &&
        alocar(a, &a->Ub, nu) && alocar(a, &a->UWb, nu) && alocar(a, &a->Vb, nv) && alocar(a, &a->VWb, nv) &&
        alocar(a, &a->r, N) && alocar(a, &a->z, N) && alocar(a, &a->zv, N) && alocar(a, &a->p, N) &&
-       alocar(a, &a->ap, N) && alocar(a, &a->parc, SOMA_CTAS) && alocar(a, &a->esc, 4) && alocar(a, &a->bf, N) &&
+       alocar(a, &a->ap, N) && alocar(a, &a->parc, SOMA_CTAS) && alocar(a, &a->esc, 8) && alocar(a, &a->bf, N) &&
        alocar(a, &a->xf, N);
   if (ok) a->pcg = criarPcg(d->nx, d->ny, TQ_PREC_FP32, TQ_ENGINE_PLAIN);
   if (!ok || !a->pcg) {
