@@ -403,11 +403,20 @@ def executar_lote(args, rank, mundo, dist):
         if dist is not None:
             dist.barrier()
 
-    def medir(precisao, motor, com_relogio=False, e2e=False):
+    def opcoes(precisao, motor):
         precond = _abi.TQ_PRECOND_BLOCK if motor == _abi.TQ_ENGINE_FUSED else _abi.TQ_PRECOND_REFERENCE
-        lote = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H,
-                    {"tolerance": TOL, "iterations": MAX_ITER, "precision": precisao, "engine": motor,
-                     "preconditioner": precond, "device": dev})
+        return {"tolerance": TOL, "iterations": MAX_ITER, "precision": precisao, "engine": motor,
+                "preconditioner": precond, "device": dev}
+
+    # the atlas grouping, chosen by measuring candidates (tanque.lote.autoajustar) on the mixed
+    # configuration, before any timed or warm-up frame
+    from tanque.lote import autoajustar
+    limite, ajuste = autoajustar(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H,
+                                 opcoes(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED), DT_QUADRO, sub)
+
+    def medir(precisao, motor, com_relogio=False, e2e=False):
+        grafo = motor == _abi.TQ_ENGINE_FUSED
+        lote = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H, opcoes(precisao, motor), limite_grosso=limite)
         fluxos = [torch.cuda.ExternalStream(s.stream()) for s in lote.sims]
         lig = _abi.carregar()
         saidas = []
@@ -416,7 +425,7 @@ def executar_lote(args, rank, mundo, dist):
                 cap = s.n + 16
                 saidas.append((torch.empty(cap * 12, dtype=torch.float32, pin_memory=True).numpy(), cap))
         for q in range(args.warmup):
-            lote.avancar(DT_QUADRO, sub)
+            lote.avancar(DT_QUADRO, sub, grafo=grafo)
         lote.sincronizar()
         barreira()
         for s in lote.sims:
@@ -435,7 +444,7 @@ def executar_lote(args, rank, mundo, dist):
             e0.record(p0)
             for f in fluxos[1:]:
                 f.wait_event(e0)
-            lote.avancar(DT_QUADRO, sub)
+            lote.avancar(DT_QUADRO, sub, grafo=grafo)
             if e2e:
                 for s, (buf, cap) in zip(lote.sims, saidas):
                     n = C.c_int32(0)
@@ -507,8 +516,11 @@ def executar_lote(args, rank, mundo, dist):
                         "for every tank",
             "tank_cells": sum(t["nx"] * t["ny"] for t in todos), "atlases_rank0": misto["atlas"],
             "atlas_padding_frac_rank0": round(1 - sum(t["nx"] * t["ny"] for t in meus) / sum(misto["celulas"]), 4),
+            "autotuner": {"coarsest_level_limit": limite,
+                          "seconds_per_frame_by_limit": {str(k): round(v, 4) for k, v in ajuste.items()}},
             "atlas_cells_rank0": sum(misto["celulas"]), "particles_rank0": misto["particulas"], "tolerance": TOL,
-            "mixed_precision": "fp16 V-cycle storage", "mixed_engine": "fused",
+            "mixed_precision": "fp16 V-cycle storage",
+            "mixed_engine": "fused, block preconditioner, each atlas's frame replayed from a CUDA graph",
             "l2": "flushed (256 MB write) between timed steps", "parallelism": f"tanks split over {mundo} GPU(s) by cells",
         },
         "fp32_plain": {"value": round(valor_plano, 1), "unit": "tank-substeps/s", "mgpcg_gbs": round(r_p["gbs"], 1),

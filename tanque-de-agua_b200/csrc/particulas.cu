@@ -151,11 +151,31 @@ __device__ inline void velocidadeEm(const Dev& d, double x, double y, double vma
 // clamp, micro-steps through the projected grid velocity with SDF push-out, kill when deep
 // in a wall.  Dead particles get x = NaN and are removed by the compaction at the end of the
 // call (the reference removes them at the end of the same loop, :636).
+// The largest speed of the warp's live particles into *alvo (double bits; speeds are >= 0, so
+// their bits order as unsigned integers): the high words' maximum, then the low words' among the
+// lanes holding it, each by one __reduce_max_sync, and one atomicMax per warp instead of one per
+// particle on a single address.
+__device__ __forceinline__ void maxVelocidadeWarp(unsigned ativos, double vel, unsigned long long* alvo) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(vel);
+  const unsigned hi = (unsigned)(b >> 32), lo = (unsigned)b;
+  const unsigned mhi = __reduce_max_sync(ativos, hi);
+  const unsigned comMax = __ballot_sync(ativos, hi == mhi);
+  if (hi == mhi) {
+    const unsigned mlo = __reduce_max_sync(comMax, lo);
+    if ((int)(threadIdx.x & 31) == __ffs(comMax) - 1) {
+      const unsigned long long m = ((unsigned long long)mhi << 32) | mlo;
+      if (m) atomicMax(alvo, m);
+    }
+  }
+}
+
 __global__ void k_g2p(Dev d, double dt) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= d.esc->n) return;
-  const float4 a = d.p0[k];
-  if (!(a.x == a.x)) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool dentro = k < d.esc->n;
+  const float4 a = dentro ? d.p0[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const bool vivo = dentro && a.x == a.x;  // a particle marked dead earlier is skipped
+  const unsigned ativos = __ballot_sync(0xffffffffu, vivo);  // every lane of the warp takes part
+  if (!vivo) return;
   const float4 e = d.p2[k];
   const int nx = d.nx, ny = d.ny;
   const double h = d.h;
@@ -210,7 +230,7 @@ __global__ void k_g2p(Dev d, double dt) {
     abs2 = (float)((double)abs2 + (c2 / n - (double)abs2) * mistura);
   }
   if (vel > vmax) { vx *= vmax / vel; vy *= vmax / vel; }
-  if (vel > 0) atomicMax(&d.esc->vmaxBits, (unsigned long long)__double_as_longlong(vel));
+  maxVelocidadeWarp(ativos, vel > 0 ? vel : 0.0, &d.esc->vmaxBits);  // (NaN and 0 leave the maximum alone)
   double micro = fmin(MAX_MICROPASSOS, fmax(1.0, ceil((fmin(vel, vmax) * dt) / (MICROPASSO * h))));
   double dm = dt / micro;
   int nm = (int)micro;

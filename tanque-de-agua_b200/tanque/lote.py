@@ -186,10 +186,14 @@ class Lote:
     def n(self) -> int:
         return sum(s.n for s in self.sims)
 
-    def avancar(self, dt: float, subpassos: int = 1):
-        """One frame of every atlas (each on its simulation's stream)."""
+    def avancar(self, dt: float, subpassos: int = 1, grafo: bool = False):
+        """One frame of every atlas (each on its simulation's stream); with `grafo` the
+        substeps replay from each atlas's CUDA graph (tq_advance_graph) where available."""
         for s in self.sims:
-            s.avancar(dt, subpassos)
+            if grafo and hasattr(s, "avancarGrafo"):
+                s.avancarGrafo(dt, subpassos)
+            else:
+                s.avancar(dt, subpassos)
 
     def sincronizar(self):
         for s in self.sims:
@@ -225,6 +229,32 @@ class Lote:
         for s in self.sims:
             if hasattr(s, "fechar"):
                 s.fechar()
+
+
+def autoajustar(fabrica, Cena, tanques: list[dict], h: float, opcoes: dict, dt: float, subpassos: int,
+                candidatos=(3000, 6000, 12000), repeticoes: int = 1) -> tuple[int, dict]:
+    """The atlas grouping by measurement: for each candidate limit of the coarsest level's cells
+    (which sets how many atlases the batch makes, their padding, and each atlas's V-cycle depth
+    and coarsest-level size), build the batch, run one warm-up frame, then time `repeticoes`
+    frames of every atlas (wall time after the handles' streams drain), and keep the fastest.
+    Candidates whose coarsest level exceeds what the fused solver's CTA 0 holds are skipped by
+    the grouping itself.  Returns (limit, {limit: seconds per frame})."""
+    import time
+    tempos = {}
+    for lim in candidatos:
+        lote = Lote(fabrica, Cena, tanques, h, opcoes, limite_grosso=lim)
+        try:
+            lote.avancar(dt, subpassos, grafo=True)
+            lote.sincronizar()
+            t0 = time.perf_counter()
+            for _ in range(repeticoes):
+                lote.avancar(dt, subpassos, grafo=True)
+            lote.sincronizar()
+            tempos[lim] = (time.perf_counter() - t0) / repeticoes
+        finally:
+            lote.fechar()
+    melhor = min(tempos, key=lambda k: (tempos[k], k))
+    return melhor, tempos
 
 
 def repartir(tanques: list[dict], partes: int) -> list[list[int]]:
