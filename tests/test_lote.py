@@ -146,3 +146,33 @@ def test_repartir_entre_gpus(partes):
     cargas = [sum(t[k]["nx"] * t[k]["ny"] for k in g) for g in grupos]
     maior = max(x["nx"] * x["ny"] for x in t)
     assert max(cargas) - min(cargas) <= maior  # LPT: within one tank of balance
+
+
+def test_autoajuste_escolhe_o_mais_rapido():
+    """tanque.lote.autoajustar builds the batch per candidate grouping, times its frames and keeps
+    the fastest (here a fake simulation whose frame costs a fixed time per atlas plus a time per
+    atlas cell: the candidates trade atlas count against padding)."""
+    import time as _t
+
+    from tanque import Cena
+    from tanque.lote import Lote, autoajustar, gerar_tanques
+
+    class Falsa:
+        def __init__(self, cena, opcoes):
+            self.celulas = cena.nx * cena.ny
+
+        def adicionar(self, p, checar):
+            return 0
+
+        def avancar(self, dt, sub):
+            _t.sleep(0.004 + self.celulas * 2e-8)
+
+        def sincronizar(self):
+            pass
+
+    t = gerar_tanques(n=24, s=9, h=1 / 128, largura=(40, 160), altura=(30, 120))
+    melhor, tempos = autoajustar(Falsa, Cena, t, 1 / 128, {}, 1 / 60, 2, candidatos=(200, 800, 3200))
+    assert set(tempos) == {200, 800, 3200}
+    assert melhor == min(tempos, key=tempos.get)
+    grupos = {lim: len(Lote(Falsa, Cena, t, 1 / 128, {}, limite_grosso=lim).atlas) for lim in tempos}
+    assert grupos[200] >= grupos[800] >= grupos[3200]  # a larger limit makes fewer atlases
