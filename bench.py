@@ -411,12 +411,17 @@ def executar_lote(args, rank, mundo, dist):
     # the atlas grouping, chosen by measuring candidates (tanque.lote.autoajustar) on the mixed
     # configuration, before any timed or warm-up frame
     from tanque.lote import autoajustar
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
     limite, ajuste = autoajustar(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H,
-                                 opcoes(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED), DT_QUADRO, sub)
+                                 opcoes(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED), DT_QUADRO, sub, sms=sms)
 
-    def medir(precisao, motor, com_relogio=False, e2e=False):
-        grafo = motor == _abi.TQ_ENGINE_FUSED
-        lote = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H, opcoes(precisao, motor), limite_grosso=limite)
+    def medir(precisao, motor, com_relogio=False, e2e=False, grafo=None):
+        """Frames of the batch (`grafo`: each atlas's frame from its CUDA graph, the default
+        for the fused engine, with the SMs split between the atlases so their frames run side
+        by side); stage timing is recorded by eager frames only, each atlas on the whole GPU."""
+        grafo = motor == _abi.TQ_ENGINE_FUSED if grafo is None else grafo
+        lote = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H, opcoes(precisao, motor), limite_grosso=limite,
+                    sms=sms if grafo else None)
         fluxos = [torch.cuda.ExternalStream(s.stream()) for s in lote.sims]
         lig = _abi.carregar()
         saidas = []
@@ -474,7 +479,7 @@ def executar_lote(args, rank, mundo, dist):
                 piores.append(float(np.max(r[agua, 1] / r[agua, 0])) if agua.any() else 0.0)
         solves = [estatisticas_solve(s) for s in lote.sims]
         celulas = [at["cena"].nx * at["cena"].ny for at in lote.atlas]
-        res = dict(ms=ms, lancamentos=lanc, particulas=lote.n, etapas=etapas, celulas=celulas,
+        res = dict(ms=ms, lancamentos=lanc, particulas=lote.n, etapas=etapas, celulas=celulas, ctas=lote.ctas,
                    max_rel_tanque=max(piores) if piores else None, solves=solves,
                    atlas=[[at["cena"].nx, at["cena"].ny] for at in lote.atlas], relogios=rel.resumo() if rel else None,
                    d2h=d2h / max(args.steps, 1))
@@ -490,11 +495,13 @@ def executar_lote(args, rank, mundo, dist):
         return dict(gbs=b / t / 1e9 if t > 0 else 0.0, iters=iters, bytes=b, s=t)
 
     misto = medir(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED, com_relogio=True)
+    # the same configuration eagerly, for the solve's stage time (a graph records no events)
+    misto_etapas = medir(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED, grafo=False)
     plano = medir(_abi.TQ_PREC_FP32, _abi.TQ_ENGINE_PLAIN)
     e2e = medir(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED, e2e=True)
     tempos = tempos_max_ranks([misto["ms"], plano["ms"], e2e["ms"]], dist, "cuda")
     valor, valor_plano, valor_e2e = (len(todos) * args.steps * sub / (t / 1000) for t in tempos)
-    r_m, r_p = solve(misto, "fp16"), solve(plano, "fp32")
+    r_m, r_p = solve(misto_etapas, "fp16"), solve(plano, "fp32")
     if rank != 0:
         return None
     return {
@@ -520,14 +527,19 @@ def executar_lote(args, rank, mundo, dist):
                           "seconds_per_frame_by_limit": {str(k): round(v, 4) for k, v in ajuste.items()}},
             "atlas_cells_rank0": sum(misto["celulas"]), "particles_rank0": misto["particulas"], "tolerance": TOL,
             "mixed_precision": "fp16 V-cycle storage",
-            "mixed_engine": "fused, block preconditioner, each atlas's frame replayed from a CUDA graph",
+            "mixed_engine": "fused, block preconditioner, each atlas's frame replayed from a CUDA graph, the atlases "
+                            "side by side on shares of the SMs (fused_ctas)",
+            "fused_ctas_rank0": misto["ctas"],
             "l2": "flushed (256 MB write) between timed steps", "parallelism": f"tanks split over {mundo} GPU(s) by cells",
         },
         "fp32_plain": {"value": round(valor_plano, 1), "unit": "tank-substeps/s", "mgpcg_gbs": round(r_p["gbs"], 1),
+                       "ms_solve_per_substep_all_atlases": round(r_p["s"] * 1000 / max(args.steps * sub, 1), 3),
                        "pcg_iters_per_atlas_substep": round(r_p["iters"], 2),
                        "stop": "the atlas's true residual as a whole (the plain engine has no per-tank test)",
                        "solves_per_atlas": plano["solves"]},
         "mixed": {"mgpcg_gbs": round(r_m["gbs"], 1), "pcg_iters_per_atlas_substep": round(r_m["iters"], 2),
+                  "ms_solve_per_substep_all_atlases": round(r_m["s"] * 1000 / max(args.steps * sub, 1), 3),
+                  "eager_value": round(len(todos) * args.steps * sub / (misto_etapas["ms"] / 1000), 1),
                   "speedup_vs_fp32_plain": round(valor / valor_plano, 3),
                   "stop": "every tank's own true residual <= 1e-6 of its own r0 (tq_set_tanks)",
                   "max_tank_true_rel_residual_last_solve": misto["max_rel_tanque"],

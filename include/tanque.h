@@ -94,7 +94,10 @@ typedef struct tq_options {
   int32_t capacity;          /* particle capacity; 0: ceil(nx*ny*PARTICULAS_MAX_POR_CELULA) */
   int32_t device;            /* CUDA device ordinal */
   int32_t preconditioner;    /* TQ_PRECOND_*, default TQ_PRECOND_REFERENCE */
-  int32_t reserved[6];
+  int32_t fused_ctas;        /* FUSED engine: CTAs of the persistent solve (one per SM at
+                                most); 0 = one per SM.  Fewer let several handles' solves run
+                                side by side (tq_launch_graph) */
+  int32_t reserved[5];
 } tq_options;
 
 /* Fills defaults for an nx x ny tank of cell size h. */
@@ -203,6 +206,12 @@ int tq_substep(tq_sim* s, double dt);
  * substeps.  The PLAIN engine in tolerance mode reads its stop flag on the host and cannot be
  * captured: TQ_E_STATE.  No counterpart in the reference (it has no graph API). */
 int tq_advance_graph(tq_sim* s, double dt, int32_t substeps);
+/* tq_advance_graph without the wait at its end: the frame is queued on the handle's stream and
+ * the call returns (the air relabel before it still waits for the stream).  Handles on
+ * different streams then step side by side: with tq_options.fused_ctas splitting the SMs,
+ * their persistent solves run at the same time.  A solve that gave up on a bounded wait is
+ * reported by the next tq_sync. */
+int tq_launch_graph(tq_sim* s, double dt, int32_t substeps);
 
 /* SimulacaoCPU.atualizarAr() (js/fisica-cpu.js:162-167) — RastreadorDeAr.atualizar
  * (js/ar.js:56-153) on the device. */
@@ -281,7 +290,10 @@ enum tq_scalar {
   TQ_SCALAR_SOLVE_ITERS = 13,   /* their iterations in total */
   TQ_SCALAR_SOLVE_MAX_REL = 14, /* largest true ||b - A q|| / ||r0|| among them */
   TQ_SCALAR_SOLVE_REPLACEMENTS = 15, /* residual replacements among them (see tq_solve_pressure) */
-  TQ_SCALAR_COUNT_ = 16
+  TQ_SCALAR_CLOSED_REGIONS = 16, /* closed regions (water sealed from every air cell at pressure
+                                    0) whose right-hand side the last tolerance-mode solve
+                                    projected onto A's range (see tq_solve_pressure) */
+  TQ_SCALAR_COUNT_ = 17
 };
 int tq_get_scalar(tq_sim* s, int32_t which, double* out);
 int tq_set_scalar(tq_sim* s, int32_t which, double value);
@@ -290,7 +302,8 @@ int tq_set_scalar(tq_sim* s, int32_t which, double value);
  * (js/pressao-cpu.js:343, 386, 401). */
 int tq_last_norms(tq_sim* s, double* out, int32_t cap, int32_t* n);
 
-/* Waits for the handle's stream. */
+/* Waits for the handle's stream; reports a queued solve that gave up on a bounded wait
+ * (TQ_E_TIMEOUT). */
 int tq_sync(tq_sim* s);
 
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own device work
@@ -325,8 +338,8 @@ typedef struct tq_solve_info {
   int32_t iterations;    /* iterations run */
   int32_t converged;     /* tolerance mode: 1 when ||b - A q|| <= tolerance * ||r0||; else 0 */
   int32_t replacements;  /* residual replacements (tolerance mode) */
-  int32_t pad;
-  double residual0;      /* ||r0|| */
+  int32_t closed_regions; /* tolerance mode: closed regions whose right-hand side was projected */
+  double residual0;      /* ||r0|| (of the projected right-hand side in tolerance mode) */
   double residual;       /* the last recursive ||r|| */
   double true_residual;  /* ||b - A q|| in FP64 of the final iterate (tolerance mode), else -1 */
 } tq_solve_info;
@@ -342,6 +355,14 @@ typedef struct tq_solve_info {
  * the true residual replaces the recursive one and CG goes on with the same search direction
  * (residual replacement), which keeps the FP32 rounding of the recursive residual far below
  * the tolerance.
+ * Closed regions (tolerance mode): a 4-connected set of unknowns (water cells, joined to their
+ * water neighbours and to the active bubbles they face) that touches no air cell at pressure 0
+ * is water sealed by walls; A is singular on it (its null vector the constant over the
+ * region's water cells and bubble pressures) and b's component along that vector cannot be
+ * removed, so a solve stopping on the residual could never stop there.  Before the solve each
+ * closed region's right-hand side (-div on water, rhs on bubbles) loses its mean over the
+ * region's unknowns; open regions are untouched and the caller's div and rhs are not written.
+ * The reference, with its fixed count, solves the unprojected system as far as it gets.
  * q is returned rounded to FP32, so b - A q of the returned float q carries their rounding
  * (about 1e-7 of |A| |q| per cell) on top of the reported true residual.
  * norms receives the recursive residual history (initial, then one per iteration).

@@ -491,11 +491,112 @@ void vizinhosPorFaces(const Nivel<S>& f, Nivel<S>& g) {
 // then far below the tolerance by the end of the solve.
 constexpr double FATOR_TROCA = 1e-3;
 
-// What a solve reports beside q (tq_solve_info).
+// What a solve reports beside q (tq_solve_info), and the closed regions it projected.
 struct InfoPCG {
-  int iters = 0, convergiu = 0, trocas = 0;
+  int iters = 0, convergiu = 0, trocas = 0, regioes = 0;
   double r0 = 0, r = 0, rv = -1;
 };
+
+// Closed regions of a tolerance-mode solve (no counterpart in the reference; the library's
+// regioes.cu).  The unknowns are the water cells and one pressure per active bubble (a label
+// >= 2 with an interior air cell facing water, as montarBolhas finds them).  A 4-connected set
+// of them, water joined to water and to the active bubbles it faces, that touches no Dirichlet
+// cell (air outside an active bubble) is closed: A is singular on it, its null vector the
+// constant, and b's component along it cannot be removed by any q.  Each closed region's
+// right-hand side (-div on water, rhs on bubbles) loses its mean over the region's unknowns, in
+// double, rounded back to S.  Each projected region's root (its smallest water cell) is then
+// pinned: tipoSolve marks it air at pressure 0 for the solve (unless it carries a bubble
+// label), which makes the region's block nonsingular; with the projected right-hand side the
+// pinned row holds by itself.  Returns the number of closed regions (at most MAX_REGIOES are
+// projected, as on the device).
+constexpr int MAX_REGIOES = 4096;
+template <class S>
+int projetarFechadas(int nx, int ny, const uint8_t* tipo, const uint32_t* rot, S* div, S* rhs, uint8_t* tipoSolve) {
+  const int N = nx * ny;
+  std::vector<char> ativa(MAX_BOLHAS, 0);
+  if (rot)
+    for (int j = 1; j < ny - 1; j++)
+      for (int i = 1; i < nx - 1; i++) {
+        const int c = i + j * nx;
+        const uint32_t b = rot[c];
+        if (tipo[c] != AR || b < 2 || b >= (uint32_t)MAX_BOLHAS) continue;
+        if (tipo[c - 1] == AGUA || tipo[c + 1] == AGUA || tipo[c - nx] == AGUA || tipo[c + nx] == AGUA) ativa[b] = 1;
+      }
+  std::vector<int> pai(N + MAX_BOLHAS);
+  for (int c = 0; c < N + MAX_BOLHAS; c++) pai[c] = c;
+  auto raiz = [&](int a) {
+    while (pai[a] != a) {
+      pai[a] = pai[pai[a]];
+      a = pai[a];
+    }
+    return a;
+  };
+  auto unir = [&](int a, int b) {
+    a = raiz(a);
+    b = raiz(b);
+    if (a != b) pai[a > b ? a : b] = a < b ? a : b;  // the smallest index is the root
+  };
+  std::vector<char> toca(N, 0);
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      const int c = i + j * nx;
+      if (tipo[c] != AGUA) continue;
+      const int nb[4] = {c - 1, c + 1, c - nx, c + nx};
+      const bool dentro[4] = {i > 0, i < nx - 1, j > 0, j < ny - 1};
+      for (int q = 0; q < 4; q++) {
+        if (!dentro[q]) continue;
+        const uint8_t t = tipo[nb[q]];
+        if (t == AGUA) unir(c, nb[q]);
+        else if (t == AR) {
+          const uint32_t b = rot ? rot[nb[q]] : 0;
+          if (rot && b >= 2 && b < (uint32_t)MAX_BOLHAS && ativa[b]) unir(c, N + (int)b);
+          else toca[c] = 1;
+        }
+      }
+    }
+  std::vector<char> aberto(N, 0);
+  for (int c = 0; c < N; c++)
+    if (tipo[c] == AGUA && toca[c]) aberto[raiz(c)] = 1;
+  std::vector<int> id(N, -1);
+  int nReg = 0;
+  for (int c = 0; c < N; c++)
+    if (tipo[c] == AGUA && raiz(c) == c && !aberto[c]) {
+      if (nReg < MAX_REGIOES) id[c] = nReg;
+      nReg++;
+    }
+  std::vector<double> soma(MAX_REGIOES, 0.0);
+  std::vector<long> cont(MAX_REGIOES, 0);
+  for (int c = 0; c < N; c++) {
+    if (tipo[c] != AGUA) continue;
+    const int r = id[raiz(c)];
+    if (r < 0) continue;
+    soma[r] += -(double)div[c];
+    cont[r]++;
+  }
+  if (rot)
+    for (int b = 2; b < MAX_BOLHAS; b++) {
+      if (!ativa[b]) continue;
+      const int r = id[raiz(N + b)];
+      if (r < 0) continue;
+      soma[r] += (double)rhs[b];
+      cont[r]++;
+    }
+  for (int c = 0; c < N; c++) {
+    tipoSolve[c] = tipo[c];
+    if (tipo[c] != AGUA) continue;
+    const int r = id[raiz(c)];
+    if (r < 0) continue;
+    div[c] = (S)((double)div[c] + soma[r] / (double)cont[r]);
+    if (raiz(c) == c && (!rot || rot[c] < 2)) tipoSolve[c] = AR;
+  }
+  if (rot)
+    for (int b = 2; b < MAX_BOLHAS; b++) {
+      if (!ativa[b]) continue;
+      const int r = id[raiz(N + b)];
+      if (r >= 0) rhs[b] = (S)((double)rhs[b] - soma[r] / (double)cont[r]);
+    }
+  return nReg < MAX_REGIOES ? nReg : MAX_REGIOES;
+}
 
 // resolverPCG, js/pressao-cpu.js:296-402.  tol = 0 is the reference's fixed count.  tol > 0 (no
 // counterpart in the reference) keeps q in double during the solve and stops when the TRUE
@@ -515,6 +616,26 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
   Nivel<S>& n0 = L.n[0];
   int nx = n0.nx, ny = n0.ny;
   int k = nx * ny;
+  // tolerance mode: the solve reads copies of div and the bubble rhs in which every closed
+  // region's right-hand side has lost its mean (projetarFechadas)
+  std::vector<S> divP, rhsP;
+  std::vector<uint8_t> tipoP;
+  BolhasPCG<S> bP{};
+  int regioes = 0;
+  if (tol > 0) {
+    divP.assign(div, div + k);
+    tipoP.assign(k, 0);
+    if (bolhas) {
+      rhsP.assign(bolhas->rhs, bolhas->rhs + MAX_BOLHAS);
+      bP = *bolhas;
+      bP.rhs = rhsP.data();
+      bolhas = &bP;
+    }
+    regioes = projetarFechadas<S>(nx, ny, tipo, bolhas ? bolhas->rotulo : nullptr, divP.data(),
+                                  bolhas ? rhsP.data() : nullptr, tipoP.data());
+    div = divP.data();
+    tipo = tipoP.data();
+  }
   Nivel<S>& op = L.op;
   if (op.nx != nx || op.ny != ny) {
     op.nx = nx;
@@ -728,6 +849,7 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
   if (bolhas)
     for (uint32_t b : ativos) bolhas->y[b] = (S)yb.get(b);
   inf.r = normas.back();
+  inf.regioes = regioes;
   if (info) *info = inf;
   return normas;
 }
@@ -1940,6 +2062,7 @@ int tqo_get_scalar(tqo_sim* s, int32_t which, double* out) {
       case TQ_SCALAR_SOLVE_ITERS: *out = (double)S_.itersAcum; break;
       case TQ_SCALAR_SOLVE_MAX_REL: *out = S_.maxRel; break;
       case TQ_SCALAR_SOLVE_REPLACEMENTS: *out = (double)S_.trocasAcum; break;
+      case TQ_SCALAR_CLOSED_REGIONS: *out = S_.info.regioes; break;
       default: return fail(TQ_E_ARG, "unknown scalar");
     }
   });
@@ -1995,7 +2118,7 @@ int tqo_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float*
     info->iterations = inf.iters;
     info->converged = inf.convergiu;
     info->replacements = inf.trocas;
-    info->pad = 0;
+    info->closed_regions = inf.regioes;
     info->residual0 = inf.r0;
     info->residual = inf.r;
     info->true_residual = inf.rv;

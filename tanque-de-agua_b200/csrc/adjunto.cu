@@ -487,10 +487,15 @@ __global__ void k_adj_somar(const double* parc, int m, double* out) {
 
 // ---------------------------------------------------------------- CG kernels
 // The CG's scalars live on the device (esc): [0] ||b||^2, [1] alpha, [2] beta, [3] r.z, [4] the
-// latest dot, [5] a second dot, [6] the stop flag (as a double: 0 running, 1 stopped).  Every
-// update kernel returns at once after the flag is set, so the host reads it every few
-// iterations only and the result is that of stopping at the exact iteration.
-enum { E_B2 = 0, E_AL = 1, E_BE = 2, E_RZ = 3, E_D1 = 4, E_D2 = 5, E_PARA = 6 };
+// latest dot, [5] a second dot, [6] the stop flag (as a double: 0 running, else the iteration
+// count at the stop, at least 1), [8] the same flag as an int for the V-cycle's kernels.  Every
+// kernel of an iteration returns at once after the flag is set, so the host reads it only now
+// and then and the result is that of stopping at the exact iteration.
+enum { E_B2 = 0, E_AL = 1, E_BE = 2, E_RZ = 3, E_D1 = 4, E_D2 = 5, E_PARA = 6, E_PARA_INT = 8, E_N = 9 };
+__device__ inline void pararCG(double* esc, int iteracoes) {
+  esc[E_PARA] = iteracoes > 0 ? iteracoes : 1;
+  *reinterpret_cast<int*>(esc + E_PARA_INT) = 1;
+}
 
 // A v on water cells (js/pressao-cpu.js:84-93, true types; air is 0)
 __global__ void k_adj_aplicar(Dispositivo D, const uint8_t* tipo, const double* v, double* out, const double* esc) {
@@ -547,22 +552,24 @@ __global__ void k_adj_copiar_se(double* dst, const double* src, size_t n, const 
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
     dst[k] = src[k];
 }
-// the scalar steps of one CG iteration (one thread): modo 0 start (||b||^2 in E_D1 -> E_B2, the
-// flag cleared, rz from E_D2); 1 alpha = rz / p.Ap (E_D1); 2 the stop test on r.r (E_D1);
-// 3 Polak-Ribiere beta from r.z (E_D1) and r.zOld (E_D2)
-__global__ void k_adj_escalares(double* esc, int modo, double tol2) {
+// the scalar steps of one CG iteration (one thread; `it` the iteration, from 0): modo 0 start
+// (||b||^2 in E_D1 -> E_B2, the flag cleared unless b = 0); 1 alpha = rz / p.Ap (E_D1); 2 the
+// stop test on r.r (E_D1); 3 Polak-Ribiere beta from r.z (E_D1) and r.zOld (E_D2); 4 rz
+__global__ void k_adj_escalares(double* esc, int modo, double tol2, int it) {
   if (modo == 0) {
     esc[E_B2] = esc[E_D1];
-    esc[E_PARA] = esc[E_B2] == 0 ? 1.0 : 0.0;
+    esc[E_PARA] = 0.0;
+    *reinterpret_cast<int*>(esc + E_PARA_INT) = 0;
+    if (esc[E_B2] == 0) pararCG(esc, 0);
     return;
   }
   if (esc[E_PARA] != 0) return;
   if (modo == 1) {
     const double pap = esc[E_D1];
-    if (pap == 0) esc[E_PARA] = 1.0;
+    if (pap == 0) pararCG(esc, it);
     else esc[E_AL] = esc[E_RZ] / pap;
   } else if (modo == 2) {
-    if (esc[E_D1] <= tol2 * esc[E_B2]) esc[E_PARA] = 1.0;
+    if (esc[E_D1] <= tol2 * esc[E_B2]) pararCG(esc, it + 1);
   } else if (modo == 3) {
     const double rzn = esc[E_D1], cruz = esc[E_D2];
     esc[E_BE] = fmax(0.0, (rzn - cruz) / esc[E_RZ]);
@@ -859,7 +866,8 @@ struct tq_adj {
   double *bufB, *bufBin;  // 8 x cap
   double *ugb, *vgb, *ugb2, *vgb2, *qb, *lam, *Ub, *UWb, *Vb, *VWb;
   // CG
-  double *r, *z, *zv, *p, *ap, *parc, *esc;  // esc: the CG's scalars (E_*) and a host-read slot
+  double *r, *z, *zv, *p, *ap, *parc, *esc;  // esc: the CG's scalars (E_*) and a host-read slot (7)
+  int itFrente = 0, itTras = 0;                // the last forward / adjoint solve's iteration count
   float *bf, *xf;
   double gth[2] = {0, 0};
 };
@@ -906,22 +914,29 @@ void somaDisp(tq_adj* a, const double* x, const double* y, int n, double* destin
 }
 
 // A x = b on the water cells of `tipo` (device): CG in FP64 preconditioned by the FP32 V-cycle,
-// Polak-Ribiere beta, to ||r|| <= 1e-12 ||b||.  The scalars stay on the device; the host reads
-// the stop flag every VERIFICAR iterations.  Returns TQ_OK or an error.
+// Polak-Ribiere beta, to ||r|| <= 1e-12 ||b||.  The scalars stay on the device.  The host reads
+// the stop flag every VERIFICAR iterations, and at every iteration from two before the count
+// the previous solve of the same kind took (*estimativa, updated here): the solves of a run
+// take similar counts, so few iterations run past the stop (each of those returns at once in
+// every kernel but still costs its launches).  Returns TQ_OK or an error.
 constexpr int VERIFICAR = 8;
-int resolver(tq_adj* a, const uint8_t* tipo, const double* bdev, double* x) {
+int resolver(tq_adj* a, const uint8_t* tipo, const double* bdev, double* x, int* estimativa) {
   const int N = a->N;
   const int g = gridDe(N);
   cudaStream_t st = a->s;
   double* esc = a->esc;
+  const int* pararInt = reinterpret_cast<const int*>(esc + E_PARA_INT);
+  int it = 0;
   auto escalares = [&](int modo) {
     contarLancamento();
-    k_adj_escalares<<<1, 1, 0, st>>>(esc, modo, TOL_SOLVE * TOL_SOLVE);
+    k_adj_escalares<<<1, 1, 0, st>>>(esc, modo, TOL_SOLVE * TOL_SOLVE, it);
   };
+  bool preparar = true;  // the levels' types and masks: once per solve
   auto precond = [&](int qual) {  // z = M r (the V-cycle on r scaled to unit norm; ||r||^2 in esc[qual])
     contarLancamento();
     k_adj_para_float<<<g, TB, 0, st>>>(N, tipo, a->r, esc, qual, a->bf);
-    int e = cicloVDispositivo(a->pcg, tipo, a->bf, a->xf, st);
+    int e = cicloVDispositivo(a->pcg, tipo, a->bf, a->xf, st, preparar, pararInt);
+    preparar = false;
     contarLancamento();
     k_adj_de_float<<<g, TB, 0, st>>>(N, tipo, a->xf, esc, qual, a->z);
     return e;
@@ -935,7 +950,7 @@ int resolver(tq_adj* a, const uint8_t* tipo, const double* bdev, double* x) {
   k_adj_copiar_se<<<g, TB, 0, st>>>(a->p, a->z, N, esc);
   somaDisp(a, a->r, a->z, N, esc + E_D1);
   escalares(4);  // rz
-  for (int it = 0; it < 2000; it++) {
+  for (; it < 2000; it++) {
     contarLancamento();
     k_adj_aplicar<<<g, TB, 0, st>>>(a->D, tipo, a->p, a->ap, esc);
     somaDisp(a, a->p, a->ap, N, esc + E_D1);
@@ -952,12 +967,15 @@ int resolver(tq_adj* a, const uint8_t* tipo, const double* bdev, double* x) {
     escalares(3);  // beta
     contarLancamento();
     k_adj_direcao<<<g, TB, 0, st>>>(N, tipo, esc, a->z, a->p);
-    if (it % VERIFICAR == VERIFICAR - 1) {
+    if (it % VERIFICAR == VERIFICAR - 1 || it + 1 >= *estimativa - 2) {
       double para = 0;
       if (cudaMemcpyAsync(&para, esc + E_PARA, sizeof para, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
           cudaStreamSynchronize(st) != cudaSuccess)
         return TQ_E_CUDA;
-      if (para != 0) return TQ_OK;
+      if (para != 0) {
+        *estimativa = (int)para;
+        return TQ_OK;
+      }
     }
   }
   std::snprintf(g_erroAdj, sizeof g_erroAdj, "adjoint pressure solve did not reach 1e-12 in 2000 iterations");
@@ -1000,7 +1018,7 @@ int passoFrente(tq_adj* a, int s, int n, Fita* f) {
   k_adj_faces<<<gridDe(nf), TB, 0, st>>>(D, U, UW, V, VW, a->u, a->v);
   contarLancamento();
   k_adj_div<<<gridDe(N), TB, 0, st>>>(D, tipo, a->u, a->v, a->b);
-  int r = resolver(a, tipo, a->b, a->q);
+  int r = resolver(a, tipo, a->b, a->q, &a->itFrente);
   if (r) return r;
   uint8_t* val = f ? f->val : a->valT;  // (CAMADAS_EXT + 1) x (nu + nv)
   contarLancamento();
@@ -1096,7 +1114,7 @@ int tq_adj_create(const tq_adj_scene* d, int32_t device, tq_adj** out) {
        alocar(a, &a->ugb2, nu) && alocar(a, &a->vgb2, nv) && alocar(a, &a->qb, N) && alocar(a, &a->lam, N) &&
        alocar(a, &a->Ub, nu) && alocar(a, &a->UWb, nu) && alocar(a, &a->Vb, nv) && alocar(a, &a->VWb, nv) &&
        alocar(a, &a->r, N) && alocar(a, &a->z, N) && alocar(a, &a->zv, N) && alocar(a, &a->p, N) &&
-       alocar(a, &a->ap, N) && alocar(a, &a->parc, SOMA_CTAS) && alocar(a, &a->esc, 8) && alocar(a, &a->bf, N) &&
+       alocar(a, &a->ap, N) && alocar(a, &a->parc, SOMA_CTAS) && alocar(a, &a->esc, E_N) && alocar(a, &a->bf, N) &&
        alocar(a, &a->xf, N);
   if (ok) a->pcg = criarPcg(d->nx, d->ny, TQ_PREC_FP32, TQ_ENGINE_PLAIN);
   if (!ok || !a->pcg) {
@@ -1277,7 +1295,7 @@ int tq_adj_backward(tq_adj* a, double grad_loss, float* dv0, double* dtheta) {
       // gradient reverse (gather per cell), the adjoint solve, divergence / walls / normalisation
       contarLancamento();
       k_adj_grad_T<<<gridDe(N), TB, 0, st>>>(a->D, f.tipo, a->ugb, a->vgb, a->qb);
-      int r = resolver(a, f.tipo, a->qb, a->lam);
+      int r = resolver(a, f.tipo, a->qb, a->lam, &a->itTras);
       if (r) return r;
       const int nfc = nu > nv ? nu : nv;
       contarLancamento();

@@ -15,11 +15,11 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "uniao.cuh"
 
 namespace tq {
 
 constexpr unsigned long long VAZIO = ~0ull;
-constexpr int LIMITE_UNIAO = 1 << 22;  // bound on the lock-free retry loops
 
 struct Rastreador {
   int nx, ny, N;
@@ -52,28 +52,7 @@ struct Rastreador {
   int nBlocos;
 };
 
-// ---------------------------------------------------------------- union-find
-__device__ inline int raiz(int* pai, int a) {
-  for (int g = 0; g < LIMITE_UNIAO; g++) {
-    int p = pai[a];
-    if (p == a) return a;
-    int gp = pai[p];
-    if (gp != p) pai[a] = gp;  // path halving: gp is an ancestor of a
-    a = p;
-  }
-  return a;
-}
-__device__ inline bool unir(int* pai, int a, int b) {
-  for (int g = 0; g < LIMITE_UNIAO; g++) {
-    a = raiz(pai, a);
-    b = raiz(pai, b);
-    if (a == b) return true;
-    if (a < b) { int t = a; a = b; b = t; }
-    if (atomicCAS(&pai[a], a, b) == a) return true;  // larger root under the smaller
-  }
-  return false;
-}
-
+// ---------------------------------------------------------------- union-find (uniao.cuh)
 __global__ void k_ar_iniciar(Rastreador r, const uint8_t* tipo) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= r.N) return;
@@ -98,13 +77,7 @@ __global__ void k_ar_unir(Rastreador r, const uint8_t* tipo) {
 __global__ void k_ar_achatar(Rastreador r) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= r.N || r.pai[c] < 0) return;
-  int a = c;
-  for (int g = 0; g < LIMITE_UNIAO; g++) {
-    int p = r.pai[a];
-    if (p == a) break;
-    a = p;
-  }
-  r.pai[c] = a;
+  r.pai[c] = raizLeitura(r.pai, c);
 }
 
 // Per-cell statistics of js/ar.js:75-95, gathered at the component's root: cells, touches the

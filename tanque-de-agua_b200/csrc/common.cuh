@@ -67,7 +67,7 @@ struct Escalares {
   double proxTroca;           // plain engine: the recursive norm that triggers the next replacement
   int aceitas;                // particles accepted by the last add
   int pendentes;              // label-propagation work list length
-  int pad;
+  int regioes;                // closed regions the last tolerance-mode solve projected (pcg.cu)
   unsigned int tickets[16];   // last-block-done counters of the reductions
   // convergence of the solves (tolerance mode), written on the device at the end of each solve
   double normaVerd;           // true ||b - A q|| of the last solve's iterate (-1: fixed count)

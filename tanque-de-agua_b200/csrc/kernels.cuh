@@ -33,15 +33,28 @@ void lancarPosPressao(const Dev& d, double dt, bool ar, cudaStream_t s);
 void lancarGradiente(const Dev& d, cudaStream_t s);
 void lancarExtrapolar(const Dev& d, cudaStream_t s);
 
+// regioes.cu — the closed regions of a solve (water sealed from every Dirichlet cell): their
+// right-hand side projected onto A's range and one cell of each pinned at 0 (tolerance mode).
+struct Regioes;
+Regioes* criarRegioes(int N);
+void destruirRegioes(Regioes* R);
+// Queues the labelling and projection; *out = d with div / rhsBolhaF / tipo at the solve's copies.
+void projetarFechadas(Regioes* R, const Dev& d, bool bolhas, cudaStream_t s, Dev* out);
+int erroRegioes(Regioes* R, cudaStream_t s);
+
 // pcg.cu — the pressure solve on the handle's grid.
 struct Pcg;
-Pcg* criarPcg(int nx, int ny, int precisao, int motor);
+// ctasFundido: the fused engine's CTA count (0: one per SM).
+Pcg* criarPcg(int nx, int ny, int precisao, int motor, int ctasFundido = 0);
 void destruirPcg(Pcg* p);
 // Solves for d.q on the cells d.tipo marks as water; bubbles from d.rotulo / d.rhsB / d.yB when
 // `bolhas`; precond is TQ_PRECOND_*.  The FUSED engine queues the solve without waiting; the
 // PLAIN engine reads its stop flag every few iterations in tolerance mode.  The iteration count,
 // residual history and convergence record stay in d.esc.  Returns TQ_OK or an error status.
+// In tolerance mode the right-hand side of each closed region first loses its mean (regioes.cu).
 int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, int precond, cudaStream_t s);
+// Allocates what a tolerance-mode solve allocates on first use (before a stream capture).
+int reservarTolerancia(Pcg* p);
 // The last solve's residual history from the device (waits for the stream); its length, or -1.
 int normasPcg(Pcg* p, const Dev& d, double* out, int cap, cudaStream_t s);
 // TQ_E_TIMEOUT if a fused solve since the last call gave up on a bounded wait (waits for the stream).
@@ -51,8 +64,10 @@ int motorPcg(Pcg* p);
 // Phase trace of the fused engine (%globaltimer at each grid barrier of the last solve).
 void perfilPcg(Pcg* p, bool ligar);
 int lerPerfilPcg(Pcg* p, unsigned long long* out, int cap);
-// One V-cycle from device buffers (level-0 types, right-hand side, result).
-int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cudaStream_t s);
+// One V-cycle on device buffers (tq_vcycle).  A solver running many on the same types prepares
+// the levels once (preparar on its first call only) and may pass a device stop flag.
+int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cudaStream_t s, bool preparar = true,
+                      const int* parar = nullptr);
 // One V-cycle with the level hierarchy in a static device array (tq_vcycle_noalloc): its
 // capacity, the bytes a grid needs, the array's address on the current device (looked up once
 // per device) and the cycle itself.

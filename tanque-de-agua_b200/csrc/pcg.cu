@@ -678,8 +678,9 @@ __global__ void __launch_bounds__(DOT_T) k_produto(Dev d, int modo, const float*
 // ---------------------------------------------------------------- the solver object
 
 
-Pcg* criarPcg(int nx, int ny, int precisao, int motor) {
+Pcg* criarPcg(int nx, int ny, int precisao, int motor, int ctasFundido) {
   Pcg* p = new Pcg();
+  p->ctasFundido = ctasFundido;
   p->nx = nx;
   p->ny = ny;
   p->N = nx * ny;
@@ -748,6 +749,7 @@ void destruirPcg(Pcg* p) {
   }
   cudaFree(p->vizOp);
   if (p->q64) cudaFree(p->q64);
+  destruirRegioes(p->regioes);
   delete p;
 }
 
@@ -870,16 +872,25 @@ static void produto(Pcg* p, const Dev& d, int modo, const float* a, const float*
 // exact iteration, with one host round trip per LOTE_VERIFICACAO iterations instead of one each.
 constexpr int LOTE_VERIFICACAO = 8;
 
-int resolverPressao(Pcg* p, const Dev& d, int iteracoes, double tol, bool bolhas, int precond, cudaStream_t s) {
+int reservarTolerancia(Pcg* p) {
+  if (!p->regioes && !(p->regioes = criarRegioes(p->N))) return TQ_E_NOMEM;
+  if (p->motor != TQ_ENGINE_FUSED && !p->q64 && cudaMalloc(&p->q64, (size_t)p->N * sizeof(double)) != cudaSuccess)
+    return TQ_E_NOMEM;
+  return TQ_OK;
+}
+
+int resolverPressao(Pcg* p, const Dev& d0, int iteracoes, double tol, bool bolhas, int precond, cudaStream_t s) {
+  Dev d = d0;
+  double* q64 = nullptr;
+  if (tol > 0) {
+    if (reservarTolerancia(p)) return TQ_E_NOMEM;
+    projetarFechadas(p->regioes, d0, bolhas, s, &d);  // d reads the projected right-hand sides
+    q64 = p->q64;
+  }
   if (p->motor == TQ_ENGINE_FUSED) return resolverPressaoFundido(p, d, iteracoes, tol, bolhas, precond, s);
   const bool bloco = precond == TQ_PRECOND_BLOCK;
   const int nb = blocos(d.N, 256);
   const int nbx = blocos(d.N > MAX_BOLHAS ? d.N : MAX_BOLHAS, 256);
-  double* q64 = nullptr;
-  if (tol > 0) {
-    if (!p->q64 && cudaMalloc(&p->q64, (size_t)d.N * sizeof(double)) != cudaSuccess) return TQ_E_NOMEM;
-    q64 = p->q64;
-  }
   // operator (true types) and preconditioner types
   lanca(k_viz, nb, 256, 0, s, d.tipo, d.nx, d.ny, p->vizOp);
   lanca(k_mg_tipo0, nb, 256, 0, s, d.tipo, d.rotulo, p->tipoL[0], d.N, bolhas ? 1 : 0, bloco ? 1 : 0);
@@ -954,7 +965,10 @@ int normasPcg(Pcg* p, const Dev& d, double* out, int cap, cudaStream_t s) {
     return -1;
   return n;
 }
-int erroPcg(Pcg* p, cudaStream_t s) { return erroFundido(p->fundido, s); }
+int erroPcg(Pcg* p, cudaStream_t s) {
+  const int e = erroFundido(p->fundido, s);
+  return e ? e : erroRegioes(p->regioes, s);
+}
 int motorPcg(Pcg* p) { return p->motor; }
 void perfilPcg(Pcg* p, bool ligar) { perfilFundido(p->fundido, ligar); }
 int lerPerfilPcg(Pcg* p, unsigned long long* out, int cap) { return lerPerfilFundido(p->fundido, out, cap); }
@@ -973,8 +987,10 @@ __global__ void k_descarregar_x(NivelDev<T> n0, float* x) {
   if (c >= n0.nx * n0.ny) return;
   x[c] = carregar(n0.x[c]);
 }
-int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cudaStream_t s) {
-  prepararNiveis(p, tipo, false, s);
+int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cudaStream_t s, bool preparar,
+                      const int* parar) {
+  if (preparar) prepararNiveis(p, tipo, false, s);
+  p->parar = parar;  // the cycle's kernels return at once while *parar != 0
   int nb = blocos(p->N, 256);
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
@@ -985,6 +1001,7 @@ int cicloVDispositivo(Pcg* p, const uint8_t* tipo, const float* b, float* x, cud
     using T = std::remove_pointer_t<decltype(tag)>;
     lanca(k_descarregar_x<T>, nb, 256, 0, s, nivel<T>(p, 0), x);
   });
+  p->parar = nullptr;
   return cudaGetLastError() == cudaSuccess ? TQ_OK : TQ_E_CUDA;
 }
 

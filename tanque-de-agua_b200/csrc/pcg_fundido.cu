@@ -58,6 +58,9 @@ constexpr int NPARC = 4;                           // partial slots per CTA
 // recursive one has fallen by this factor since the last replacement: the rounding it gathers,
 // about 1e-7 of the residual it started from per iteration, then stays far below the tolerance.
 constexpr double FATOR_TROCA = 1e-3;
+// With tanks (tq_set_tanks) the whole grid's recursive residual below the tolerance only starts
+// the per-tank checks of the true residual: one every VERIF_TANQUES iterations, not every one.
+constexpr int VERIF_TANQUES = 4;
 constexpr int PERFIL_MAX = 1 << 16;                // phase-trace capacity
 constexpr int PERFIL_SECAO = 1 << 14;              // coarse-section stamps (after the phase trace)
 // per-warp shared-memory areas (floats)
@@ -1549,9 +1552,10 @@ __device__ __noinline__ void somarPorTanque(const Args& a, const float* v, doubl
 // sums (d.rvT) plus the squared true rows of the tank's bubbles, against tol^2 ||r0_t||^2.  Thread
 // t takes tanks t, t + TF, ..., adding its bubbles in the active list's order, so every CTA
 // reaches the same answer from the same global values (the barrier before made them visible).
-// CTA 0 leaves the totals in d.rvT for tq_get_tank_residuals.
+// Nothing is written here: every CTA reads d.rvT in this phase.  With `gravar` (CTA 0 alone,
+// after the solve's last barrier) the totals go to d.rvT for tq_get_tank_residuals.
 template <class FB>
-__device__ bool tanquesConvergiram(const Args& a, int nAt, FB rbVerd) {
+__device__ bool tanquesConvergiram(const Args& a, int nAt, FB rbVerd, bool gravar = false) {
   const Dev& d = a.d;
   bool ok = true;
   for (int t = threadIdx.x; t < d.nTanques; t += TF) {
@@ -1564,7 +1568,7 @@ __device__ bool tanquesConvergiram(const Args& a, int nAt, FB rbVerd) {
     }
     const double r0 = __ldcg(d.r0T + t);
     ok = ok && s <= a.tol * a.tol * r0;
-    if (blockIdx.x == 0) d.rvT[t] = s;
+    if (gravar) d.rvT[t] = s;
   }
   return __syncthreads_and(ok) != 0;
 }
@@ -1911,6 +1915,10 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
   bool convergiu = false;
   double normaVerd = -1.0;
   double proxTroca = norma0 * FATOR_TROCA;  // the next residual replacement's threshold
+  int proxVerif = 0;                          // with tanks: the next iteration that may check
+  auto rbVerd = [&](int b) {  // a bubble's true row, from faseVerdade's sums
+    return (double)d.rhsBolhaF[b] - (__ldcg(&d.facesB[b]) * __ldcg(&d.yB[b]) - (double)__ldcg(&a.accV[b]) / ESC);
+  };
 
   for (int it = 0; it < a.iteracoes; it++) {
     float* zc = cz ? a.z2 : d.z;
@@ -2000,20 +2008,20 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     somasGlobais(a, 0, [](int) { return 0.0; }, [](int) { return 0.0; }, sh, somas);
     double norma = sqrt(somas[0]);
     itersFeitas = it + 1;
-    bool fim = it == a.iteracoes - 1 || (a.tol > 0 && norma <= a.tol * norma0);
+    const bool ultima = it == a.iteracoes - 1;
+    bool fim = ultima || (a.tol > 0 && norma <= a.tol * norma0);
+    if (fim && !ultima && d.nTanques && it < proxVerif && norma > proxTroca) fim = false;
     if (a.q64 && (fim || norma <= proxTroca)) {
       // tolerance mode: the true residual of the FP64 iterate decides, and replaces the
       // recursive one unless the solve ends here
+      proxVerif = it + VERIF_TANQUES;
       faseVerdade(a, sh);
       if (!barreira(a, ep)) return;
-      auto rbVerd = [&](int b) {
-        return (double)d.rhsBolhaF[b] - (__ldcg(&d.facesB[b]) * __ldcg(&d.yB[b]) - (double)__ldcg(&a.accV[b]) / ESC);
-      };
       somasGlobais(a, nAt, [&](int b) { const double v = rbVerd(b); return v * v; }, [](int) { return 0.0; }, sh, somas);
       normaVerd = sqrt(somas[0] + somas[2]);
       // with tanks, each tank's own residual decides; without, the whole grid's
       convergiu = d.nTanques ? tanquesConvergiram(a, nAt, rbVerd) : normaVerd <= a.tol * norma0;
-      fim = convergiu || it == a.iteracoes - 1;
+      fim = convergiu || ultima;
       if (!fim) {
         // replacement: r (water) was rewritten by faseVerdade, the bubble rows follow; the
         // iteration goes on with the same search direction
@@ -2062,6 +2070,7 @@ __global__ void __launch_bounds__(TF, 1) k_mgpcg(const __grid_constant__ Args a)
     e->trocasAcum += trocas;
     if (a.q64 && norma0 > 0 && normaVerd / norma0 > e->maxRel) e->maxRel = normaVerd / norma0;
   }
+  if (blockIdx.x == 0 && d.nTanques && a.q64) tanquesConvergiram(a, nAt, rbVerd, true);  // each tank's total
   if (blockIdx.x == 0)
     for (int k = threadIdx.x; k < nAt; k += TF) {
       int b = __ldcg(&a.ativos[k]);
@@ -2116,7 +2125,8 @@ Fundido* criarFundido(Pcg* p) {
             cudaFuncSetAttribute(f->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemMax) == cudaSuccess &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&porSM, f->kern, TF, f->smem) == cudaSuccess && porSM >= 1;
   if (ok) {
-    f->G = sms;  // one CTA per SM: co-resident, as the grid barrier needs
+    // one CTA per SM (co-resident, as the grid barrier needs), or the requested fewer
+    f->G = p->ctasFundido > 0 && p->ctasFundido < sms ? p->ctasFundido : sms;
     const size_t N = p->N;
     const size_t nLc = (size_t)p->nxL[Lc] * p->nyL[Lc];
     ok = cudaMalloc(&f->niveis, MAX_NIVEIS * sizeof(NivelF)) == cudaSuccess &&

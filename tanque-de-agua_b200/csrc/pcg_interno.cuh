@@ -15,6 +15,7 @@ struct Fundido;
 
 struct Pcg {
   int nx, ny, N, precisao, motor;
+  int ctasFundido = 0;  // the fused engine's CTA count (0: one per SM)
   int L;
   int nxL[MAX_NIVEIS], nyL[MAX_NIVEIS];
   bool meia[MAX_NIVEIS];  // level stored in half precision
@@ -26,6 +27,7 @@ struct Pcg {
   const int* parar = nullptr;  // the running plain solve's stop flag (NivelDev::parar)
   size_t smemGrosso = 0;
   Fundido* fundido = nullptr;
+  Regioes* regioes = nullptr;  // tolerance mode's closed-region projection, allocated on first use
 };
 
 // pcg_fundido.cu

@@ -292,6 +292,7 @@ int tq_create(const tq_options* o, tq_sim** out) {
   if (o->engine != TQ_ENGINE_PLAIN && o->engine != TQ_ENGINE_FUSED) return falha(TQ_E_ARG, "bad engine");
   if (o->preconditioner != TQ_PRECOND_REFERENCE && o->preconditioner != TQ_PRECOND_BLOCK)
     return falha(TQ_E_ARG, "bad preconditioner");
+  if (o->fused_ctas < 0) return falha(TQ_E_ARG, "fused_ctas must be >= 0");
   int st = iniciarCuda(o->device);
   if (st) return st;
   tq_sim* s = new (std::nothrow) tq_sim();
@@ -344,7 +345,7 @@ int tq_create(const tq_options* o, tq_sim** out) {
        aloca(s, &d.ap, N) && aloca(s, &d.parciais, 4096) && aloca(s, &d.esc, 1);
   int nbMax = blocos(cap > (int)N ? cap : (int)N, 1024) + 1;
   ok = ok && aloca(s, &s->cont, nbMax) && aloca(s, &s->offs, nbMax) && aloca(s, &s->estado, 4);
-  if (ok) s->pcg = criarPcg(s->nx, s->ny, o->precision, o->engine);
+  if (ok) s->pcg = criarPcg(s->nx, s->ny, o->precision, o->engine, o->fused_ctas);
   if (ok && s->pcg) s->ar = criarRastreador(s->nx, s->ny);
   if (!ok || !s->pcg || !s->ar) {
     tq_destroy(s);
@@ -604,7 +605,24 @@ int tq_advance(tq_sim* s, double dt, int32_t sub) {
   return fimDePasso(s);
 }
 
+// tq_advance_graph without the final wait: the frame is queued on the handle's stream and its
+// solve errors are reported by tq_sync.
+static int lancarGrafo(tq_sim* s, double dt, int32_t sub);
+
 int tq_advance_graph(tq_sim* s, double dt, int32_t sub) {
+  int r = lancarGrafo(s, dt, sub);
+  return r ? r : fimDePasso(s);
+}
+
+int tq_launch_graph(tq_sim* s, double dt, int32_t sub) {
+  int r = lancarGrafo(s, dt, sub);
+  if (r) return r;
+  compactar(s);
+  CK(cudaGetLastError());
+  return TQ_OK;
+}
+
+static int lancarGrafo(tq_sim* s, double dt, int32_t sub) {
   if (!s) return falha(TQ_E_ARG, "null handle");
   if (!(dt > 0) || sub < 1) return falha(TQ_E_ARG, "need dt > 0 and substeps >= 1");
   if (motorPcg(s->pcg) == TQ_ENGINE_PLAIN && s->o.tolerance > 0)
@@ -621,6 +639,10 @@ int tq_advance_graph(tq_sim* s, double dt, int32_t sub) {
     s->grafoExec = nullptr;
     s->grafo = nullptr;
     s->timing = false;  // stage events are not recorded into the graph
+    if (s->o.tolerance > 0 && reservarTolerancia(s->pcg)) {  // no allocation inside the capture
+      s->timing = timing;
+      return falha(TQ_E_NOMEM, "tolerance-mode buffers");
+    }
     CK(cudaStreamBeginCapture(s->s, cudaStreamCaptureModeThreadLocal));
     int r = TQ_OK;
     for (int k = 0; k < sub && !r; k++) r = subpasso(s, dt / sub);
@@ -647,7 +669,7 @@ int tq_advance_graph(tq_sim* s, double dt, int32_t sub) {
   }
   contarLancamento();
   CK(cudaGraphLaunch(s->grafoExec, s->s));
-  return fimDePasso(s);
+  return TQ_OK;
 }
 
 int tq_count(tq_sim* s, int32_t* n) {
@@ -818,6 +840,13 @@ int tq_get_scalar(tq_sim* s, int32_t w, double* out) {
       return TQ_OK;
     }
     case TQ_SCALAR_PCG_TRUE_RES: return baixar(s, out, &s->d.esc->normaVerd, sizeof(double));
+    case TQ_SCALAR_CLOSED_REGIONS: {
+      int v = 0;
+      int st = baixar(s, &v, &s->d.esc->regioes, sizeof v);
+      if (st) return st;
+      *out = v;
+      return TQ_OK;
+    }
     case TQ_SCALAR_PCG_CONVERGED:
     case TQ_SCALAR_SOLVES:
     case TQ_SCALAR_SOLVES_CAPPED:
@@ -889,6 +918,9 @@ int tq_last_norms(tq_sim* s, double* out, int32_t cap, int32_t* n) {
 int tq_sync(tq_sim* s) {
   if (!s) return falha(TQ_E_ARG, "null handle");
   CK(cudaStreamSynchronize(s->s));
+  int r = erroPcg(s->pcg, s->s);  // a solve queued by tq_launch_graph that gave up
+  if (r == TQ_E_TIMEOUT) return falha(r, "pressure solve: a bounded wait gave up");
+  if (r) return falhaCuda(cudaGetLastError(), "pressure solve");
   return TQ_OK;
 }
 
@@ -1013,7 +1045,7 @@ int tq_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float* 
     info->iterations = e.iters;
     info->converged = e.convergiu;
     info->replacements = e.trocas;
-    info->pad = 0;
+    info->closed_regions = tolerance > 0 ? e.regioes : 0;
     info->residual0 = e.norma0;
     info->residual = e.norma;
     info->true_residual = e.normaVerd;

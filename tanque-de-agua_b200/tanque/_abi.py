@@ -42,6 +42,7 @@ TQ_SCALAR_GRAVITY_X, TQ_SCALAR_GRAVITY_Y = 7, 8
 TQ_SCALAR_PCG_TRUE_RES, TQ_SCALAR_PCG_CONVERGED = 9, 10
 TQ_SCALAR_SOLVES, TQ_SCALAR_SOLVES_CAPPED, TQ_SCALAR_SOLVE_ITERS = 11, 12, 13
 TQ_SCALAR_SOLVE_MAX_REL, TQ_SCALAR_SOLVE_REPLACEMENTS = 14, 15
+TQ_SCALAR_CLOSED_REGIONS = 16
 
 
 class TqOptions(C.Structure):
@@ -50,7 +51,8 @@ class TqOptions(C.Structure):
         ("iterations", C.c_int32), ("air", C.c_int32), ("tau_density", C.c_double),
         ("surface_tension", C.c_double), ("tolerance", C.c_double), ("precision", C.c_int32),
         ("engine", C.c_int32), ("p2g_mode", C.c_int32), ("capacity", C.c_int32),
-        ("device", C.c_int32), ("preconditioner", C.c_int32), ("reserved", C.c_int32 * 6),
+        ("device", C.c_int32), ("preconditioner", C.c_int32), ("fused_ctas", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -83,7 +85,8 @@ class TqAdjScene(C.Structure):
 
 class TqSolveInfo(C.Structure):
     _fields_ = [
-        ("iterations", C.c_int32), ("converged", C.c_int32), ("replacements", C.c_int32), ("pad", C.c_int32),
+        ("iterations", C.c_int32), ("converged", C.c_int32), ("replacements", C.c_int32),
+        ("closed_regions", C.c_int32),
         ("residual0", C.c_double), ("residual", C.c_double), ("true_residual", C.c_double),
     ]
 
@@ -127,6 +130,7 @@ ASSINATURAS = {
 }
 SO_PRODUTO = {
     "advance_graph": (C.c_int, [_P, _D, _I]),
+    "launch_graph": (C.c_int, [_P, _D, _I]),
     "emit_faucet": (C.c_int, [_P, C.POINTER(TqFaucet), C.POINTER(_I)]),
     "set_tanks": (C.c_int, [_P, _I, _P]),
     "get_tank_residuals": (C.c_int, [_P, C.POINTER(_D), _I, C.POINTER(_I)]),

@@ -146,21 +146,53 @@ def recortar(Cena, cena_atlas, x0: int, x1: int):
     return c
 
 
+def repartir_ctas(pesos: list[float], total: int, minimo: int = 4) -> list[int] | None:
+    """The SMs of one GPU split between atlases whose persistent solves run side by side: each
+    atlas gets CTAs in proportion to its weight (its cells), at least `minimo` (or
+    total // atlases when smaller), and the counts add up to at most `total` (one CTA per SM, so
+    every solve stays co-resident).  None when there are more atlases than SMs."""
+    n = len(pesos)
+    if n == 0:
+        return []
+    if n > total:
+        return None
+    minimo = max(1, min(minimo, total // n))
+    W = float(sum(pesos)) or 1.0
+    c = [max(minimo, int(total * p / W)) for p in pesos]
+    while sum(c) > total:  # take from the largest share above the minimum
+        k = max(range(n), key=lambda i: (c[i], -i))
+        if c[k] <= minimo:
+            break
+        c[k] -= 1
+    return c
+
+
 class Lote:
     """A batch of tanks as atlases, each advanced by one simulation made by `fabrica(cena,
-    opcoes)` (SimulacaoGPU, or the oracle's class in tests)."""
+    opcoes)` (SimulacaoGPU, or the oracle's class in tests).
+
+    `sms`: the GPU's SM count, to run the atlases' frames side by side: each atlas's fused
+    solve gets a share of the SMs (tq_options.fused_ctas, repartir_ctas by cells) and
+    avancar(grafo=True) queues every atlas's frame (tq_launch_graph) before waiting for any."""
 
     def __init__(self, fabrica, Cena, tanques: list[dict], h: float, opcoes: dict | None = None,
-                 limite_grosso: int = LIMITE_GROSSO, margem: int = MARGEM):
+                 limite_grosso: int = LIMITE_GROSSO, margem: int = MARGEM, sms: int | None = None):
         self.tanques = tanques
         self.h = h
         self.margem = margem
         self.grupos = agrupar(tanques, limite_grosso, margem)
         self.atlas, self.sims = [], []
         self.onde = {}  # tank -> (atlas, position in the atlas)
+        atlas = [montar_atlas(Cena, [tanques[k] for k in g], h, margem) for g in self.grupos]
+        fundido = (opcoes or {}).get("engine", _abi.TQ_ENGINE_PLAIN) == _abi.TQ_ENGINE_FUSED
+        self.ctas = (repartir_ctas([at["cena"].nx * at["cena"].ny for at in atlas], sms)
+                     if sms and fundido and len(atlas) > 1 else None)
         for a, g in enumerate(self.grupos):
-            at = montar_atlas(Cena, [tanques[k] for k in g], h, margem)
-            sim = fabrica(at["cena"], dict(opcoes or {}))
+            at = atlas[a]
+            o_at = dict(opcoes or {})
+            if self.ctas:
+                o_at["fused_ctas"] = self.ctas[a]
+            sim = fabrica(at["cena"], o_at)
             sim.adicionar(at["particulas"], False)
             # every tank's own convergence (tq_set_tanks) where the engine offers it: the fused
             # engine in tolerance mode
@@ -188,7 +220,15 @@ class Lote:
 
     def avancar(self, dt: float, subpassos: int = 1, grafo: bool = False):
         """One frame of every atlas (each on its simulation's stream); with `grafo` the
-        substeps replay from each atlas's CUDA graph (tq_advance_graph) where available."""
+        substeps replay from each atlas's CUDA graph (tq_advance_graph) where available, and
+        with the SMs split between the atlases (`sms`) every frame is queued before the first
+        is waited for, so the atlases run side by side."""
+        if grafo and self.ctas and all(hasattr(s, "lancarGrafo") for s in self.sims):
+            for s in self.sims:
+                s.lancarGrafo(dt, subpassos)
+            for s in self.sims:
+                s.sincronizar()
+            return
         for s in self.sims:
             if grafo and hasattr(s, "avancarGrafo"):
                 s.avancarGrafo(dt, subpassos)
@@ -232,7 +272,7 @@ class Lote:
 
 
 def autoajustar(fabrica, Cena, tanques: list[dict], h: float, opcoes: dict, dt: float, subpassos: int,
-                candidatos=(3000, 6000, 12000), repeticoes: int = 1) -> tuple[int, dict]:
+                candidatos=(3000, 6000, 12000), repeticoes: int = 1, sms: int | None = None) -> tuple[int, dict]:
     """The atlas grouping by measurement: for each candidate limit of the coarsest level's cells
     (which sets how many atlases the batch makes, their padding, and each atlas's V-cycle depth
     and coarsest-level size), build the batch, run one warm-up frame, then time `repeticoes`
@@ -242,7 +282,7 @@ def autoajustar(fabrica, Cena, tanques: list[dict], h: float, opcoes: dict, dt: 
     import time
     tempos = {}
     for lim in candidatos:
-        lote = Lote(fabrica, Cena, tanques, h, opcoes, limite_grosso=lim)
+        lote = Lote(fabrica, Cena, tanques, h, opcoes, limite_grosso=lim, sms=sms)
         try:
             lote.avancar(dt, subpassos, grafo=True)
             lote.sincronizar()

@@ -114,6 +114,12 @@ class Simulacao:
         self._lig("advance", self._h, float(dt), int(subpassos))
         self._andou = True
 
+    def lancarGrafo(self, dt: float, subpassos: int = 1):
+        """avancarGrafo without waiting for the frame (tq_launch_graph); sincronizar() waits
+        and reports a solve that gave up."""
+        self._lig("launch_graph", self._h, float(dt), int(subpassos))
+        self._andou = True
+
     def avancarGrafo(self, dt: float, subpassos: int = 1):
         """avancar with the substeps replayed from a CUDA graph (tq_advance_graph): same bits."""
         self._lig("advance_graph", self._h, float(dt), int(subpassos))
@@ -337,7 +343,7 @@ def resolver_pressao(tipo, div, q, iteracoes=ITERACOES_PCG, tolerancia=0.0, bolh
     args += [precond, normas, 1024, C.byref(nn), C.byref(inf)]
     lig("solve_pressure", *args)
     if info is not None:
-        info.update({k: getattr(inf, k) for k, _ in _abi.TqSolveInfo._fields_ if k != "pad"})
+        info.update({k: getattr(inf, k) for k, _ in _abi.TqSolveInfo._fields_})
     return np.array(normas[: nn.value])
 
 

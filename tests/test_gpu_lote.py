@@ -23,6 +23,8 @@ H = 1 / 128
 SOLVE = {"tolerance": 1e-6, "iterations": 200}
 MOTORES = [pytest.param({"precision": _abi.TQ_PREC_FP32, "engine": _abi.TQ_ENGINE_PLAIN}, id="fp32-plain"),
            pytest.param({"precision": _abi.TQ_PREC_FP16, "engine": _abi.TQ_ENGINE_FUSED}, id="fp16-fused"),
+           pytest.param({"precision": _abi.TQ_PREC_FP16, "engine": _abi.TQ_ENGINE_FUSED, "fused_ctas": 21},
+                        id="fp16-fused-21-ctas"),
            pytest.param({"precision": _abi.TQ_PREC_FP16, "engine": _abi.TQ_ENGINE_FUSED, "paredes": True},
                         id="fp16-fused-pulando-paredes")]
 # The fused engine skips blocks of wall alone on levels of at least two rounds of its warps;
@@ -101,6 +103,42 @@ def test_lote_no_gpu(lib_gpu):
         assert np.all(np.isfinite(q[:, :4]))
         assert np.all(q[:, 0] > 0) and np.all(q[:, 0] < t[k]["nx"] * H)
     lote.fechar()
+
+
+def test_atlas_lado_a_lado(lib_gpu):
+    """The atlases' frames side by side: the SMs split between the atlases' fused solves
+    (tq_options.fused_ctas) and every frame queued before any is waited for
+    (tq_launch_graph).  Against the same batch stepped one atlas at a time on the whole GPU:
+    every solve of both converges for every tank, and the particles agree to the solves'
+    accuracy (positions to 1e-4 m after two frames; the reductions' order differs with the CTA
+    count, so the bits do)."""
+    import torch
+    t = _tanques()
+    opc = dict(SOLVE, iterations=1000, precision=_abi.TQ_PREC_FP16, engine=_abi.TQ_ENGINE_FUSED,
+               preconditioner=_abi.TQ_PRECOND_BLOCK)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    lado = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, t, H, opc, limite_grosso=300, sms=sms)
+    seq = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, t, H, opc, limite_grosso=300)
+    assert lado.ctas is not None and len(lado.ctas) == len(lado.sims) >= 2 and sum(lado.ctas) <= sms
+    assert seq.ctas is None
+    for lote in (lado, seq):
+        for s in lote.sims:
+            s.definirEscalar(_abi.TQ_SCALAR_SOLVES, 0)
+        for _ in range(2):
+            lote.avancar(1 / 60, 4, grafo=True)
+        lote.sincronizar()
+        for s in lote.sims:
+            assert s.escalar(_abi.TQ_SCALAR_SOLVES) == 8
+            assert s.escalar(_abi.TQ_SCALAR_SOLVES_CAPPED) == 0
+            r = s.residuosTanques()
+            agua = r[:, 0] > 0
+            assert np.all(r[agua, 1] <= 1e-6 * r[agua, 0])
+    for k in range(len(t)):
+        a, b = lado.particulas(k), seq.particulas(k)
+        assert a.shape == b.shape
+        assert float(np.max(np.abs(a[:, :2].astype(np.float64) - b[:, :2]))) < 1e-4
+    lado.fechar()
+    seq.fechar()
 
 
 @pytest.mark.parametrize("precond", [_abi.TQ_PRECOND_REFERENCE, _abi.TQ_PRECOND_BLOCK], ids=["referencia", "bloco"])

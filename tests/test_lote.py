@@ -176,3 +176,22 @@ def test_autoajuste_escolhe_o_mais_rapido():
     assert melhor == min(tempos, key=tempos.get)
     grupos = {lim: len(Lote(Falsa, Cena, t, 1 / 128, {}, limite_grosso=lim).atlas) for lim in tempos}
     assert grupos[200] >= grupos[800] >= grupos[3200]  # a larger limit makes fewer atlases
+
+
+@pytest.mark.parametrize("total", [148, 60, 9, 7])
+def test_repartir_ctas(total):
+    """The SMs split between atlases in proportion to their cells, each at least the minimum
+    (or total // atlases when that is smaller), the sum within the SM count; no split with
+    more atlases than SMs."""
+    from tanque.lote import repartir_ctas
+    pesos = [3_000_000, 2_900_000, 740_000, 700_000, 500_000, 170_000, 160_000, 150_000]
+    c = repartir_ctas(pesos, total)
+    if total < len(pesos):
+        assert c is None
+        return
+    assert len(c) == len(pesos) and sum(c) <= total
+    assert min(c) >= max(1, min(4, total // len(pesos)))
+    if total >= 60:
+        assert c == sorted(c, reverse=True)  # larger atlases, more CTAs
+        assert c[0] >= int(total * pesos[0] / sum(pesos)) - len(pesos)
+    assert repartir_ctas([], total) == []
