@@ -897,6 +897,9 @@ int resolverPressao(Pcg* p, const Dev& d0, int iteracoes, double tol, bool bolha
   prepararNiveis(p, p->tipoL[0], bloco, s);
   cudaMemsetAsync(d.facesB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
   cudaMemsetAsync(d.celsB, 0, MAX_BOLHAS * sizeof(uint32_t), s);
+  // the previous solve left its stop flag set: clear it before the first kernel that tests it
+  // (the initial bubble sums and rows below; NORMA0 resets the rest of the record)
+  cudaMemsetAsync(&d.esc->pronto, 0, sizeof(int), s);
   if (bolhas) {
     lanca(k_bolhas_faces, nb, 256, 0, s, d);
     lanca(k_bolhas_celulas, nb, 256, 0, s, d);

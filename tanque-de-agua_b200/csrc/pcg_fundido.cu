@@ -116,6 +116,7 @@ struct Fundido {
   long long limite = LIMITE_CICLOS;
   int segurarCta = -1;
   long long segurarCiclos = 0;
+  int varredurasBloco = VARREDURAS;  // red-black sweeps per smoother pass, block preconditioner
 };
 
 struct Args {
@@ -152,6 +153,7 @@ struct Args {
   int segurarCta;            // test hook: this CTA arrives late at the first barrier (-1: none)
   long long segurarCiclos;   // ... after waiting this many cycles (bounded)
   int bloco;  // TQ_PRECOND_BLOCK: bubble rows Jacobi, V-cycle on water, coarse masks from faces
+  int varreduras;  // red-black sweeps per smoother pass (VARREDURAS, the reference's, unless BLOCK)
   // tolerance mode: q accumulates in FP64 (q64) and the solve stops on the true residual
   // ||b - A q64|| (FP64), with residual replacement; null in fixed-count mode
   double* q64;
@@ -478,7 +480,7 @@ __device__ __forceinline__ void meiaReg(float (&x)[2][4], const float (&bq)[2][4
 // The VARREDURAS red-black sweeps (js/pressao-cpu.js:114-137) of the warp's block in registers;
 // v = neighbour mask | 16 water | 128 in grid, bq = right side; ordem 0 sweeps colour 0 first.
 __device__ __forceinline__ void varrerReg(float (&x)[2][4], const int (&v)[2][4], const float (&bq)[2][4],
-                                         const Moldura& f, int ordem, bool masc) {
+                                         const Moldura& f, int ordem, bool masc, int nVarr) {
   float iq[2][4], at[2][4];
 #pragma unroll
   for (int c = 0; c < 2; c++)
@@ -490,7 +492,7 @@ __device__ __forceinline__ void varrerReg(float (&x)[2][4], const int (&v)[2][4]
     }
   // rolled loop: the pass code stays small in the instruction cache, which each phase enters cold
 #pragma unroll 1
-  for (int h = 0; h < 2 * VARREDURAS; h++) {
+  for (int h = 0; h < 2 * nVarr; h++) {
     if (((h & 1) ^ ordem) == 0) meiaReg<0>(x, bq, iq, at, f, v, masc);
     else meiaReg<1>(x, bq, iq, at, f, v, masc);
   }
@@ -668,7 +670,7 @@ __device__ __forceinline__ void suavizarBloco(const Args& a, const NivelF& n, in
   for (int cr = 0; cr < 2; cr++)
 #pragma unroll
     for (int m = 0; m < 4; m++) mexe |= (v[cr][m] & 16) && (v[cr][m] & 15);
-  if (__any_sync(0xffffffffu, mexe)) varrerReg(x, v, bq, f, ordem, a.bloco != 0);
+  if (__any_sync(0xffffffffu, mexe)) varrerReg(x, v, bq, f, ordem, a.bloco != 0, a.varreduras);
   if (MODO == M_JUNTAR) {
     const float inv = 1.0f / ru.escala;
     float rv[2][4], zv[2][4];
@@ -949,7 +951,8 @@ struct NivelS {
 // One smoother pass over a level held in shared memory: the level's 16x16 blocks are taken in
 // turn by the CTA's warps, each sweeping its block in registers (varrerReg) from the snapshot
 // `src` and writing `dst`.
-__device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int ordem, int src, int dst, bool masc) {
+__device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int ordem, int src, int dst, bool masc,
+                       int nVarr) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, gl = lane >> 3, k = lane & 7;
   const int nx = n.nx, ny = n.ny;
   const int nbx = (nx + desl + 15) >> 4, nby = (ny + desl + 15) >> 4;
@@ -986,7 +989,7 @@ __device__ void passoS(float* F, const uint8_t* U, const NivelS n, int desl, int
       f.bai[j] = okB ? F[src + gx + (oy - 1) * nx] : 0.0f;
       f.cim[j] = okT ? F[src + gx + (oy + 16) * nx] : 0.0f;
     }
-    varrerReg(x, v, bq, f, ordem, masc);
+    varrerReg(x, v, bq, f, ordem, masc, nVarr);
 #pragma unroll
     for (int cr = 0; cr < 2; cr++)
 #pragma unroll
@@ -1166,9 +1169,9 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
   for (int l = a.Lc; l < a.L - 1; l++) {
     const NivelS f = s[l];
     const NivelS g = s[l + 1];
-    passoS(F, U, f, 0, 0, f.xa, f.xb, a.bloco != 0);
+    passoS(F, U, f, 0, 0, f.xa, f.xb, a.bloco != 0, a.varreduras);
     marcaSecao(a, marcar);
-    passoS(F, U, f, 8, 0, f.xb, f.xa, a.bloco != 0);
+    passoS(F, U, f, 8, 0, f.xb, f.xa, a.bloco != 0, a.varreduras);
     marcaSecao(a, marcar);
     // restringir: residuals of the fine level into its free x buffer, then the 4x4 gathers.
     // Out-of-range and dry neighbours enter with weight or value 0, which adds +0 to a sum.
@@ -1351,9 +1354,9 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
     }
     __syncthreads();
     marcaSecao(a, marcar);
-    passoS(F, U, f, 8, 1, f.xa, f.xb, a.bloco != 0);
+    passoS(F, U, f, 8, 1, f.xa, f.xb, a.bloco != 0, a.varreduras);
     marcaSecao(a, marcar);
-    passoS(F, U, f, 0, 1, f.xb, f.xa, a.bloco != 0);
+    passoS(F, U, f, 0, 1, f.xb, f.xa, a.bloco != 0, a.varreduras);
     marcaSecao(a, marcar);
   }
   const NivelS t = s[a.Lc];
@@ -2154,6 +2157,10 @@ Fundido* criarFundido(Pcg* p) {
       if (v > 0 && v <= LIMITE_CICLOS) f->limite = v;
     }
     if (const char* e = getenv("TQ_BARRIER_HOLD_CTA")) f->segurarCta = atoi(e);
+    if (const char* e = getenv("TQ_BLOCK_SWEEPS")) {
+      const int v = atoi(e);
+      if (v >= 1 && v <= 16) f->varredurasBloco = v;
+    }
     if (const char* e = getenv("TQ_BARRIER_HOLD_CYCLES")) {
       const long long v = atoll(e);
       f->segurarCiclos = v > 0 && v <= 4 * LIMITE_CICLOS ? v : 0;
@@ -2218,6 +2225,7 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   Fundido* f = p->fundido;
   Args a{};
   a.bloco = precond == TQ_PRECOND_BLOCK ? 1 : 0;
+  a.varreduras = a.bloco ? f->varredurasBloco : VARREDURAS;
   a.limite = f->limite;
   a.segurarCta = f->segurarCta;
   a.segurarCiclos = f->segurarCiclos;

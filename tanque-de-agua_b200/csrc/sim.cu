@@ -891,6 +891,7 @@ int tq_set_scalar(tq_sim* s, int32_t w, double v) {
       CK(cudaMemsetAsync(&e->solves, 0, sizeof e->solves + sizeof e->capados + sizeof e->itersAcum +
                                             sizeof e->trocasAcum + sizeof e->maxRel, s->s));
       CK(cudaStreamSynchronize(s->s));
+      s->itersBase = 0;  // the stage timing counts iterations from the same origin
       return TQ_OK;
     }
     case TQ_SCALAR_VMAX: {

@@ -205,3 +205,30 @@ def test_grafo_plano_com_tolerancia_recusado(lib_gpu):
     with pytest.raises(_abi.ErroTanque) as e:
         g.avancarGrafo(1 / 60, 2)
     assert e.value.status == _abi.TQ_E_STATE
+
+
+@pytest.mark.parametrize("precond", [_abi.TQ_PRECOND_REFERENCE, _abi.TQ_PRECOND_BLOCK], ids=["referencia", "bloco"])
+@pytest.mark.parametrize("motor", MOTORES)
+@pytest.mark.parametrize("nome", ["bolha", "copo"])
+def test_solve_nao_herda_o_anterior(lib_gpu, nome, motor, precond):
+    """A handle that has solved before gives the same substep, bit for bit, as a fresh handle
+    given the same state: nothing of a solve (its stop flag, its bubble sums) reaches the next.
+    A scene with trapped air and the cup scene, every solve to the tolerance."""
+    from estado import copiar_estado
+    opc = {"tolerance": 1e-6, "iterations": 1000, "precision": _abi.TQ_PREC_FP32, "engine": motor,
+           "preconditioner": precond}
+    cena, agua = CENAS[nome](Cena)
+    usada = SimulacaoGPU(cena, opc)
+    usada.adicionar(agua, False)
+    for _ in range(3):
+        usada.avancar(1 / 120, 2)
+    nova = SimulacaoGPU(cena, opc)
+    copiar_estado(usada, nova)
+    for s in (usada, nova):
+        s.subpasso(1 / 240)
+        assert s.escalar(_abi.TQ_SCALAR_PCG_CONVERGED) == 1
+    if nome == "bolha":  # trapped air: bubble rows in the solve
+        assert int(np.count_nonzero(usada.campo("vivo"))) >= 1
+    for campo in ["q", "u", "v", "pressaoBolha"]:
+        assert np.array_equal(usada.campo(campo), nova.campo(campo)), campo
+    assert usada.escalar(_abi.TQ_SCALAR_PCG_ITERS) == nova.escalar(_abi.TQ_SCALAR_PCG_ITERS)
