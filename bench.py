@@ -479,7 +479,9 @@ def executar_lote(args, rank, mundo, dist):
                 piores.append(float(np.max(r[agua, 1] / r[agua, 0])) if agua.any() else 0.0)
         solves = [estatisticas_solve(s) for s in lote.sims]
         celulas = [at["cena"].nx * at["cena"].ny for at in lote.atlas]
+        ms_atlas = [round(x, 2) for x in lote.ms_atlas()] if grafo else None
         res = dict(ms=ms, lancamentos=lanc, particulas=lote.n, etapas=etapas, celulas=celulas, ctas=lote.ctas,
+                   ms_atlas=ms_atlas,
                    max_rel_tanque=max(piores) if piores else None, solves=solves,
                    atlas=[[at["cena"].nx, at["cena"].ny] for at in lote.atlas], relogios=rel.resumo() if rel else None,
                    d2h=d2h / max(args.steps, 1))
@@ -530,6 +532,7 @@ def executar_lote(args, rank, mundo, dist):
             "mixed_engine": "fused, block preconditioner, each atlas's frame replayed from a CUDA graph, the atlases "
                             "side by side on shares of the SMs (fused_ctas)",
             "fused_ctas_rank0": misto["ctas"],
+            "sm_split": "CTAs in proportion to the atlas's cells, at least 4",
             "l2": "flushed (256 MB write) between timed steps", "parallelism": f"tanks split over {mundo} GPU(s) by cells",
         },
         "fp32_plain": {"value": round(valor_plano, 1), "unit": "tank-substeps/s", "mgpcg_gbs": round(r_p["gbs"], 1),
@@ -543,6 +546,7 @@ def executar_lote(args, rank, mundo, dist):
                   "speedup_vs_fp32_plain": round(valor / valor_plano, 3),
                   "stop": "every tank's own true residual <= 1e-6 of its own r0 (tq_set_tanks)",
                   "max_tank_true_rel_residual_last_solve": misto["max_rel_tanque"],
+                  "last_frame_ms_per_atlas": misto["ms_atlas"],
                   "solves_per_atlas": misto["solves"]},
         "roofline": {"kernel": "MGPCG pressure solve", "bound": "hbm", "achieved": round(r_m["gbs"], 1),
                      "peak": hbm, "peak_source": origem_pico, "unit": "GB/s", "frac": round(r_m["gbs"] / hbm, 4),

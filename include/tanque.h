@@ -293,7 +293,10 @@ enum tq_scalar {
   TQ_SCALAR_CLOSED_REGIONS = 16, /* closed regions (water sealed from every air cell at pressure
                                     0) whose right-hand side the last tolerance-mode solve
                                     projected onto A's range (see tq_solve_pressure) */
-  TQ_SCALAR_COUNT_ = 17
+  TQ_SCALAR_GRAPH_FRAME_MS = 17, /* device time (ms) of the last frame replayed from the graph
+                                    (tq_advance_graph / tq_launch_graph); waits for it; 0 before
+                                    the first */
+  TQ_SCALAR_COUNT_ = 18
 };
 int tq_get_scalar(tq_sim* s, int32_t which, double* out);
 int tq_set_scalar(tq_sim* s, int32_t which, double value);

@@ -2063,6 +2063,7 @@ int tqo_get_scalar(tqo_sim* s, int32_t which, double* out) {
       case TQ_SCALAR_SOLVE_MAX_REL: *out = S_.maxRel; break;
       case TQ_SCALAR_SOLVE_REPLACEMENTS: *out = (double)S_.trocasAcum; break;
       case TQ_SCALAR_CLOSED_REGIONS: *out = S_.info.regioes; break;
+      case TQ_SCALAR_GRAPH_FRAME_MS: *out = 0.0; break;  // no graphs on the CPU
       default: return fail(TQ_E_ARG, "unknown scalar");
     }
   });

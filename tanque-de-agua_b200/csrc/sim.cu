@@ -85,6 +85,9 @@ struct tq_sim {
   cudaGraphExec_t grafoExec = nullptr;
   double grafoDt = 0, grafoG[2] = {0, 0};  // gravity is a kernel argument baked into the graph
   int grafoSub = 0, grafoN = -1;
+  // device time of the last graph frame: events around its launch on the handle's stream
+  cudaEvent_t quadroEv[2] = {nullptr, nullptr};
+  bool quadroMedido = false;
 };
 
 namespace {
@@ -371,6 +374,8 @@ int tq_destroy(tq_sim* s) {
   if (s->s) cudaStreamSynchronize(s->s);
   if (s->grafoExec) cudaGraphExecDestroy(s->grafoExec);
   if (s->grafo) cudaGraphDestroy(s->grafo);
+  for (auto& e : s->quadroEv)
+    if (e) cudaEventDestroy(e);
   destruirPcg(s->pcg);
   destruirRastreador(s->ar);
   for (void* p : s->alocados) cudaFree(p);
@@ -667,8 +672,14 @@ static int lancarGrafo(tq_sim* s, double dt, int32_t sub) {
     s->grafoG[0] = s->o.gravity[0];
     s->grafoG[1] = s->o.gravity[1];
   }
+  if (!s->quadroEv[0] && (cudaEventCreate(&s->quadroEv[0]) != cudaSuccess ||
+                          cudaEventCreate(&s->quadroEv[1]) != cudaSuccess))
+    return falhaCuda(cudaGetLastError(), "frame events");
+  CK(cudaEventRecord(s->quadroEv[0], s->s));
   contarLancamento();
   CK(cudaGraphLaunch(s->grafoExec, s->s));
+  CK(cudaEventRecord(s->quadroEv[1], s->s));
+  s->quadroMedido = true;
   return TQ_OK;
 }
 
@@ -840,6 +851,15 @@ int tq_get_scalar(tq_sim* s, int32_t w, double* out) {
       return TQ_OK;
     }
     case TQ_SCALAR_PCG_TRUE_RES: return baixar(s, out, &s->d.esc->normaVerd, sizeof(double));
+    case TQ_SCALAR_GRAPH_FRAME_MS: {
+      *out = 0.0;
+      if (!s->quadroMedido) return TQ_OK;
+      CK(cudaEventSynchronize(s->quadroEv[1]));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, s->quadroEv[0], s->quadroEv[1]));
+      *out = ms;
+      return TQ_OK;
+    }
     case TQ_SCALAR_CLOSED_REGIONS: {
       int v = 0;
       int st = baixar(s, &v, &s->d.esc->regioes, sizeof v);

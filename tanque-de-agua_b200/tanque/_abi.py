@@ -42,7 +42,7 @@ TQ_SCALAR_GRAVITY_X, TQ_SCALAR_GRAVITY_Y = 7, 8
 TQ_SCALAR_PCG_TRUE_RES, TQ_SCALAR_PCG_CONVERGED = 9, 10
 TQ_SCALAR_SOLVES, TQ_SCALAR_SOLVES_CAPPED, TQ_SCALAR_SOLVE_ITERS = 11, 12, 13
 TQ_SCALAR_SOLVE_MAX_REL, TQ_SCALAR_SOLVE_REPLACEMENTS = 14, 15
-TQ_SCALAR_CLOSED_REGIONS = 16
+TQ_SCALAR_CLOSED_REGIONS, TQ_SCALAR_GRAPH_FRAME_MS = 16, 17
 
 
 class TqOptions(C.Structure):

@@ -176,7 +176,8 @@ class Lote:
     avancar(grafo=True) queues every atlas's frame (tq_launch_graph) before waiting for any."""
 
     def __init__(self, fabrica, Cena, tanques: list[dict], h: float, opcoes: dict | None = None,
-                 limite_grosso: int = LIMITE_GROSSO, margem: int = MARGEM, sms: int | None = None):
+                 limite_grosso: int = LIMITE_GROSSO, margem: int = MARGEM, sms: int | None = None,
+                 pesos: list[float] | None = None, minimo: int = 4):
         self.tanques = tanques
         self.h = h
         self.margem = margem
@@ -185,8 +186,9 @@ class Lote:
         self.onde = {}  # tank -> (atlas, position in the atlas)
         atlas = [montar_atlas(Cena, [tanques[k] for k in g], h, margem) for g in self.grupos]
         fundido = (opcoes or {}).get("engine", _abi.TQ_ENGINE_PLAIN) == _abi.TQ_ENGINE_FUSED
-        self.ctas = (repartir_ctas([at["cena"].nx * at["cena"].ny for at in atlas], sms)
-                     if sms and fundido and len(atlas) > 1 else None)
+        if pesos is None:
+            pesos = [at["cena"].nx * at["cena"].ny for at in atlas]
+        self.ctas = repartir_ctas(pesos, sms, minimo) if sms and fundido and len(atlas) > 1 else None
         for a, g in enumerate(self.grupos):
             at = atlas[a]
             o_at = dict(opcoes or {})
@@ -240,6 +242,11 @@ class Lote:
             if hasattr(s, "sincronizar"):
                 s.sincronizar()
 
+    def ms_atlas(self) -> list[float]:
+        """Device time (ms) of each atlas's last frame replayed from its graph
+        (TQ_SCALAR_GRAPH_FRAME_MS)."""
+        return [s.escalar(_abi.TQ_SCALAR_GRAPH_FRAME_MS) for s in self.sims]
+
     def colunas(self, k: int) -> tuple[int, int, int]:
         """(atlas, first column, end column) of tank k's cells, frame included."""
         a, i = self.onde[k]
@@ -272,7 +279,7 @@ class Lote:
 
 
 def autoajustar(fabrica, Cena, tanques: list[dict], h: float, opcoes: dict, dt: float, subpassos: int,
-                candidatos=(3000, 6000, 12000), repeticoes: int = 1, sms: int | None = None) -> tuple[int, dict]:
+                candidatos=(1500, 3000, 6000, 12000), repeticoes: int = 1, sms: int | None = None) -> tuple[int, dict]:
     """The atlas grouping by measurement: for each candidate limit of the coarsest level's cells
     (which sets how many atlases the batch makes, their padding, and each atlas's V-cycle depth
     and coarsest-level size), build the batch, run one warm-up frame, then time `repeticoes`

@@ -195,3 +195,4 @@ def test_repartir_ctas(total):
         assert c == sorted(c, reverse=True)  # larger atlases, more CTAs
         assert c[0] >= int(total * pesos[0] / sum(pesos)) - len(pesos)
     assert repartir_ctas([], total) == []
+
