@@ -410,10 +410,14 @@ def executar_lote(args, rank, mundo, dist):
 
     # the atlas grouping, chosen by measuring candidates (tanque.lote.autoajustar) on the mixed
     # configuration, before any timed or warm-up frame
-    from tanque.lote import autoajustar
+    from tanque.lote import autoajustar, pesar_por_iteracoes
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     limite, ajuste = autoajustar(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H,
                                  opcoes(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED), DT_QUADRO, sub, sms=sms)
+    # then the SMs' split between the side-by-side atlases: by cells, or by cells x iterations
+    pesos, ajuste_ctas = pesar_por_iteracoes(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H,
+                                             opcoes(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED), DT_QUADRO, sub,
+                                             limite, sms)
 
     def medir(precisao, motor, com_relogio=False, e2e=False, grafo=None):
         """Frames of the batch (`grafo`: each atlas's frame from its CUDA graph, the default
@@ -421,7 +425,7 @@ def executar_lote(args, rank, mundo, dist):
         by side); stage timing is recorded by eager frames only, each atlas on the whole GPU."""
         grafo = motor == _abi.TQ_ENGINE_FUSED if grafo is None else grafo
         lote = Lote(lambda c, o: SimulacaoGPU(c, o), Cena, meus, LOTE_H, opcoes(precisao, motor), limite_grosso=limite,
-                    sms=sms if grafo else None)
+                    sms=sms if grafo else None, pesos=pesos if grafo else None)
         fluxos = [torch.cuda.ExternalStream(s.stream()) for s in lote.sims]
         lig = _abi.carregar()
         saidas = []
@@ -532,7 +536,8 @@ def executar_lote(args, rank, mundo, dist):
             "mixed_engine": "fused, block preconditioner, each atlas's frame replayed from a CUDA graph, the atlases "
                             "side by side on shares of the SMs (fused_ctas)",
             "fused_ctas_rank0": misto["ctas"],
-            "sm_split": "CTAs in proportion to the atlas's cells, at least 4",
+            "sm_split": {"weights": "cells x mean iterations" if pesos is not None else "cells",
+                         "min_ctas": 4, "seconds_per_frame": {k: round(v, 4) for k, v in ajuste_ctas.items()}},
             "l2": "flushed (256 MB write) between timed steps", "parallelism": f"tanks split over {mundo} GPU(s) by cells",
         },
         "fp32_plain": {"value": round(valor_plano, 1), "unit": "tank-substeps/s", "mgpcg_gbs": round(r_p["gbs"], 1),

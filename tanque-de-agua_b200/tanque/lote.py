@@ -304,6 +304,39 @@ def autoajustar(fabrica, Cena, tanques: list[dict], h: float, opcoes: dict, dt: 
     return melhor, tempos
 
 
+def pesar_por_iteracoes(fabrica, Cena, tanques: list[dict], h: float, opcoes: dict, dt: float, subpassos: int,
+                        limite_grosso: int, sms: int) -> tuple[list[float] | None, dict]:
+    """Weights of the SM split between side-by-side atlases, by measurement: an atlas's work is
+    its cells times its solves' mean iteration count (the per-tank stop makes atlases of equal
+    size take different counts).  The split by cells runs a warm-up frame and a timed frame,
+    whose solve records give each atlas's mean iterations; the split by cells x iterations
+    then runs the same; the faster is kept.  Returns its weights (None: the cells) and the
+    seconds per frame of both."""
+    import time
+    tempos, pesos_trab = {}, None
+    for nome in ("celulas", "trabalho"):
+        lote = Lote(fabrica, Cena, tanques, h, opcoes, limite_grosso=limite_grosso, sms=sms,
+                    pesos=None if nome == "celulas" else pesos_trab)
+        try:
+            if lote.ctas is None:
+                return None, {}
+            lote.avancar(dt, subpassos, grafo=True)
+            for s in lote.sims:
+                s.definirEscalar(_abi.TQ_SCALAR_SOLVES, 0)
+            t0 = time.perf_counter()
+            lote.avancar(dt, subpassos, grafo=True)
+            tempos[nome] = time.perf_counter() - t0
+            if nome == "celulas":
+                pesos_trab = []
+                for at, s in zip(lote.atlas, lote.sims):
+                    n = max(s.escalar(_abi.TQ_SCALAR_SOLVES), 1.0)
+                    pesos_trab.append(at["cena"].nx * at["cena"].ny * s.escalar(_abi.TQ_SCALAR_SOLVE_ITERS) / n)
+        finally:
+            lote.fechar()
+    melhor = min(tempos, key=lambda k: (tempos[k], k))
+    return (pesos_trab if melhor == "trabalho" else None), tempos
+
+
 def repartir(tanques: list[dict], partes: int) -> list[list[int]]:
     """Tank indices per GPU: largest tank first onto the least-loaded GPU (by cells).  The tanks
     are independent, so the GPUs share no data while they step."""

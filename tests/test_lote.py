@@ -196,3 +196,59 @@ def test_repartir_ctas(total):
         assert c[0] >= int(total * pesos[0] / sum(pesos)) - len(pesos)
     assert repartir_ctas([], total) == []
 
+
+
+def test_pesar_por_iteracoes():
+    """tanque.lote.pesar_por_iteracoes: the SM split by cells, then by cells x the solves' mean
+    iterations (read from the handles' solve records after a frame), each timed over a frame;
+    the faster is kept.  Fake simulations whose solves take more iterations on smaller atlases,
+    a frame lasting as long as the slowest atlas (cells x iterations / CTAs), gain from it."""
+    import time as _t
+
+    from tanque import Cena, _abi
+    from tanque.lote import Lote, pesar_por_iteracoes
+
+    class Falsa:
+        def __init__(self, cena, opcoes):
+            self.celulas = cena.nx * cena.ny
+            self.iters = 2e5 / self.celulas
+            self.ctas = opcoes.get("fused_ctas", 148)
+            self.ms, self.solves, self.acum = 0.0, 0, 0.0
+
+        def adicionar(self, p, checar):
+            return 0
+
+        def lancarGrafo(self, dt, sub):
+            self.ms = 1e-3 * self.celulas * self.iters / self.ctas
+            self.solves += sub
+            self.acum += sub * self.iters
+
+        def sincronizar(self):
+            pass
+
+        def definirEscalar(self, qual, v):
+            assert qual == _abi.TQ_SCALAR_SOLVES and v == 0
+            self.solves, self.acum = 0, 0.0
+
+        def escalar(self, qual):
+            return {_abi.TQ_SCALAR_SOLVES: self.solves, _abi.TQ_SCALAR_SOLVE_ITERS: self.acum}[qual]
+
+        def fechar(self):
+            pass
+
+    orig = Lote.avancar
+
+    def avancar(self, dt, sub=1, grafo=False):
+        orig(self, dt, sub, grafo)
+        _t.sleep(max(s.ms for s in self.sims) / 1000)
+
+    t = gerar_tanques(n=16, s=5, h=1 / 128, largura=(40, 120), altura=(30, 60))
+    Lote.avancar = avancar
+    try:
+        pesos, tempos = pesar_por_iteracoes(Falsa, Cena, t, 1 / 128, {"engine": _abi.TQ_ENGINE_FUSED}, 1 / 60, 2,
+                                            200, 148)
+    finally:
+        Lote.avancar = orig
+    assert set(tempos) == {"celulas", "trabalho"}
+    assert tempos["trabalho"] < tempos["celulas"]
+    assert pesos is not None and max(pesos) / min(pesos) < 1.01  # cells x iterations: equal here
