@@ -54,6 +54,12 @@ MAX_ITER = 1000
 # first V-cycle).
 BYTES_ITER = {"fp32": 156.0, "fp16": 120.0, "bf16": 120.0}
 BYTES_SETUP = {"fp32": 110.0, "fp16": 85.0, "bf16": 85.0}
+# The block preconditioner's V-cycle takes one smoother pass a leg on the levels above 0, whose
+# cells add up to a third of level 0's: per fine cell its V-cycle moves 71 + (2*13 + 10 + 9) / 3
+# = 86 B instead of 71 * 4/3 = 94.7 (FP32), 38 + (2*7 + 5.5 + 4.5) / 3 = 46 B instead of
+# 38 * 4/3 = 50.7 (16-bit).
+BYTES_ITER_BLOCO = {"fp32": 147.3, "fp16": 115.3, "bf16": 115.3}
+BYTES_SETUP_BLOCO = {"fp32": 101.3, "fp16": 80.3, "bf16": 80.3}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fused FP16 solve of this
 # scene, from one ncu capture of the kernel: the solve's working set stays in L2.
 TRAFEGO_SOLVE_BYTES = 90_651_136
@@ -318,16 +324,17 @@ def executar_gpu(args, rank, mundo, dist):
     tempos = tempos_max_ranks([misto["ms"], fundido32["ms"], plano["ms"], e2e["ms"]], dist, "cuda")
     valor, valor_f32, valor_plano, valor_e2e = (vazao_replicas(mundo, args.steps, SUB, t) for t in tempos)
 
-    def roofline(res, rotulo):
+    def roofline(res, rotulo, bloco=False):
         et = res["etapas"]
         n_sub = max(et["subpassos"], 1)
         iters = et["iteracoes"] / n_sub
         t_solve = et["pressao"] / n_sub / 1000
-        b = NX * NY * (iters * BYTES_ITER[rotulo] + BYTES_SETUP[rotulo])
+        bi, bs = (BYTES_ITER_BLOCO, BYTES_SETUP_BLOCO) if bloco else (BYTES_ITER, BYTES_SETUP)
+        b = NX * NY * (iters * bi[rotulo] + bs[rotulo])
         gbs = b / t_solve / 1e9 if t_solve > 0 else 0.0
         return dict(iters=iters, ms_solve=t_solve * 1000, gbs=gbs, bytes=b)
 
-    r_m = roofline(misto_etapas, "fp16")
+    r_m = roofline(misto_etapas, "fp16", bloco=True)
     r_p = roofline(plano, "fp32")
     if rank != 0:
         return None
@@ -387,7 +394,7 @@ def executar_lote(args, rank, mundo, dist):
 
     import torch
     from tanque import Cena, SimulacaoGPU, _abi, passo_maximo
-    from tanque.lote import BYTES_POR_CELULA_ITER, Lote, gerar_tanques, repartir
+    from tanque.lote import BYTES_POR_CELULA_ITER, BYTES_POR_CELULA_ITER_BLOCO, Lote, gerar_tanques, repartir
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
@@ -492,10 +499,11 @@ def executar_lote(args, rank, mundo, dist):
         lote.fechar()
         return res
 
-    def solve(res, rotulo):
+    def solve(res, rotulo, bloco=False):
         """Pressure-solve figures of one rank: algorithmic MGPCG bytes over the solves' time."""
         t = sum(e["pressao"] for e in res["etapas"]) / 1000
-        b = sum(c * (e["iteracoes"] * BYTES_POR_CELULA_ITER[rotulo][0] + e["subpassos"] * BYTES_POR_CELULA_ITER[rotulo][1])
+        mb = BYTES_POR_CELULA_ITER_BLOCO if bloco else BYTES_POR_CELULA_ITER
+        b = sum(c * (e["iteracoes"] * mb[rotulo][0] + e["subpassos"] * mb[rotulo][1])
                 for c, e in zip(res["celulas"], res["etapas"]))
         iters = sum(e["iteracoes"] for e in res["etapas"]) / max(sum(e["subpassos"] for e in res["etapas"]), 1)
         return dict(gbs=b / t / 1e9 if t > 0 else 0.0, iters=iters, bytes=b, s=t)
@@ -507,7 +515,7 @@ def executar_lote(args, rank, mundo, dist):
     e2e = medir(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED, e2e=True)
     tempos = tempos_max_ranks([misto["ms"], plano["ms"], e2e["ms"]], dist, "cuda")
     valor, valor_plano, valor_e2e = (len(todos) * args.steps * sub / (t / 1000) for t in tempos)
-    r_m, r_p = solve(misto_etapas, "fp16"), solve(plano, "fp32")
+    r_m, r_p = solve(misto_etapas, "fp16", bloco=True), solve(plano, "fp32")
     if rank != 0:
         return None
     return {

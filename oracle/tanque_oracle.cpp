@@ -415,22 +415,28 @@ void resolverGrosso(Nivel<S>& n) {
     }
 }
 
-// cicloV, js/pressao-cpu.js:241-255
+// cicloV, js/pressao-cpu.js:241-255.  umaPassada (TQ_PRECOND_BLOCK; no counterpart in the
+// reference): the levels above 0 take one smoother pass a leg, shift 8, red-black on the way
+// down and black-red on the way up (the cycle stays symmetric).  On dumped pressure problems of
+// the 840x536 scene it costs 5-10 % more PCG iterations and saves 6 of the fused solver's 23
+// phases per iteration.
 template <class S>
-void cicloV(Niveis<S>& L, double omega = 1) {
+void cicloV(Niveis<S>& L, double omega = 1, bool umaPassada = false) {
   const int ida[2] = {0, 1}, volta[2] = {1, 0};
   int NL = (int)L.n.size();
   std::fill(L.n[0].x.begin(), L.n[0].x.end(), (S)0);
   for (int l = 0; l < NL - 1; l++) {
-    suavizar(L.n[l], 0, ida, omega);
+    const bool um = umaPassada && l >= 1;
+    if (!um) suavizar(L.n[l], 0, ida, omega);
     suavizar(L.n[l], 8, ida, omega);
     restringir(L.n[l], L.n[l + 1]);
   }
   resolverGrosso(L.n[NL - 1]);
   for (int l = NL - 2; l >= 0; l--) {
+    const bool um = umaPassada && l >= 1;
     prolongar(L.n[l + 1], L.n[l]);
     suavizar(L.n[l], 8, volta, omega);
-    suavizar(L.n[l], 0, volta, omega);
+    if (!um) suavizar(L.n[l], 0, volta, omega);
   }
 }
 
@@ -767,7 +773,7 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
   auto precondicionar = [&](std::vector<S>& destino, MapaB& destinoB) {
     n0.b = r;
     if (bloco) {  // bubble air is air to the V-cycle (r = 0 there); bubble rows: Jacobi
-      cicloV(L);
+      cicloV(L, 1.0, true);
       destino = n0.x;
       for (uint32_t b : ativos) destinoB.set(b, rb.get(b) / faces[b]);
       return;

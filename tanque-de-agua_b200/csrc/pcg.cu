@@ -811,11 +811,20 @@ static void prolongarNivel(Pcg* p, int l, cudaStream_t s) {
 }
 
 // cicloV (js/pressao-cpu.js:241-255); level-0 b and x = 0 already in place.
-static void cicloV(Pcg* p, cudaStream_t s) {
+// umaPassada (TQ_PRECOND_BLOCK): the levels above 0 take one smoother pass a leg (shift 8), whose
+// output (in tmp) becomes the level's x by swapping the two buffers; each level swaps twice a
+// cycle, so the buffers are back in place at its end (and a captured graph repeats itself).
+static void cicloV(Pcg* p, cudaStream_t s, bool umaPassada = false) {
   const int L = p->L;
+  auto trocar = [&](int l) { std::swap(p->xL[l], p->tmpL[l]); };
   for (int l = 0; l < L - 1; l++) {
-    suavizarNivel(p, l, 0, 0, true, s);
-    suavizarNivel(p, l, 8, 0, false, s);
+    if (umaPassada && l >= 1) {
+      suavizarNivel(p, l, 8, 0, true, s);
+      trocar(l);
+    } else {
+      suavizarNivel(p, l, 0, 0, true, s);
+      suavizarNivel(p, l, 8, 0, false, s);
+    }
     restringirNivel(p, l, s);
   }
   NivelDev<float> g = nivel<float>(p, L - 1);
@@ -823,8 +832,13 @@ static void cicloV(Pcg* p, cudaStream_t s) {
   lanca(k_grosso, 1, 1024, p->smemGrosso, s, g, p->smemGrosso ? 1 : 0);
   for (int l = L - 2; l >= 0; l--) {
     prolongarNivel(p, l, s);
-    suavizarNivel(p, l, 8, 1, true, s);
-    suavizarNivel(p, l, 0, 1, false, s);
+    if (umaPassada && l >= 1) {
+      suavizarNivel(p, l, 8, 1, true, s);
+      trocar(l);
+    } else {
+      suavizarNivel(p, l, 8, 1, true, s);
+      suavizarNivel(p, l, 0, 1, false, s);
+    }
   }
 }
 
@@ -852,7 +866,7 @@ static void precondicionar(Pcg* p, const Dev& d, bool bolhas, bool bloco, cudaSt
     using T = std::remove_pointer_t<decltype(tag)>;
     lanca(k_pre_espalhar<T>, nb, 256, 0, s, d, nivel<T>(p, 0), espalhar ? 1 : 0);
   });
-  cicloV(p, s);
+  cicloV(p, s, bloco);
   if (espalhar) cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;

@@ -157,6 +157,7 @@ struct Args {
   long long segurarCiclos;   // ... after waiting this many cycles (bounded)
   int bloco;  // TQ_PRECOND_BLOCK: bubble rows Jacobi, V-cycle on water, coarse masks from faces
   int varreduras;  // red-black sweeps per smoother pass (VARREDURAS, the reference's, unless BLOCK)
+  int umaPassada;  // BLOCK: one smoother pass a leg on the grid levels above 0 (see cicloV)
   // tolerance mode: q accumulates in FP64 (q64) and the solve stops on the true residual
   // ||b - A q64|| (FP64), with residual replacement; null in fixed-count mode
   double* q64;
@@ -1169,12 +1170,28 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
   __syncthreads();
   marcaSecao(a, marcar);
   const float pes[4] = {0.25f, 0.75f, 0.75f, 0.25f};
+  // the block preconditioner's single pass (see cicloV) ends in xb: the level's two buffers swap
+  // roles in this CTA's table (rebuilt at each call)
+  auto trocarS = [&](int l) {
+    if (threadIdx.x == 0) {
+      const int t = s[l].xa;
+      s[l].xa = s[l].xb;
+      s[l].xb = t;
+    }
+    __syncthreads();
+  };
   for (int l = a.Lc; l < a.L - 1; l++) {
-    const NivelS f = s[l];
+    NivelS f = s[l];
     const NivelS g = s[l + 1];
-    passoS(F, U, f, 0, 0, f.xa, f.xb, a.bloco != 0, a.varreduras);
-    marcaSecao(a, marcar);
-    passoS(F, U, f, 8, 0, f.xb, f.xa, a.bloco != 0, a.varreduras);
+    if (a.umaPassada) {
+      passoS(F, U, f, 8, 0, f.xa, f.xb, a.bloco != 0, a.varreduras);
+      trocarS(l);
+      f = s[l];
+    } else {
+      passoS(F, U, f, 0, 0, f.xa, f.xb, a.bloco != 0, a.varreduras);
+      marcaSecao(a, marcar);
+      passoS(F, U, f, 8, 0, f.xb, f.xa, a.bloco != 0, a.varreduras);
+    }
     marcaSecao(a, marcar);
     // restringir: residuals of the fine level into its free x buffer, then the 4x4 gathers.
     // Out-of-range and dry neighbours enter with weight or value 0, which adds +0 to a sum.
@@ -1358,8 +1375,12 @@ __device__ __noinline__ void secaoGrossa(const Args& a, unsigned char* smem, Niv
     __syncthreads();
     marcaSecao(a, marcar);
     passoS(F, U, f, 8, 1, f.xa, f.xb, a.bloco != 0, a.varreduras);
-    marcaSecao(a, marcar);
-    passoS(F, U, f, 0, 1, f.xb, f.xa, a.bloco != 0, a.varreduras);
+    if (a.umaPassada) {
+      trocarS(l);
+    } else {
+      marcaSecao(a, marcar);
+      passoS(F, U, f, 0, 1, f.xb, f.xa, a.bloco != 0, a.varreduras);
+    }
     marcaSecao(a, marcar);
   }
   const NivelS t = s[a.Lc];
@@ -1395,17 +1416,37 @@ __device__ void aplicarSecaoDensa(const Args& a, unsigned char* dyn) {
 }
 
 // ---------------------------------------------------------------- the V-cycle
+// After a single smoother pass (x -> tmp) the pass's output becomes the level's x: every CTA
+// swaps the two snapshots in its own copy of the level table, at the same point of the solve.
+// The barrier that follows (it opens with __syncthreads) publishes the swap to the CTA.
+__device__ __forceinline__ void trocarXTmp(int l) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    void* t = s_niv[l].x;
+    s_niv[l].x = s_niv[l].tmp;
+    s_niv[l].tmp = t;
+  }
+}
+
 // cicloV (js/pressao-cpu.js:241-255) between the spread of the residual (first pass) and the
-// gather of z (last pass): 5 Lc + 1 phases, each ending at a grid barrier.
+// gather of z (last pass): 5 Lc + 1 phases, each ending at a grid barrier.  With the block
+// preconditioner the grid levels above 0 take one smoother pass a leg (shift 8, red-black down
+// and black-red up, so the cycle stays symmetric): 3 Lc + 3 phases.
 template <class T>
 __device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char* smem, NivelS* tabS, int* tileOff,
                        const Reuniao& ru, double* sh, bool secaoDensa) {
   for (int l = 0; l < a.Lc; l++) {
     const int meia = s_niv[l].meia;
-    faseSuavizar<T>(a, l, 0, 0, true, l == 0 ? M_ESPALHAR : M_ZERO, areas, meia, ru, sh);
-    if (!barreira(a, ep)) return false;
-    faseSuavizar<T>(a, l, 8, 0, false, M_NORMAL, areas, meia, ru, sh);
-    if (!barreira(a, ep)) return false;
+    if (a.umaPassada && l >= 1) {
+      faseSuavizar<T>(a, l, 8, 0, true, M_ZERO, areas, meia, ru, sh);
+      trocarXTmp(l);
+      if (!barreira(a, ep)) return false;
+    } else {
+      faseSuavizar<T>(a, l, 0, 0, true, l == 0 ? M_ESPALHAR : M_ZERO, areas, meia, ru, sh);
+      if (!barreira(a, ep)) return false;
+      faseSuavizar<T>(a, l, 8, 0, false, M_NORMAL, areas, meia, ru, sh);
+      if (!barreira(a, ep)) return false;
+    }
     if (meia) faseRestringir<T>(a, l, areas);
     else faseRestringir<float>(a, l, areas);
     if (!barreira(a, ep)) return false;
@@ -1416,6 +1457,11 @@ __device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char*
   for (int l = a.Lc - 1; l >= 0; l--) {
     const int meia = s_niv[l].meia;
     faseSuavizar<T>(a, l, 8, 1, true, M_PROL, areas, meia, ru, sh);
+    if (a.umaPassada && l >= 1) {
+      trocarXTmp(l);
+      if (!barreira(a, ep)) return false;
+      continue;
+    }
     if (!barreira(a, ep)) return false;
     faseSuavizar<T>(a, l, 0, 1, false, l == 0 ? M_JUNTAR : M_NORMAL, areas, meia, ru, sh);
     if (!barreira(a, ep)) return false;
@@ -2225,6 +2271,7 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
   Args a{};
   a.bloco = precond == TQ_PRECOND_BLOCK ? 1 : 0;
   a.varreduras = a.bloco ? f->varredurasBloco : VARREDURAS;
+  a.umaPassada = a.bloco;
   a.limite = f->limite;
   a.segurarCta = f->segurarCta;
   a.segurarCiclos = f->segurarCiclos;

@@ -43,13 +43,18 @@ def secao(lv) -> int:
     return Lc
 
 
-def rotulos(Lc: int) -> list[str]:
+def rotulos(Lc: int, bloco: bool = False) -> list[str]:
+    """The fused solver's phases of one PCG iteration; with the block preconditioner the levels
+    above 0 take one smoother pass a leg."""
     out = ["DA", "B"]
     for l in range(Lc):
-        out += [("s0+spread L0" if l == 0 else f"s0 L{l}"), f"s8 L{l}", f"restr {l}>{l + 1}"]
+        if bloco and l >= 1:
+            out += [f"s8 L{l}", f"restr {l}>{l + 1}"]
+        else:
+            out += [("s0+spread L0" if l == 0 else f"s0 L{l}"), f"s8 L{l}", f"restr {l}>{l + 1}"]
     out += ["coarse section"]
     for l in range(Lc - 1, -1, -1):
-        out += [f"prol+s8 L{l}", ("s0+gather L0" if l == 0 else f"s0 L{l} up")]
+        out += [f"prol+s8 L{l}"] if bloco and l >= 1 else [f"prol+s8 L{l}", ("s0+gather L0" if l == 0 else f"s0 L{l} up")]
     return out
 
 
@@ -98,14 +103,15 @@ def main(argv=None):
         lig.lib.tq_get_phase_trace(sim._h, buf, 65536, C.byref(n))
         d = np.diff(np.array(buf[:n.value], dtype=np.int64)) / 1000.0
         Lc = secao(niveis(cena.nx, cena.ny))
-        per = 2 + 5 * Lc + 1
+        nomes = rotulos(Lc, args.precond == _abi.TQ_PRECOND_BLOCK)
+        per = len(nomes)
         # the last iteration runs DA and B only, then (tolerance mode) the true residual, then
         # the closing barrier
         fim = len(d) - (4 if args.tolerance > 0 else 3)
         ini = fim - (it - 1) * per
         if it > 1 and ini >= 0:
             med = np.median(d[ini:fim].reshape(it - 1, per), axis=0)
-            out["phases_us"] = {r: round(float(v), 2) for r, v in zip(rotulos(Lc), med)}
+            out["phases_us"] = {r: round(float(v), 2) for r, v in zip(nomes, med)}
             out["iteration_us"] = round(float(med.sum()), 1)
             out["pcg_iterations"] = it
             out["setup_us"] = round(float(d[:ini].sum()), 1)
