@@ -54,7 +54,7 @@ MAX_ITER = 1000
 # first V-cycle).
 BYTES_ITER = {"fp32": 156.0, "fp16": 120.0, "bf16": 120.0}
 BYTES_SETUP = {"fp32": 110.0, "fp16": 85.0, "bf16": 85.0}
-# The block preconditioner's V-cycle takes one smoother pass a leg on the levels above 0, whose
+# TQ_PRECOND_BLOCK_1's V-cycle takes one smoother pass a leg on the levels above 0, whose
 # cells add up to a third of level 0's: per fine cell its V-cycle moves 71 + (2*13 + 10 + 9) / 3
 # = 86 B instead of 71 * 4/3 = 94.7 (FP32), 38 + (2*7 + 5.5 + 4.5) / 3 = 46 B instead of
 # 38 * 4/3 = 50.7 (16-bit).
@@ -314,7 +314,9 @@ def executar_gpu(args, rank, mundo, dist):
         return res
 
     FUSED, PLAIN = _abi.TQ_ENGINE_FUSED, _abi.TQ_ENGINE_PLAIN
-    BLOCO, REF = _abi.TQ_PRECOND_BLOCK, _abi.TQ_PRECOND_REFERENCE
+    # the block preconditioner with one smoother pass a leg above level 0: the faster of the two
+    # block cycles on this latency-bound scene (the batch's large atlases take TQ_PRECOND_BLOCK)
+    BLOCO, REF = _abi.TQ_PRECOND_BLOCK_1, _abi.TQ_PRECOND_REFERENCE
     misto = medir(_abi.TQ_PREC_FP16, FUSED, BLOCO, grafo=True, com_relogio=True)
     misto_etapas = medir(_abi.TQ_PREC_FP16, FUSED, BLOCO, etapas=True)
     fundido32 = medir(_abi.TQ_PREC_FP32, FUSED, BLOCO, grafo=True)
@@ -356,14 +358,15 @@ def executar_gpu(args, rank, mundo, dist):
                         "added every frame, sigma=0.0728; one step = 1 relabel + 14 substeps of 1/840 s",
             "particles": misto["particulas"], "tolerance": TOL, "tolerance_on": "true FP64 residual ||b - A q||",
             "iteration_cap": MAX_ITER, "mixed_precision": "fp16 V-cycle storage",
-            "mixed_engine": "fused, block preconditioner, frames replayed from a CUDA graph",
+            "mixed_engine": "fused, block preconditioner with one smoother pass a leg above level 0 "
+                            "(TQ_PRECOND_BLOCK_1), frames replayed from a CUDA graph",
             "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{mundo}",
         },
         "mixed": {"solve": misto["solve"], "mgpcg_gbs": round(r_m["gbs"], 1), "pcg_iters": round(r_m["iters"], 2),
                   "ms_solve": round(r_m["ms_solve"], 4), "speedup_vs_fp32_plain": round(valor / valor_plano, 3),
                   "speedup_vs_fp32_fused": round(valor / valor_f32, 3)},
         "fp32_fused": {"value": round(valor_f32, 2), "unit": "steps/s", "solve": fundido32["solve"],
-                       "engine": "fused, block preconditioner, CUDA graph"},
+                       "engine": "fused, TQ_PRECOND_BLOCK_1, CUDA graph"},
         "fp32_plain": {"value": round(valor_plano, 2), "unit": "steps/s", "solve": plano["solve"],
                        "mgpcg_gbs": round(r_p["gbs"], 1), "pcg_iters": round(r_p["iters"], 2),
                        "ms_solve": round(r_p["ms_solve"], 4),
@@ -515,7 +518,7 @@ def executar_lote(args, rank, mundo, dist):
     e2e = medir(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED, e2e=True)
     tempos = tempos_max_ranks([misto["ms"], plano["ms"], e2e["ms"]], dist, "cuda")
     valor, valor_plano, valor_e2e = (len(todos) * args.steps * sub / (t / 1000) for t in tempos)
-    r_m, r_p = solve(misto_etapas, "fp16", bloco=True), solve(plano, "fp32")
+    r_m, r_p = solve(misto_etapas, "fp16"), solve(plano, "fp32")
     if rank != 0:
         return None
     return {
@@ -541,7 +544,8 @@ def executar_lote(args, rank, mundo, dist):
                           "seconds_per_frame_by_limit": {str(k): round(v, 4) for k, v in ajuste.items()}},
             "atlas_cells_rank0": sum(misto["celulas"]), "particles_rank0": misto["particulas"], "tolerance": TOL,
             "mixed_precision": "fp16 V-cycle storage",
-            "mixed_engine": "fused, block preconditioner, each atlas's frame replayed from a CUDA graph, the atlases "
+            "mixed_engine": "fused, block preconditioner (TQ_PRECOND_BLOCK), each atlas's frame replayed from a CUDA "
+                            "graph, the atlases "
                             "side by side on shares of the SMs (fused_ctas)",
             "fused_ctas_rank0": misto["ctas"],
             "sm_split": {"weights": "cells x mean iterations" if pesos is not None else "cells",

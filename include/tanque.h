@@ -66,6 +66,12 @@ extern "C" {
  *            differ from the reference's.  FUSED engine only. */
 #define TQ_PRECOND_REFERENCE 0
 #define TQ_PRECOND_BLOCK 1
+/* TQ_PRECOND_BLOCK_1: TQ_PRECOND_BLOCK whose V-cycle takes one smoother pass a leg on the
+ *            levels above 0 (shift 8, red-black down and black-red up, so it stays symmetric)
+ *            instead of two: more iterations, fewer and cheaper ones.  Faster where the solve
+ *            is latency-bound (the 840x536 scene: 107 iterations of 122 us against 97 of 152
+ *            us); slower on large atlases, whose level-0 passes dominate. */
+#define TQ_PRECOND_BLOCK_1 2
 
 /* Particle-to-grid transfer semantics (the oracle implements both; the CUDA library only
  * TQ_P2G_FIXED, the integer accumulation of js/gpu/fisica.js:77-131). */

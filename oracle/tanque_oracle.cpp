@@ -415,7 +415,7 @@ void resolverGrosso(Nivel<S>& n) {
     }
 }
 
-// cicloV, js/pressao-cpu.js:241-255.  umaPassada (TQ_PRECOND_BLOCK; no counterpart in the
+// cicloV, js/pressao-cpu.js:241-255.  umaPassada (TQ_PRECOND_BLOCK_1; no counterpart in the
 // reference): the levels above 0 take one smoother pass a leg, shift 8, red-black on the way
 // down and black-red on the way up (the cycle stays symmetric).  On dumped pressure problems of
 // the 840x536 scene it costs 5-10 % more PCG iterations and saves 6 of the fused solver's 23
@@ -611,14 +611,16 @@ int projetarFechadas(int nx, int ny, const uint8_t* tipo, const uint32_t* rot, S
 // each time the recursive one has fallen by FATOR_TROCA since the last replacement; unless the
 // solve ends there, it replaces the recursive one and the iteration goes on with the same
 // search direction (a residual replacement without restart).
-// precond = TQ_PRECOND_BLOCK replaces precondicionar (:352-361) by the block-diagonal form:
+// precond = TQ_PRECOND_BLOCK (and BLOCK_1, with one smoother pass a leg above level 0, see
+// cicloV) replaces precondicionar (:352-361) by the block-diagonal form:
 // bubble rows z_b = r_b / faces_b, the V-cycle on the water alone (enclosed air stays air) with
 // coarse neighbour masks from the fine faces (vizinhosPorFaces).
 template <class S>
 std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div, S* q,
                                 int iteracoes, const BolhasPCG<S>* bolhas, double tol,
                                 int precond = TQ_PRECOND_REFERENCE, InfoPCG* info = nullptr) {
-  const bool bloco = precond == TQ_PRECOND_BLOCK;
+  const bool bloco = precond == TQ_PRECOND_BLOCK || precond == TQ_PRECOND_BLOCK_1;
+  const bool umaPassada = precond == TQ_PRECOND_BLOCK_1;
   Nivel<S>& n0 = L.n[0];
   int nx = n0.nx, ny = n0.ny;
   int k = nx * ny;
@@ -773,7 +775,7 @@ std::vector<double> resolverPCG(Niveis<S>& L, const uint8_t* tipo, const S* div,
   auto precondicionar = [&](std::vector<S>& destino, MapaB& destinoB) {
     n0.b = r;
     if (bloco) {  // bubble air is air to the V-cycle (r = 0 there); bubble rows: Jacobi
-      cicloV(L, 1.0, true);
+      cicloV(L, 1.0, umaPassada);
       destino = n0.x;
       for (uint32_t b : ativos) destinoB.set(b, rb.get(b) / faces[b]);
       return;
@@ -1936,7 +1938,7 @@ static int validar(const tq_options* o) {
   if (o->nx < 3 || o->ny < 3 || !(o->h > 0)) return fail(TQ_E_ARG, "grid must be at least 3x3 with h > 0");
   if (o->iterations < 1) return fail(TQ_E_ARG, "iterations must be >= 1");
   if (o->p2g_mode != TQ_P2G_FLOAT && o->p2g_mode != TQ_P2G_FIXED) return fail(TQ_E_ARG, "bad p2g_mode");
-  if (o->preconditioner != TQ_PRECOND_REFERENCE && o->preconditioner != TQ_PRECOND_BLOCK)
+  if (o->preconditioner < TQ_PRECOND_REFERENCE || o->preconditioner > TQ_PRECOND_BLOCK_1)
     return fail(TQ_E_ARG, "bad preconditioner");
   return TQ_OK;
 }
@@ -2107,7 +2109,7 @@ int tqo_solve_pressure(int32_t nx, int32_t ny, const uint8_t* tipo, const float*
                        int32_t preconditioner, double* norms, int32_t norms_cap, int32_t* n_norms,
                        tq_solve_info* info) {
   if (nx < 3 || ny < 3 || !tipo || !div || !q || iterations < 1) return fail(TQ_E_ARG, "bad arguments");
-  if (preconditioner != TQ_PRECOND_REFERENCE && preconditioner != TQ_PRECOND_BLOCK)
+  if (preconditioner < TQ_PRECOND_REFERENCE || preconditioner > TQ_PRECOND_BLOCK_1)
     return fail(TQ_E_ARG, "bad preconditioner");
   Niveis<float> L;
   montarNiveis(L, nx, ny);

@@ -811,7 +811,7 @@ static void prolongarNivel(Pcg* p, int l, cudaStream_t s) {
 }
 
 // cicloV (js/pressao-cpu.js:241-255); level-0 b and x = 0 already in place.
-// umaPassada (TQ_PRECOND_BLOCK): the levels above 0 take one smoother pass a leg (shift 8), whose
+// umaPassada (TQ_PRECOND_BLOCK_1): the levels above 0 take one smoother pass a leg (shift 8), whose
 // output (in tmp) becomes the level's x by swapping the two buffers; each level swaps twice a
 // cycle, so the buffers are back in place at its end (and a captured graph repeats itself).
 static void cicloV(Pcg* p, cudaStream_t s, bool umaPassada = false) {
@@ -859,14 +859,14 @@ static void prepararNiveis(Pcg* p, const uint8_t* tipo0, bool bloco, cudaStream_
   }
 }
 
-static void precondicionar(Pcg* p, const Dev& d, bool bolhas, bool bloco, cudaStream_t s) {
+static void precondicionar(Pcg* p, const Dev& d, bool bolhas, bool bloco, bool umaPassada, cudaStream_t s) {
   int nb = blocos(d.N, 256);
   const bool espalhar = bolhas && !bloco;  // with BLOCK the V-cycle does not see the bubbles
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
     lanca(k_pre_espalhar<T>, nb, 256, 0, s, d, nivel<T>(p, 0), espalhar ? 1 : 0);
   });
-  cicloV(p, s, bloco);
+  cicloV(p, s, umaPassada);
   if (espalhar) cudaMemsetAsync(d.accB, 0, MAX_BOLHAS * sizeof(long long), s);
   comTipo(p, 0, [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
@@ -902,7 +902,8 @@ int resolverPressao(Pcg* p, const Dev& d0, int iteracoes, double tol, bool bolha
     q64 = p->q64;
   }
   if (p->motor == TQ_ENGINE_FUSED) return resolverPressaoFundido(p, d, iteracoes, tol, bolhas, precond, s);
-  const bool bloco = precond == TQ_PRECOND_BLOCK;
+  const bool bloco = precond == TQ_PRECOND_BLOCK || precond == TQ_PRECOND_BLOCK_1;
+  const bool umaPassada = precond == TQ_PRECOND_BLOCK_1;
   const int nb = blocos(d.N, 256);
   const int nbx = blocos(d.N > MAX_BOLHAS ? d.N : MAX_BOLHAS, 256);
   // operator (true types) and preconditioner types
@@ -927,7 +928,7 @@ int resolverPressao(Pcg* p, const Dev& d0, int iteracoes, double tol, bool bolha
   }
   produto(p, d, NORMA0, d.r, d.r, nullptr, 0, tol, bolhas, iteracoes, s);
   p->parar = &d.esc->pronto;  // the V-cycle kernels return once the solve has stopped
-  precondicionar(p, d, bolhas, bloco, s);
+  precondicionar(p, d, bolhas, bloco, umaPassada, s);
   lanca(k_copiar_pz, nbx, 256, 0, s, d);
   produto(p, d, RZ0, d.r, d.z, nullptr, 0, tol, bolhas, iteracoes, s);
   int it = 0;
@@ -959,7 +960,7 @@ int resolverPressao(Pcg* p, const Dev& d0, int iteracoes, double tol, bool bolha
       if (pronto) break;
     }
     lanca(k_guardar_z, nbx, 256, 0, s, d);
-    precondicionar(p, d, bolhas, bloco, s);
+    precondicionar(p, d, bolhas, bloco, umaPassada, s);
     produto(p, d, BETA, d.r, d.z, d.zOld, it, tol, bolhas, iteracoes, s);
     lanca(k_direcao, nbx, 256, 0, s, d);
   }

@@ -157,7 +157,7 @@ struct Args {
   long long segurarCiclos;   // ... after waiting this many cycles (bounded)
   int bloco;  // TQ_PRECOND_BLOCK: bubble rows Jacobi, V-cycle on water, coarse masks from faces
   int varreduras;  // red-black sweeps per smoother pass (VARREDURAS, the reference's, unless BLOCK)
-  int umaPassada;  // BLOCK: one smoother pass a leg on the grid levels above 0 (see cicloV)
+  int umaPassada;  // BLOCK_1: one smoother pass a leg on the grid levels above 0 (see cicloV)
   // tolerance mode: q accumulates in FP64 (q64) and the solve stops on the true residual
   // ||b - A q64|| (FP64), with residual replacement; null in fixed-count mode
   double* q64;
@@ -1429,9 +1429,9 @@ __device__ __forceinline__ void trocarXTmp(int l) {
 }
 
 // cicloV (js/pressao-cpu.js:241-255) between the spread of the residual (first pass) and the
-// gather of z (last pass): 5 Lc + 1 phases, each ending at a grid barrier.  With the block
-// preconditioner the grid levels above 0 take one smoother pass a leg (shift 8, red-black down
-// and black-red up, so the cycle stays symmetric): 3 Lc + 3 phases.
+// gather of z (last pass): 5 Lc + 1 phases, each ending at a grid barrier.  With
+// TQ_PRECOND_BLOCK_1 the grid levels above 0 take one smoother pass a leg (shift 8, red-black
+// down and black-red up, so the cycle stays symmetric): 3 Lc + 3 phases.
 template <class T>
 __device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char* smem, NivelS* tabS, int* tileOff,
                        const Reuniao& ru, double* sh, bool secaoDensa) {
@@ -2269,9 +2269,9 @@ int resolverPressaoFundido(Pcg* p, const Dev& d, int iteracoes, double tol, bool
                            cudaStream_t s) {
   Fundido* f = p->fundido;
   Args a{};
-  a.bloco = precond == TQ_PRECOND_BLOCK ? 1 : 0;
+  a.bloco = precond == TQ_PRECOND_BLOCK || precond == TQ_PRECOND_BLOCK_1 ? 1 : 0;
   a.varreduras = a.bloco ? f->varredurasBloco : VARREDURAS;
-  a.umaPassada = a.bloco;
+  a.umaPassada = precond == TQ_PRECOND_BLOCK_1 ? 1 : 0;
   a.limite = f->limite;
   a.segurarCta = f->segurarCta;
   a.segurarCiclos = f->segurarCiclos;

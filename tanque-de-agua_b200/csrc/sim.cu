@@ -293,7 +293,7 @@ int tq_create(const tq_options* o, tq_sim** out) {
   if (o->p2g_mode != TQ_P2G_FIXED) return falha(TQ_E_ARG, "the CUDA library implements TQ_P2G_FIXED only");
   if (o->precision < TQ_PREC_FP32 || o->precision > TQ_PREC_BF16) return falha(TQ_E_ARG, "bad precision");
   if (o->engine != TQ_ENGINE_PLAIN && o->engine != TQ_ENGINE_FUSED) return falha(TQ_E_ARG, "bad engine");
-  if (o->preconditioner != TQ_PRECOND_REFERENCE && o->preconditioner != TQ_PRECOND_BLOCK)
+  if (o->preconditioner < TQ_PRECOND_REFERENCE || o->preconditioner > TQ_PRECOND_BLOCK_1)
     return falha(TQ_E_ARG, "bad preconditioner");
   if (o->fused_ctas < 0) return falha(TQ_E_ARG, "fused_ctas must be >= 0");
   int st = iniciarCuda(o->device);

@@ -25,7 +25,7 @@ TQ_E_STATE = -7
 TQ_PREC_FP32, TQ_PREC_FP16, TQ_PREC_BF16 = 0, 1, 2
 TQ_ENGINE_PLAIN, TQ_ENGINE_FUSED = 0, 1
 TQ_P2G_FLOAT, TQ_P2G_FIXED = 0, 1
-TQ_PRECOND_REFERENCE, TQ_PRECOND_BLOCK = 0, 1
+TQ_PRECOND_REFERENCE, TQ_PRECOND_BLOCK, TQ_PRECOND_BLOCK_1 = 0, 1, 2
 
 # enum tq_field (include/tanque.h) -> (numpy dtype, size in units of N / nu / nv / 4096 / sdf)
 CAMPOS_ENUM = {

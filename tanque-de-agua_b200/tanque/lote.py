@@ -352,5 +352,5 @@ def repartir(tanques: list[dict], partes: int) -> list[list[int]]:
 # Algorithmic HBM bytes of the pressure solve per atlas cell: (per PCG iteration, per solve's
 # setup), for FP32 and 16-bit V-cycle storage (the same model as the single-tank benchmark).
 BYTES_POR_CELULA_ITER = {"fp32": (156.0, 110.0), "fp16": (120.0, 85.0), "bf16": (120.0, 85.0)}
-# the same with the block preconditioner (one smoother pass a leg on the levels above 0)
+# the same with TQ_PRECOND_BLOCK_1 (one smoother pass a leg on the levels above 0)
 BYTES_POR_CELULA_ITER_BLOCO = {"fp32": (147.3, 101.3), "fp16": (115.3, 80.3), "bf16": (115.3, 80.3)}

@@ -2,7 +2,7 @@
 times of the last frame or, with --phases, the fused solver's per-phase times of one substep.
 
     python -m tanque.rodar [--scene ultra|atlas] [--frames F] [--substeps S] [--precision 0|1|2]
-                           [--engine 0|1] [--precond 0|1] [--tolerance T] [--phases]
+                           [--engine 0|1] [--precond 0|1|2] [--tolerance T] [--phases]
 
 `ultra` is the 450k-cell scene of the throughput benchmark; `atlas` is the largest atlas of
 the 256-tank batch (tanque.lote).  Frames are 1/60 s split into S substeps (default: 14 for
@@ -65,7 +65,8 @@ def main(argv=None):
     ap.add_argument("--substeps", type=int, default=0, help="0: 14 (ultra) or the capillary limit (atlas)")
     ap.add_argument("--precision", type=int, default=1, help="0 FP32, 1 FP16, 2 BF16 V-cycle storage")
     ap.add_argument("--engine", type=int, default=1, help="0 plain, 1 fused")
-    ap.add_argument("--precond", type=int, default=1, help="0 reference, 1 block preconditioner")
+    ap.add_argument("--precond", type=int, default=1,
+                    help="0 reference, 1 block preconditioner, 2 block with one smoother pass a leg above level 0")
     ap.add_argument("--tolerance", type=float, default=1e-6)
     ap.add_argument("--phases", action="store_true", help="per-phase times of one more substep (fused engine)")
     args = ap.parse_args(argv)
@@ -103,7 +104,7 @@ def main(argv=None):
         lig.lib.tq_get_phase_trace(sim._h, buf, 65536, C.byref(n))
         d = np.diff(np.array(buf[:n.value], dtype=np.int64)) / 1000.0
         Lc = secao(niveis(cena.nx, cena.ny))
-        nomes = rotulos(Lc, args.precond == _abi.TQ_PRECOND_BLOCK)
+        nomes = rotulos(Lc, args.precond == _abi.TQ_PRECOND_BLOCK_1)
         per = len(nomes)
         # the last iteration runs DA and B only, then (tolerance mode) the true residual, then
         # the closing barrier

@@ -33,7 +33,8 @@ def problema(nome, passos=6):
 
 @pytest.mark.parametrize("motor", MOTORES)
 @pytest.mark.parametrize("prec", PRECS)
-@pytest.mark.parametrize("precond", [_abi.TQ_PRECOND_REFERENCE, _abi.TQ_PRECOND_BLOCK], ids=["referencia", "bloco"])
+@pytest.mark.parametrize("precond", [_abi.TQ_PRECOND_REFERENCE, _abi.TQ_PRECOND_BLOCK, _abi.TQ_PRECOND_BLOCK_1],
+                         ids=["referencia", "bloco", "bloco1"])
 @pytest.mark.parametrize("nome", ["bolha", "copo"])
 def test_tolerancia_verdadeira(lib_gpu, nome, precond, prec, motor):
     """Both engines stop on the true FP64 residual; q, y and the iteration count agree with the

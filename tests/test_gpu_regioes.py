@@ -29,6 +29,7 @@ MOTORES = [
     pytest.param(_abi.TQ_PREC_FP32, _abi.TQ_ENGINE_PLAIN, _abi.TQ_PRECOND_REFERENCE, id="fp32-plain"),
     pytest.param(_abi.TQ_PREC_FP32, _abi.TQ_ENGINE_FUSED, _abi.TQ_PRECOND_REFERENCE, id="fp32-fused"),
     pytest.param(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED, _abi.TQ_PRECOND_BLOCK, id="fp16-fused-block"),
+    pytest.param(_abi.TQ_PREC_FP16, _abi.TQ_ENGINE_FUSED, _abi.TQ_PRECOND_BLOCK_1, id="fp16-fused-block1"),
 ]
 
 

@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
 SUB = 14
 
 
-@pytest.mark.parametrize("precond", [_abi.TQ_PRECOND_REFERENCE, _abi.TQ_PRECOND_BLOCK], ids=["referencia", "bloco"])
+@pytest.mark.parametrize("precond", [_abi.TQ_PRECOND_REFERENCE, _abi.TQ_PRECOND_BLOCK, _abi.TQ_PRECOND_BLOCK_1],
+                         ids=["referencia", "bloco", "bloco1"])
 def test_subpasso_ultra(lib_gpu, precond):
     opc = {"tolerance": 1e-6, "iterations": 1000, "preconditioner": precond}
     cena_g, _, agua, torneira = cena_ultra(Cena)
@@ -53,7 +54,7 @@ def test_erro_ultra_contra_fp64(lib_gpu, capsys):
     storage once both solves meet the true 1e-6.  Bound: 1e-3 relative on q, u, v and the
     divergence; bubble volumes exact."""
     from estado import divergencia
-    opc = {"tolerance": 1e-6, "iterations": 1000, "preconditioner": _abi.TQ_PRECOND_BLOCK}
+    opc = {"tolerance": 1e-6, "iterations": 1000, "preconditioner": _abi.TQ_PRECOND_BLOCK_1}
     cena_g, _, agua, torneira = cena_ultra(Cena)
     cena_o, _, _, _ = cena_ultra(CenaOraculo)
     g = SimulacaoGPU(cena_g, dict(opc, engine=_abi.TQ_ENGINE_FUSED, precision=_abi.TQ_PREC_FP16))

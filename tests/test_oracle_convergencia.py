@@ -35,11 +35,12 @@ def resolver(tipo, div, bol, precond, iters=400, tol=1e-6):
     return q, b, n, info
 
 
+@pytest.mark.parametrize("bloco", [_abi.TQ_PRECOND_BLOCK, _abi.TQ_PRECOND_BLOCK_1], ids=["bloco", "bloco1"])
 @pytest.mark.parametrize("nome", ["bolha", "copo"])
-def test_bloco_e_referencia_dao_o_mesmo_q(nome):
+def test_bloco_e_referencia_dao_o_mesmo_q(nome, bloco):
     tipo, div, bol = problema(nome)
     q_r, b_r, n_r, i_r = resolver(tipo, div, bol, _abi.TQ_PRECOND_REFERENCE)
-    q_b, b_b, n_b, i_b = resolver(tipo, div, bol, _abi.TQ_PRECOND_BLOCK)
+    q_b, b_b, n_b, i_b = resolver(tipo, div, bol, bloco)
     for i in (i_r, i_b):
         assert i["converged"] == 1
         assert 0 <= i["true_residual"] <= 1e-6 * i["residual0"]

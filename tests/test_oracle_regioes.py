@@ -110,7 +110,8 @@ def projetado(tipo, div, bol):
 
 
 @pytest.mark.parametrize("bolha", [False, True], ids=["agua-selada", "selada-com-bolha"])
-@pytest.mark.parametrize("precond", [_abi.TQ_PRECOND_REFERENCE, _abi.TQ_PRECOND_BLOCK], ids=["ref", "bloco"])
+@pytest.mark.parametrize("precond", [_abi.TQ_PRECOND_REFERENCE, _abi.TQ_PRECOND_BLOCK, _abi.TQ_PRECOND_BLOCK_1],
+                         ids=["ref", "bloco", "bloco1"])
 def test_regiao_fechada_converge(bolha, precond):
     tipo, div, bol = dados(bolha)
     q = np.zeros(tipo.size, np.float32)
