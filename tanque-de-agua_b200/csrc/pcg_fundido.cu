@@ -792,24 +792,19 @@ __device__ __noinline__ void faseSuavizarT(const Args& a, int l, int desl, int o
   }
 }
 
+// Every grid level below the coarse section is stored as T (criarFundido), so a 16-bit kernel
+// carries no FP32 copy of the passes: smaller code, which each phase enters cold.
 template <class T>
 __device__ void faseSuavizar(const Args& a, int l, int desl, int ordem, bool paraTmp, int modo, float* areas, int meia,
                              const Reuniao& ru, double* sh) {
-  if (meia) {
+  (void)meia;
+  {
     switch (modo) {
       case M_PROL: faseSuavizarT<T, M_PROL>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
       case M_ZERO: faseSuavizarT<T, M_ZERO>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
       case M_ESPALHAR: faseSuavizarT<T, M_ESPALHAR>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
       case M_JUNTAR: faseSuavizarT<T, M_JUNTAR>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
       default: faseSuavizarT<T, M_NORMAL>(a, l, desl, ordem, paraTmp, areas, ru, sh);
-    }
-  } else {
-    switch (modo) {
-      case M_PROL: faseSuavizarT<float, M_PROL>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
-      case M_ZERO: faseSuavizarT<float, M_ZERO>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
-      case M_ESPALHAR: faseSuavizarT<float, M_ESPALHAR>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
-      case M_JUNTAR: faseSuavizarT<float, M_JUNTAR>(a, l, desl, ordem, paraTmp, areas, ru, sh); break;
-      default: faseSuavizarT<float, M_NORMAL>(a, l, desl, ordem, paraTmp, areas, ru, sh);
     }
   }
 }
@@ -1447,8 +1442,7 @@ __device__ bool cicloV(const Args& a, unsigned& ep, float* areas, unsigned char*
       faseSuavizar<T>(a, l, 8, 0, false, M_NORMAL, areas, meia, ru, sh);
       if (!barreira(a, ep)) return false;
     }
-    if (meia) faseRestringir<T>(a, l, areas);
-    else faseRestringir<float>(a, l, areas);
+    faseRestringir<T>(a, l, areas);
     if (!barreira(a, ep)) return false;
   }
   if (secaoDensa) aplicarSecaoDensa(a, smem);
@@ -2152,6 +2146,11 @@ Fundido* criarFundido(Pcg* p) {
     return nullptr;
   }
   f->Lc = Lc;
+  // 16-bit storage on every grid level below the coarse section (the smallest included), so the
+  // kernel's passes exist in one storage type only (faseSuavizar); the level buffers hold 4 bytes
+  // an element whatever they store
+  if (p->precisao != TQ_PREC_FP32)
+    for (int l = 0; l < Lc; l++) p->meia[l] = true;
   size_t porWarp = (size_t)(SUAV_W > REST_W ? SUAV_W : REST_W) * 4;
   size_t areas = (size_t)WARPS * porWarp;
   f->smem = bytes > areas ? bytes : areas;
