@@ -488,10 +488,10 @@ __global__ void k_adj_somar(const double* parc, int m, double* out) {
 // ---------------------------------------------------------------- CG kernels
 // The CG's scalars live on the device (esc): [0] ||b||^2, [1] alpha, [2] beta, [3] r.z, [4] the
 // latest dot, [5] a second dot, [6] the stop flag (as a double: 0 running, else the iteration
-// count at the stop, at least 1), [8] the same flag as an int for the V-cycle's kernels.  Every
-// kernel of an iteration returns at once after the flag is set, so the host reads it only now
-// and then and the result is that of stopping at the exact iteration.
-enum { E_B2 = 0, E_AL = 1, E_BE = 2, E_RZ = 3, E_D1 = 4, E_D2 = 5, E_PARA = 6, E_PARA_INT = 8, E_N = 9 };
+// count at the stop, at least 1), [8] the same flag as an int for the V-cycle's kernels, [9] the
+// iterations done.  Every kernel of an iteration returns at once after the flag is set, so the
+// host reads it only now and then and the result is that of stopping at the exact iteration.
+enum { E_B2 = 0, E_AL = 1, E_BE = 2, E_RZ = 3, E_D1 = 4, E_D2 = 5, E_PARA = 6, E_PARA_INT = 8, E_IT = 9, E_N = 10 };
 __device__ inline void pararCG(double* esc, int iteracoes) {
   esc[E_PARA] = iteracoes > 0 ? iteracoes : 1;
   *reinterpret_cast<int*>(esc + E_PARA_INT) = 1;
@@ -552,18 +552,21 @@ __global__ void k_adj_copiar_se(double* dst, const double* src, size_t n, const 
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
     dst[k] = src[k];
 }
-// the scalar steps of one CG iteration (one thread; `it` the iteration, from 0): modo 0 start
-// (||b||^2 in E_D1 -> E_B2, the flag cleared unless b = 0); 1 alpha = rz / p.Ap (E_D1); 2 the
-// stop test on r.r (E_D1); 3 Polak-Ribiere beta from r.z (E_D1) and r.zOld (E_D2); 4 rz
-__global__ void k_adj_escalares(double* esc, int modo, double tol2, int it) {
+// the scalar steps of one CG iteration (one thread; the iteration count in E_IT): modo 0 start
+// (||b||^2 in E_D1 -> E_B2, the flag cleared unless b = 0, no iterations); 1 alpha = rz / p.Ap
+// (E_D1); 2 the stop test on r.r (E_D1); 3 Polak-Ribiere beta from r.z (E_D1) and r.zOld (E_D2),
+// the iteration counted; 4 rz
+__global__ void k_adj_escalares(double* esc, int modo, double tol2) {
   if (modo == 0) {
     esc[E_B2] = esc[E_D1];
     esc[E_PARA] = 0.0;
+    esc[E_IT] = 0.0;
     *reinterpret_cast<int*>(esc + E_PARA_INT) = 0;
     if (esc[E_B2] == 0) pararCG(esc, 0);
     return;
   }
   if (esc[E_PARA] != 0) return;
+  const int it = (int)esc[E_IT];
   if (modo == 1) {
     const double pap = esc[E_D1];
     if (pap == 0) pararCG(esc, it);
@@ -574,6 +577,7 @@ __global__ void k_adj_escalares(double* esc, int modo, double tol2, int it) {
     const double rzn = esc[E_D1], cruz = esc[E_D2];
     esc[E_BE] = fmax(0.0, (rzn - cruz) / esc[E_RZ]);
     esc[E_RZ] = rzn;
+    esc[E_IT] = it + 1;
   } else if (modo == 4) {
     esc[E_RZ] = esc[E_D1];
   }
@@ -868,6 +872,9 @@ struct tq_adj {
   // CG
   double *r, *z, *zv, *p, *ap, *parc, *esc;  // esc: the CG's scalars (E_*) and a host-read slot (7)
   int itFrente = 0, itTras = 0;                // the last forward / adjoint solve's iteration count
+  uint8_t* tipoCG = nullptr;                   // the solve's cell types (copied in at each solve)
+  double* xCG = nullptr;                       // the solve's iterate (copied out at the end)
+  cudaGraphExec_t grafoCG = nullptr;           // one CG iteration (resolver)
   float *bf, *xf;
   double gth[2] = {0, 0};
 };
@@ -920,37 +927,30 @@ void somaDisp(tq_adj* a, const double* x, const double* y, int n, double* destin
 // take similar counts, so few iterations run past the stop (each of those returns at once in
 // every kernel but still costs its launches).  Returns TQ_OK or an error.
 constexpr int VERIFICAR = 8;
-int resolver(tq_adj* a, const uint8_t* tipo, const double* bdev, double* x, int* estimativa) {
+int resolver(tq_adj* a, const uint8_t* tipoIn, const double* bdev, double* xOut, int* estimativa) {
   const int N = a->N;
   const int g = gridDe(N);
   cudaStream_t st = a->s;
   double* esc = a->esc;
   const int* pararInt = reinterpret_cast<const int*>(esc + E_PARA_INT);
-  int it = 0;
+  // the solve works on the handle's own type and iterate buffers, so one captured iteration
+  // serves every solve of the handle (forward and adjoint, every step of the tape)
+  const uint8_t* tipo = a->tipoCG;
+  double* x = a->xCG;
+  if (cudaMemcpyAsync(a->tipoCG, tipoIn, N, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return TQ_E_CUDA;
   auto escalares = [&](int modo) {
     contarLancamento();
-    k_adj_escalares<<<1, 1, 0, st>>>(esc, modo, TOL_SOLVE * TOL_SOLVE, it);
+    k_adj_escalares<<<1, 1, 0, st>>>(esc, modo, TOL_SOLVE * TOL_SOLVE);
   };
-  bool preparar = true;  // the levels' types and masks: once per solve
-  auto precond = [&](int qual) {  // z = M r (the V-cycle on r scaled to unit norm; ||r||^2 in esc[qual])
+  auto precond = [&](int qual, bool preparar) {  // z = M r (the V-cycle on r scaled to unit norm; ||r||^2 in esc[qual])
     contarLancamento();
     k_adj_para_float<<<g, TB, 0, st>>>(N, tipo, a->r, esc, qual, a->bf);
     int e = cicloVDispositivo(a->pcg, tipo, a->bf, a->xf, st, preparar, pararInt);
-    preparar = false;
     contarLancamento();
     k_adj_de_float<<<g, TB, 0, st>>>(N, tipo, a->xf, esc, qual, a->z);
     return e;
   };
-  contarLancamento();
-  k_adj_mascarar<<<g, TB, 0, st>>>(N, tipo, bdev, a->r, x);
-  somaDisp(a, a->r, a->r, N, esc + E_D1);
-  escalares(0);  // ||b||^2, flag
-  if (precond(E_B2)) return TQ_E_CUDA;
-  contarLancamento();
-  k_adj_copiar_se<<<g, TB, 0, st>>>(a->p, a->z, N, esc);
-  somaDisp(a, a->r, a->z, N, esc + E_D1);
-  escalares(4);  // rz
-  for (; it < 2000; it++) {
+  auto iteracao = [&]() {
     contarLancamento();
     k_adj_aplicar<<<g, TB, 0, st>>>(a->D, tipo, a->p, a->ap, esc);
     somaDisp(a, a->p, a->ap, N, esc + E_D1);
@@ -961,12 +961,41 @@ int resolver(tq_adj* a, const uint8_t* tipo, const double* bdev, double* x, int*
     escalares(2);  // stop test
     contarLancamento();
     k_adj_copiar_se<<<g, TB, 0, st>>>(a->zv, a->z, N, esc);
-    if (precond(E_D1)) return TQ_E_CUDA;
+    const int e = precond(E_D1, false);
     somaDisp(a, a->r, a->z, N, esc + E_D1);
     somaDisp(a, a->r, a->zv, N, esc + E_D2);
-    escalares(3);  // beta
+    escalares(3);  // beta, the iteration counted
     contarLancamento();
     k_adj_direcao<<<g, TB, 0, st>>>(N, tipo, esc, a->z, a->p);
+    return e;
+  };
+  contarLancamento();
+  k_adj_mascarar<<<g, TB, 0, st>>>(N, tipo, bdev, a->r, x);
+  somaDisp(a, a->r, a->r, N, esc + E_D1);
+  escalares(0);  // ||b||^2, flag
+  if (precond(E_B2, true)) return TQ_E_CUDA;  // the levels' types and masks, once per solve
+  contarLancamento();
+  k_adj_copiar_se<<<g, TB, 0, st>>>(a->p, a->z, N, esc);
+  somaDisp(a, a->r, a->z, N, esc + E_D1);
+  escalares(4);  // rz
+  // one CG iteration as a CUDA graph, captured on the handle's first solve: its 50-odd small
+  // launches replay as one (every argument is a buffer of the handle; the scalars live in esc)
+  if (!a->grafoCG) {
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return TQ_E_CUDA;
+    const int e = iteracao();
+    cudaGraph_t gr = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(st, &gr);
+    if (e || ec != cudaSuccess || cudaGraphInstantiate(&a->grafoCG, gr, 0) != cudaSuccess) {
+      if (gr) cudaGraphDestroy(gr);
+      a->grafoCG = nullptr;
+      std::snprintf(g_erroAdj, sizeof g_erroAdj, "capturing the adjoint solve's CG iteration failed");
+      return TQ_E_CUDA;
+    }
+    cudaGraphDestroy(gr);
+  }
+  for (int it = 0; it < 2000; it++) {
+    contarLancamento();
+    if (cudaGraphLaunch(a->grafoCG, st) != cudaSuccess) return TQ_E_CUDA;
     if (it % VERIFICAR == VERIFICAR - 1 || it + 1 >= *estimativa - 2) {
       double para = 0;
       if (cudaMemcpyAsync(&para, esc + E_PARA, sizeof para, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -974,7 +1003,8 @@ int resolver(tq_adj* a, const uint8_t* tipo, const double* bdev, double* x, int*
         return TQ_E_CUDA;
       if (para != 0) {
         *estimativa = (int)para;
-        return TQ_OK;
+        return cudaMemcpyAsync(xOut, x, sizeof(double) * N, cudaMemcpyDeviceToDevice, st) == cudaSuccess ? TQ_OK
+                                                                                                      : TQ_E_CUDA;
       }
     }
   }
@@ -1115,7 +1145,7 @@ int tq_adj_create(const tq_adj_scene* d, int32_t device, tq_adj** out) {
        alocar(a, &a->Ub, nu) && alocar(a, &a->UWb, nu) && alocar(a, &a->Vb, nv) && alocar(a, &a->VWb, nv) &&
        alocar(a, &a->r, N) && alocar(a, &a->z, N) && alocar(a, &a->zv, N) && alocar(a, &a->p, N) &&
        alocar(a, &a->ap, N) && alocar(a, &a->parc, SOMA_CTAS) && alocar(a, &a->esc, E_N) && alocar(a, &a->bf, N) &&
-       alocar(a, &a->xf, N);
+       alocar(a, &a->xf, N) && alocar(a, &a->tipoCG, N) && alocar(a, &a->xCG, N);
   if (ok) a->pcg = criarPcg(d->nx, d->ny, TQ_PREC_FP32, TQ_ENGINE_PLAIN);
   if (!ok || !a->pcg) {
     tq_adj_destroy(a);
@@ -1196,6 +1226,7 @@ int tq_adj_create(const tq_adj_scene* d, int32_t device, tq_adj** out) {
 int tq_adj_destroy(tq_adj* a) {
   if (!a) return TQ_OK;
   if (a->s) cudaStreamSynchronize(a->s);
+  if (a->grafoCG) cudaGraphExecDestroy(a->grafoCG);
   destruirPcg(a->pcg);
   for (void* p : a->mem) cudaFree(p);
   if (a->s) cudaStreamDestroy(a->s);
