@@ -279,7 +279,8 @@ class Lote:
 
 
 def autoajustar(fabrica, Cena, tanques: list[dict], h: float, opcoes: dict, dt: float, subpassos: int,
-                candidatos=(1500, 3000, 6000, 12000), repeticoes: int = 1, sms: int | None = None) -> tuple[int, dict]:
+                candidatos=(2000, 3000, 4000, 6000, 12000), repeticoes: int = 1,
+                sms: int | None = None) -> tuple[int, dict]:
     """The atlas grouping by measurement: for each candidate limit of the coarsest level's cells
     (which sets how many atlases the batch makes, their padding, and each atlas's V-cycle depth
     and coarsest-level size), build the batch, run one warm-up frame, then time `repeticoes`
