@@ -2,16 +2,20 @@
 times of the last frame or, with --phases, the fused solver's per-phase times of one substep.
 
     python -m tanque.rodar [--scene ultra|atlas] [--frames F] [--substeps S] [--precision 0|1|2]
-                           [--engine 0|1] [--precond 0|1|2] [--tolerance T] [--phases]
+                           [--engine 0|1] [--precond 0|1|2] [--tolerance T] [--iterations K]
+                           [--phases]
 
 `ultra` is the 450k-cell scene of the throughput benchmark; `atlas` is the largest atlas of
 the 256-tank batch (tanque.lote).  Frames are 1/60 s split into S substeps (default: 14 for
-ultra, the capillary limit for the atlas); every pressure solve runs to the tolerance.
+ultra, the capillary limit for the atlas); every pressure solve runs to the tolerance, or
+exactly K iterations with --tolerance 0.
 
 It is the small, self-contained driver for single-kernel profiler captures (a handful of
 launches of the pressure solve on the real workload) and for the phase trace: with --phases
 the fused kernel stamps the global timer at every grid barrier of one more substep
 (tq_get_phase_trace), and the medians over that solve's PCG iterations are printed per phase.
+The trace needs --tolerance 0: in tolerance mode the iterations that check the true residual
+add phases, so the iterations of a solve do not all have the same phases.
 """
 from __future__ import annotations
 
@@ -68,8 +72,11 @@ def main(argv=None):
     ap.add_argument("--precond", type=int, default=1,
                     help="0 reference, 1 block preconditioner, 2 block with one smoother pass a leg above level 0")
     ap.add_argument("--tolerance", type=float, default=1e-6)
+    ap.add_argument("--iterations", type=int, default=1000, help="iteration cap (the count with --tolerance 0)")
     ap.add_argument("--phases", action="store_true", help="per-phase times of one more substep (fused engine)")
     args = ap.parse_args(argv)
+    if args.phases and args.tolerance > 0:
+        ap.error("--phases needs --tolerance 0 (a fixed iteration count, the same phases every iteration)")
     if args.scene == "ultra":
         cena, _, agua, _ = cena_ultra(Cena)
         sub = args.substeps or 14
@@ -79,7 +86,7 @@ def main(argv=None):
         at = montar_atlas(Cena, [t[k] for k in agrupar(t)[0]], h)
         cena, agua = at["cena"], at["particulas"]
         sub = args.substeps or math.ceil((1 / 60) / passo_maximo(h, cena.ny * h) - 1e-9)
-    sim = SimulacaoGPU(cena, {"tolerance": args.tolerance, "iterations": 1000, "precision": args.precision,
+    sim = SimulacaoGPU(cena, {"tolerance": args.tolerance, "iterations": args.iterations, "precision": args.precision,
                               "engine": args.engine, "preconditioner": args.precond})
     sim.adicionar(agua, False)
     for q in range(args.frames):
@@ -106,9 +113,8 @@ def main(argv=None):
         Lc = secao(niveis(cena.nx, cena.ny))
         nomes = rotulos(Lc, args.precond == _abi.TQ_PRECOND_BLOCK_1)
         per = len(nomes)
-        # the last iteration runs DA and B only, then (tolerance mode) the true residual, then
-        # the closing barrier
-        fim = len(d) - (4 if args.tolerance > 0 else 3)
+        # the last iteration runs DA and B only, then the closing barrier
+        fim = len(d) - 3
         ini = fim - (it - 1) * per
         if it > 1 and ini >= 0:
             med = np.median(d[ini:fim].reshape(it - 1, per), axis=0)
