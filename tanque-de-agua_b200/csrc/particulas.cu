@@ -15,26 +15,27 @@ namespace tq {
 // Integer particle-to-grid sums of js/gpu/fisica.js:77-131 (APIC velocity with affine term,
 // weights, bilinear density at cell centres, particle count, dye x256).  The CPU engine's
 // float sums (js/fisica-cpu.js:198-267) depend on particle order; integer sums do not, so
-// any thread schedule produces the same bits.  One atomic per contribution: grouping a warp's
-// equal targets first (match + reduce, then one atomic per group) gives the same bits but was
-// measured 4x slower on the 840x536 scene (0.34 against 0.085 ms per substep): B200's L2
-// atomics cost less than the match instructions they would save.
+// any thread schedule and any grouping of the additions produce the same bits.
 __device__ __forceinline__ int chao(float v, int lo, int hi) {
   float f = floorf(v);
   f = fminf(fmaxf(f, (float)lo), (float)hi);
   return (int)f;
 }
 
-__global__ void k_p2g(Dev d) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= d.esc->n) return;
-  const float4 a = d.p0[k];
+// The cell of a particle (the count's and the dye's cell): every sum of the particle lands in
+// columns ci-1..ci+1 and rows cj-1..cj+1 (u faces at column i, v faces at row j, cell centres).
+__device__ __forceinline__ void celulaDe(float x, float y, float inv, int nx, int ny, int& ci, int& cj) {
+  ci = chao(x * inv, 0, nx - 1);
+  cj = chao(y * inv, 0, ny - 1);
+}
+
+// Every integer contribution of one particle, handed to `soma(tipo, i, j, componente, valor)`:
+// tipo 0 a u face (componente 0 the weighted velocity, 1 the weight), 1 a v face, 2 a cell
+// centre (0 the density weight, 1 the count), 3 the cell's dye (componente 0-2).
+template <class F>
+__device__ __forceinline__ void contribuicoes(const float4& a, const float4& c, const float4& e, int nx, int ny,
+                                              float hf, float inv, int ci, int cj, F soma) {
   const float x = a.x, y = a.y;
-  if (!(x == x)) return;  // marked dead earlier in this frame
-  const float4 c = d.p1[k];
-  const int nx = d.nx, ny = d.ny;
-  const float hf = d.hf;
-  const float inv = __fdiv_rn(1.0f, hf);
   {
     float fx = x * inv, fy = y * inv - 0.5f;
     int i0 = chao(fx, 0, nx - 1), j0 = chao(fy, 0, ny - 2);
@@ -50,9 +51,8 @@ __global__ void k_p2g(Dev d) {
         float t1 = c.x * dx, t2 = c.y * dy;
         float val = a.z + (t1 + t2);
         float wv = w * val;
-        int idx = i0 + aa + (j0 + b) * (nx + 1);
-        atomicAdd(&d.accU[idx].x, __float2int_rn(wv * 65536.0f));
-        atomicAdd(&d.accU[idx].y, __float2int_rn(w * 65536.0f));
+        soma(0, i0 + aa, j0 + b, 0, __float2int_rn(wv * 65536.0f));
+        soma(0, i0 + aa, j0 + b, 1, __float2int_rn(w * 65536.0f));
       }
   }
   {
@@ -70,9 +70,8 @@ __global__ void k_p2g(Dev d) {
         float t1 = c.z * dx, t2 = c.w * dy;
         float val = a.w + (t1 + t2);
         float wv = w * val;
-        int idx = i0 + aa + (j0 + b) * nx;
-        atomicAdd(&d.accV[idx].x, __float2int_rn(wv * 65536.0f));
-        atomicAdd(&d.accV[idx].y, __float2int_rn(w * 65536.0f));
+        soma(1, i0 + aa, j0 + b, 0, __float2int_rn(wv * 65536.0f));
+        soma(1, i0 + aa, j0 + b, 1, __float2int_rn(w * 65536.0f));
       }
   }
   {
@@ -80,20 +79,110 @@ __global__ void k_p2g(Dev d) {
     int i0 = chao(fx, 0, nx - 2), j0 = chao(fy, 0, ny - 2);
     float tx = fx - (float)i0, ty = fy - (float)j0;
     float ox = 1.0f - tx, oy = 1.0f - ty;
-    int cc = i0 + j0 * nx;
-    atomicAdd(&d.accCel[cc].x, __float2int_rn((ox * oy) * 65536.0f));
-    atomicAdd(&d.accCel[cc + 1].x, __float2int_rn((tx * oy) * 65536.0f));
-    atomicAdd(&d.accCel[cc + nx].x, __float2int_rn((ox * ty) * 65536.0f));
-    atomicAdd(&d.accCel[cc + nx + 1].x, __float2int_rn((tx * ty) * 65536.0f));
+    soma(2, i0, j0, 0, __float2int_rn((ox * oy) * 65536.0f));
+    soma(2, i0 + 1, j0, 0, __float2int_rn((tx * oy) * 65536.0f));
+    soma(2, i0, j0 + 1, 0, __float2int_rn((ox * ty) * 65536.0f));
+    soma(2, i0 + 1, j0 + 1, 0, __float2int_rn((tx * ty) * 65536.0f));
   }
-  int ci = chao(x * inv, 0, nx - 1), cj = chao(y * inv, 0, ny - 1);
-  int cc = ci + cj * nx;
-  atomicAdd(&d.accCel[cc].y, 1);
-  const float4 e = d.p2[k];
+  soma(2, ci, cj, 1, 1);
   if (e.y != 0.0f || e.z != 0.0f || e.w != 0.0f) {
-    atomicAdd(&d.accCor[3 * cc], __float2int_rn(e.y * 256.0f));
-    atomicAdd(&d.accCor[3 * cc + 1], __float2int_rn(e.z * 256.0f));
-    atomicAdd(&d.accCor[3 * cc + 2], __float2int_rn(e.w * 256.0f));
+    soma(3, ci, cj, 0, __float2int_rn(e.y * 256.0f));
+    soma(3, ci, cj, 1, __float2int_rn(e.z * 256.0f));
+    soma(3, ci, cj, 2, __float2int_rn(e.w * 256.0f));
+  }
+}
+
+// One CTA of P2G_T consecutive particles.  The reference's particle order (kept: it is what
+// the host reads back) stays spatially coherent: particles are seeded cell by cell, move at
+// most a cell or so per substep, and compaction is stable.  So the CTA first takes the
+// bounding box of its particles' cells; when the box with its one-cell halo fits in
+// P2G_CAIXA entries, the contributions go to shared-memory sums of the box and each nonzero
+// sum then reaches the grid with one global atomic (the particles of a cell share their faces
+// and centres: about a third of the global atomics of one per contribution).  A CTA whose box
+// is larger (particles scattered) adds every contribution to the grid directly.
+constexpr int P2G_T = 256;
+constexpr int P2G_CAIXA = 1024;
+
+__global__ void __launch_bounds__(P2G_T) k_p2g(Dev d) {
+  __shared__ int2 sU[P2G_CAIXA], sV[P2G_CAIXA], sC[P2G_CAIXA];
+  __shared__ int sD[3 * P2G_CAIXA];
+  __shared__ int caixa[4];  // min ci, min cj, max ci, max cj of the CTA's live particles
+  const int k = blockIdx.x * P2G_T + threadIdx.x;
+  const int nx = d.nx, ny = d.ny;
+  const float hf = d.hf;
+  const float inv = __fdiv_rn(1.0f, hf);
+  float4 a = make_float4(0.f, 0.f, 0.f, 0.f), c = a, e = a;
+  bool vivo = k < d.esc->n;
+  if (vivo) {
+    a = d.p0[k];
+    vivo = a.x == a.x;  // NaN: marked dead earlier in this frame
+  }
+  int ci = 0, cj = 0;
+  if (vivo) {
+    c = d.p1[k];
+    e = d.p2[k];
+    celulaDe(a.x, a.y, inv, nx, ny, ci, cj);
+  }
+  if (threadIdx.x == 0) {
+    caixa[0] = caixa[1] = 0x7fffffff;
+    caixa[2] = caixa[3] = -1;
+  }
+  __syncthreads();
+  {
+    const int mi = __reduce_min_sync(0xffffffffu, vivo ? ci : 0x7fffffff);
+    const int mj = __reduce_min_sync(0xffffffffu, vivo ? cj : 0x7fffffff);
+    const int Mi = __reduce_max_sync(0xffffffffu, vivo ? ci : -1);
+    const int Mj = __reduce_max_sync(0xffffffffu, vivo ? cj : -1);
+    if ((threadIdx.x & 31) == 0 && Mi >= 0) {
+      atomicMin(&caixa[0], mi);
+      atomicMin(&caixa[1], mj);
+      atomicMax(&caixa[2], Mi);
+      atomicMax(&caixa[3], Mj);
+    }
+  }
+  __syncthreads();
+  if (caixa[2] < 0) return;  // no live particle in this CTA (uniform)
+  const int I0 = caixa[0] - 1, J0 = caixa[1] - 1;
+  const int W = caixa[2] - caixa[0] + 3, H = caixa[3] - caixa[1] + 3;
+  if (W * H > P2G_CAIXA) {  // scattered particles: one global atomic per contribution (uniform)
+    if (vivo)
+      contribuicoes(a, c, e, nx, ny, hf, inv, ci, cj, [&](int t, int i, int j, int comp, int v) {
+        if (t == 0) atomicAdd(comp ? &d.accU[i + j * (nx + 1)].y : &d.accU[i + j * (nx + 1)].x, v);
+        else if (t == 1) atomicAdd(comp ? &d.accV[i + j * nx].y : &d.accV[i + j * nx].x, v);
+        else if (t == 2) atomicAdd(comp ? &d.accCel[i + j * nx].y : &d.accCel[i + j * nx].x, v);
+        else atomicAdd(&d.accCor[3 * (i + j * nx) + comp], v);
+      });
+    return;
+  }
+  const int nb = W * H;
+  for (int t = threadIdx.x; t < nb; t += P2G_T) {
+    sU[t] = sV[t] = sC[t] = make_int2(0, 0);
+    sD[3 * t] = sD[3 * t + 1] = sD[3 * t + 2] = 0;
+  }
+  __syncthreads();
+  if (vivo)
+    contribuicoes(a, c, e, nx, ny, hf, inv, ci, cj, [&](int t, int i, int j, int comp, int v) {
+      const int b = (i - I0) + (j - J0) * W;
+      if (t == 0) atomicAdd(comp ? &sU[b].y : &sU[b].x, v);
+      else if (t == 1) atomicAdd(comp ? &sV[b].y : &sV[b].x, v);
+      else if (t == 2) atomicAdd(comp ? &sC[b].y : &sC[b].x, v);
+      else atomicAdd(&sD[3 * b + comp], v);
+    });
+  __syncthreads();
+  // a box entry that no particle touched holds 0 in every sum (and may lie outside the
+  // grid): only nonzero sums are added, each at an index inside its array
+  for (int t = threadIdx.x; t < nb; t += P2G_T) {
+    const int i = I0 + t % W, j = J0 + t / W;
+    const int2 u = sU[t], v = sV[t], cc = sC[t];
+    if (u.x) atomicAdd(&d.accU[i + j * (nx + 1)].x, u.x);
+    if (u.y) atomicAdd(&d.accU[i + j * (nx + 1)].y, u.y);
+    if (v.x) atomicAdd(&d.accV[i + j * nx].x, v.x);
+    if (v.y) atomicAdd(&d.accV[i + j * nx].y, v.y);
+    if (cc.x) atomicAdd(&d.accCel[i + j * nx].x, cc.x);
+    if (cc.y) atomicAdd(&d.accCel[i + j * nx].y, cc.y);
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+      if (sD[3 * t + q]) atomicAdd(&d.accCor[3 * (i + j * nx) + q], sD[3 * t + q]);
   }
 }
 
@@ -578,7 +667,7 @@ void lancarMancha(const Dev& d, int n, int w, int hp, unsigned long long* acc, f
 }
 
 void lancarP2G(const Dev& d, int nHint, cudaStream_t s) {
-  if (nHint > 0) lanca(k_p2g, blocos(nHint, 256), 256, 0, s, d);
+  if (nHint > 0) lanca(k_p2g, blocos(nHint, P2G_T), P2G_T, 0, s, d);
 }
 void lancarFaces(const Dev& d, float gdx, float gdy, cudaStream_t s) {
   int m = d.nu > d.nv ? d.nu : d.nv;

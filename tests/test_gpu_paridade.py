@@ -197,6 +197,34 @@ def test_subpasso_paridade(lib_gpu, nome, motor):
     del dt
 
 
+@pytest.mark.parametrize("ordem", ["embaralhada", "meio-a-meio"])
+def test_p2g_em_qualquer_ordem(lib_gpu, ordem):
+    """The particle-to-grid sums are the oracle's bit for bit whatever the particle order.
+    Shuffled particles give every block of 256 a bounding box larger than its shared-memory
+    sums hold, so each contribution goes to the grid directly; with only the second half
+    shuffled, the blocks of the first half sum in shared memory and the rest directly.  A third
+    of the particles carry dye."""
+    o, g = par("bolha")
+    o.avancar(1 / 60 / 3, 1)
+    P = o.p.reshape(-1, CAMPOS).copy()
+    n = len(P)
+    assert n > 8 * 256
+    rng = np.random.default_rng(11)
+    perm = rng.permutation(n)
+    if ordem == "meio-a-meio":
+        perm = np.concatenate([np.arange(n // 2), n // 2 + rng.permutation(n - n // 2)])
+    P = P[perm]
+    P[::3, 9:12] = rng.random((len(P[::3]), 3)).astype(np.float32)
+    o.definirParticulas(P)
+    copiar_estado(o, g)
+    o.avancar(1 / 60 / 3, 1)
+    g.avancar(1 / 60 / 3, 1)
+    for campo in ["accU", "accV", "accCel", "accCor"]:
+        a, b = g.campo(campo), o.campo(campo)
+        assert np.array_equal(a, b), f"{campo} differs in {np.count_nonzero(a != b)} entries"
+    assert np.count_nonzero(g.campo("accCor")) > 0
+
+
 @pytest.mark.parametrize("motor", MOTORES)
 def test_deterministico(lib_gpu, motor):
     """Two runs of the same scene produce identical bits."""
