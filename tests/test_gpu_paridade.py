@@ -198,12 +198,13 @@ def test_subpasso_paridade(lib_gpu, nome, motor):
 
 
 @pytest.mark.parametrize("ordem", ["embaralhada", "meio-a-meio"])
-def test_p2g_em_qualquer_ordem(lib_gpu, ordem):
-    """The particle-to-grid sums are the oracle's bit for bit whatever the particle order.
-    Shuffled particles give every block of 256 a bounding box larger than its shared-memory
-    sums hold, so each contribution goes to the grid directly; with only the second half
-    shuffled, the blocks of the first half sum in shared memory and the rest directly.  A third
-    of the particles carry dye."""
+def test_particulas_em_qualquer_ordem(lib_gpu, ordem):
+    """The particle-to-grid sums are the oracle's bit for bit, and the grid-to-particle
+    transfer within the substep tolerances, whatever the particle order.  Shuffled particles
+    give every block of 256 a bounding box larger than its shared-memory sums hold, so each
+    contribution goes to the grid directly; with only the second half shuffled, the blocks of
+    the first half sum in shared memory and the rest directly.  A third of the particles carry
+    dye."""
     o, g = par("bolha")
     o.avancar(1 / 60 / 3, 1)
     P = o.p.reshape(-1, CAMPOS).copy()
@@ -223,6 +224,11 @@ def test_p2g_em_qualquer_ordem(lib_gpu, ordem):
         a, b = g.campo(campo), o.campo(campo)
         assert np.array_equal(a, b), f"{campo} differs in {np.count_nonzero(a != b)} entries"
     assert np.count_nonzero(g.campo("accCor")) > 0
+    pg, po = g.p.reshape(-1, CAMPOS), o.p.reshape(-1, CAMPOS)
+    assert pg.shape == po.shape
+    assert float(np.max(np.abs(pg[:, :2].astype(np.float64) - po[:, :2]))) < 1e-6
+    assert erro_relativo(pg[:, 2:8], po[:, 2:8]) < 1e-4
+    assert erro_relativo(pg[:, 8:], po[:, 8:]) < 1e-5
 
 
 @pytest.mark.parametrize("motor", MOTORES)
