@@ -64,6 +64,10 @@ BYTES_SETUP_BLOCO = {"fp32": 101.3, "fp16": 80.3, "bf16": 80.3}
 # scene with TQ_PRECOND_BLOCK_1, from one ncu capture of the kernel: the solve's working set
 # stays in L2.
 TRAFEGO_SOLVE_BYTES = 17_849_856
+# Particle bytes a substep's particle kernels move per particle: P2G reads its three float4
+# records (position/velocity, affine terms, foam/dye); G2P reads the first and third and
+# writes all three.  The grid reads behind them are cached (L1/L2) and not counted.
+BYTES_PARTICULA = {"p2g": 48, "g2p": 80}
 
 
 def picos():
@@ -337,6 +341,20 @@ def executar_gpu(args, rank, mundo, dist):
         gbs = b / t_solve / 1e9 if t_solve > 0 else 0.0
         return dict(iters=iters, ms_solve=t_solve * 1000, gbs=gbs, bytes=b)
 
+    def particulas_gbs(res, n, pico):
+        """Particle bytes per second of the P2G and G2P stages (BYTES_PARTICULA x particles over
+        the stage's device time per substep); the P2G stage also zeroes the sums and computes
+        the face velocities."""
+        et = res["etapas"]
+        n_sub = max(et["subpassos"], 1)
+        out = {"bytes_per_particle": BYTES_PARTICULA, "particles": n}
+        for k, b in BYTES_PARTICULA.items():
+            t = et[k] / n_sub / 1000
+            gbs = n * b / t / 1e9 if t > 0 else 0.0
+            out[k + "_gbs"] = round(gbs, 1)
+            out[k + "_frac_of_hbm"] = round(gbs / pico, 4)
+        return out
+
     r_m = roofline(misto_etapas, "fp16", bloco=True)
     r_p = roofline(plano, "fp32")
     if rank != 0:
@@ -374,6 +392,7 @@ def executar_gpu(args, rank, mundo, dist):
                        "engine": "plain (one launch per reference dispatch), reference preconditioner"},
         "stages_ms_per_substep": {k: round(misto_etapas["etapas"][k] / max(misto_etapas["etapas"]["subpassos"], 1), 4)
                                   for k in SimulacaoGPU.ETAPAS},
+        "particle_stages": particulas_gbs(misto_etapas, misto["particulas"], hbm),
         "roofline": {"kernel": "MGPCG pressure solve (k_mgpcg)", "bound": "hbm", "achieved": round(r_m["gbs"], 1),
                      "peak": hbm, "peak_source": origem_pico, "unit": "GB/s",
                      "frac": round(r_m["gbs"] / hbm, 4), "traffic": TRAFEGO_SOLVE_BYTES,
