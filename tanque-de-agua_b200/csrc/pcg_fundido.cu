@@ -1504,8 +1504,7 @@ __device__ __forceinline__ float aplicarF(const Args& a, int c, FV val, FB valB)
   return (float)__popc(vz & 15) * val(c) - s;
 }
 
-constexpr int KDA = 4;             // cells per thread per batch in [DA]
-constexpr int DA_FAIXA_NX = 1024;  // [DA]: contiguous ranges per CTA up to this row length
+constexpr int KDA = 4;  // cells per thread per batch in [DA]
 
 // [DA] of a PCG iteration over this CTA's cells: p = z + beta p (z alone on the first
 // iteration), A p (js/pressao-cpu.js:84-93, bubble neighbours through their p), the partial of
@@ -1521,23 +1520,7 @@ __device__ __noinline__ void faseDA(const Args& a, const float* zc, const float*
                                     double beta, const double* pbVelho, double* sh) {
   const Dev& d = a.d;
   const int N = d.N, nx = d.nx;
-  // On a grid whose rows are short (at most DA_FAIXA_NX cells), each CTA takes a contiguous
-  // range of cells: the rows above and below a cell are then mostly the CTA's own, loaded
-  // through L1 a batch or two before.  Wider rows outgrow L1 and the grid-stride order is
-  // faster.  Measured: 13.0 against 13.6 us on the 840x536 scene; 126 against 109 us on the
-  // 38,370x316 atlas (grid stride there).
-  int gt0, GT, lim;
-  if (nx <= DA_FAIXA_NX) {
-    const int por = ((N + (int)gridDim.x - 1) / (int)gridDim.x + 31) & ~31;
-    const int ini = min(N, (int)blockIdx.x * por);
-    lim = min(N, ini + por);
-    gt0 = ini + threadIdx.x;
-    GT = TF;
-  } else {
-    gt0 = blockIdx.x * TF + threadIdx.x;
-    GT = gridDim.x * TF;
-    lim = N;
-  }
+  const int gt0 = blockIdx.x * TF + threadIdx.x, GT = gridDim.x * TF, lim = N;
   auto pbNovoV = [&](int b) {
     const double zb = zbDe(a, b);
     return prim ? zb : zb + beta * __ldcg(&pbVelho[b]);
